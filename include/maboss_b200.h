@@ -1,0 +1,216 @@
+/*
+ * maboss_b200.h -- C ABI of the B200 (sm_100a) trajectory engine for stochastic Boolean
+ * networks (MaBoSS semantics).
+ *
+ * This is the boundary that replaces, for the trajectory hot path, the C++ classes of the
+ * reference implementation (paths relative to the reference project):
+ *   driver            src/parser/driver.h:14-56          -> mb_model_*
+ *   generator         src/generator.h:7-23               -> mb_model_generate_code
+ *   kernel_compiler   src/kernel_compiler.h:8-20         -> mb_context_*, mb_module_*
+ *   kernel_wrapper    src/kernel.h:5-23                  -> mb_launch_*
+ *   simulation_runner src/simulation_runner.h:8-24       -> mb_run*, mb_result_*
+ *   stats plugins     src/statistics/stats.h:15-29,
+ *                     window_average_small.h, final_states.h, fixed_states.h -> mb_launch_*_stats,
+ *                     mb_result_* and the CSV writers
+ *
+ * Conventions:
+ *   - every function returns an mb_status (MB_OK == 0) and never exits the process; the
+ *     message of the last failure on the calling thread is returned by mb_last_error();
+ *   - handles are opaque; pointers are plain host or device pointers, sizes are explicit;
+ *   - device entry points take an explicit CUDA stream (cudaStream_t passed as void*);
+ *     NULL means the context's own stream;
+ *   - trajectory buffers are Structure-of-Arrays (SoA) with a row stride equal to the batch
+ *     capacity B:  states[(slot * W + word) * B + traj], times[slot * B + traj],
+ *     entropies[slot * B + traj], last_states[word * B + traj]
+ *     (the reference uses Array-of-Structures [traj][slot][word]).
+ */
+#ifndef MABOSS_B200_H
+#define MABOSS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int mb_status;
+#define MB_OK 0
+#define MB_ERR_INVALID 1   /* bad argument or handle */
+#define MB_ERR_PARSE 2     /* malformed .bnd/.cfg or semantic model error */
+#define MB_ERR_COMPILE 3   /* NVRTC compilation failure (log in mb_last_error) */
+#define MB_ERR_CUDA 4      /* CUDA runtime/driver failure */
+#define MB_ERR_LIMIT 5     /* size beyond a supported maximum, or out of device memory */
+#define MB_ERR_NO_DEVICE 6 /* no usable sm_100 device */
+#define MB_ERR_INTERNAL 7
+
+typedef struct mb_model_s* mb_model;     /* parsed model            (reference: driver) */
+typedef struct mb_context_s* mb_context; /* device + stream         (reference: kernel_compiler's context) */
+typedef struct mb_module_s* mb_module;   /* compiled model kernels  (reference: kernel_compiler's module) */
+typedef struct mb_result_s* mb_result;   /* statistics of one run   (reference: stats_composite after finalize) */
+
+/* Run modes. */
+#define MB_MODE_FUSED_EXACT 0 /* persistent kernel; bit-exact trajectories with the reference CUDA build */
+#define MB_MODE_FUSED_FAST 1  /* persistent kernel; Philox streams; statistically equivalent */
+#define MB_MODE_EPOCH 2       /* buffered 100-slot epochs through SoA trajectory buffers */
+
+/* Trajectory status byte (src/trajectory_status.h:3-8). */
+#define MB_STATUS_CONTINUE 0
+#define MB_STATUS_FINISHED 1
+#define MB_STATUS_FIXED_POINT 2
+
+const char* mb_version(void);
+const char* mb_last_error(void);
+
+/* ------------------------------------------------------------------ models (driver) */
+
+/* driver::parse(bnd_file, cfg_file), src/parser/driver.cpp:16-31. */
+mb_status mb_model_parse_files(const char* bnd_path, const char* cfg_path, mb_model* out);
+/* Same, from in-memory text. */
+mb_status mb_model_parse_text(const char* bnd_text, const char* cfg_text, mb_model* out);
+mb_status mb_model_free(mb_model m);
+
+/* driver::nodes (src/parser/driver.h:43): count, names, node_t::istate and node_t::is_internal
+ * (src/parser/parse_types.h:16-29). */
+mb_status mb_model_num_nodes(mb_model m, int* n);
+mb_status mb_model_node_name(mb_model m, int i, char* buf, size_t cap, size_t* len);
+mb_status mb_model_node_info(mb_model m, int i, float* istate, int* is_internal);
+mb_status mb_model_set_istate(mb_model m, int i, float istate);
+
+/* driver::constants and driver::variables (src/parser/driver.h:41-42). Missing constants read
+ * as 0 like std::map::operator[] in src/main.cpp:128-132; missing variables are an error. */
+mb_status mb_model_get_constant(mb_model m, const char* name, float* value);
+mb_status mb_model_set_constant(mb_model m, const char* name, float value);
+mb_status mb_model_get_variable(mb_model m, const char* name, float* value);
+mb_status mb_model_set_variable(mb_model m, const char* name, float value);
+mb_status mb_model_num_variables(mb_model m, int* n);
+mb_status mb_model_variable_name(mb_model m, int i, char* buf, size_t cap, size_t* len);
+
+/* generator::generate_code(), src/generator.cpp:11-55. Writes the generated CUDA source
+ * (NUL-terminated, truncated to cap) and its full length. */
+mb_status mb_model_generate_code(mb_model m, char* buf, size_t cap, size_t* len);
+
+/* ------------------------------------------------------------------ device / JIT (kernel_compiler) */
+
+/* kernel_compiler::kernel_compiler(), src/kernel_compiler.cpp:46-52 (binds the primary context of
+ * `device` instead of creating a private context). */
+mb_status mb_context_create(int device, mb_context* out);
+mb_status mb_context_free(mb_context c);
+mb_status mb_context_stream(mb_context c, void** stream);
+mb_status mb_context_sm_count(mb_context c, int* sm_count);
+
+/* kernel_compiler::compile_simulation(code, discrete_time), src/kernel_compiler.cpp:61-164:
+ * NVRTC-compiles generated code together with the engine kernels for sm_100a. */
+mb_status mb_module_compile(mb_context c, const char* generated_code, mb_module* out);
+/* Generate + compile in one call; the module keeps the model's layout. */
+mb_status mb_module_compile_model(mb_context c, mb_model m, mb_module* out);
+mb_status mb_module_free(mb_module mod);
+/* NVRTC compilation of generated code + engine for sm_100a without a device (build checks);
+ * writes the cubin size and the compiler log. */
+mb_status mb_jit_check(const char* generated_code, size_t* cubin_size, char* log, size_t cap);
+mb_status mb_module_state_size(mb_module mod, int* state_size, int* state_words);
+/* NVRTC log of the compilation (may be empty). */
+mb_status mb_module_log(mb_module mod, char* buf, size_t cap, size_t* len);
+
+/* ------------------------------------------------------------------ kernel entry points (kernel_wrapper) */
+/* Size in bytes of one per-trajectory random state (curandState, XORWOW). */
+size_t mb_rand_state_size(void);
+
+/* initialize_random, src/jit_kernels/simulation.cu:23-32: curand_init(seed, first + i, 0). */
+mb_status mb_launch_initialize_random(mb_module mod, void* stream, int n, unsigned long long seed,
+                                      unsigned long long first, void* rands);
+/* initialize_initial_state, src/jit_kernels/simulation.cu:34-71 (SoA last_states). */
+mb_status mb_launch_initialize_initial_state(mb_module mod, void* stream, int n, int stride,
+                                             const float* initial_probs, uint32_t* last_states,
+                                             float* last_times, void* rands);
+/* simulate, src/generator.cpp:189-203 + src/jit_kernels/simulation.cu:77-164 (SoA buffers,
+ * `traj_len` slots per epoch); adds the number of recorded steps to *transitions (device u64). */
+mb_status mb_launch_simulate(mb_module mod, void* stream, int n, int stride, int traj_len,
+                             uint32_t* last_states, float* last_times, void* rands,
+                             uint32_t* traj_states, float* traj_times, float* traj_entropies,
+                             uint8_t* statuses, unsigned long long* transitions);
+
+/* Device-side statistics accumulators of one run (window_average_small_stats,
+ * final_states_stats, fixed_states_stats). */
+typedef struct mb_stats_s* mb_stats;
+/* window_average_small_stats ctor (src/statistics/window_average_small.cpp:7-41) + the other two:
+ * windows = ceil(max_time / time_tick); non-internal mask given as node indices. */
+mb_status mb_stats_create(mb_module mod, float time_tick, float max_time, int discrete_time,
+                          const int* noninternal_nodes, int n_noninternal, long long sample_count,
+                          mb_stats* out);
+mb_status mb_stats_free(mb_stats st);
+/* window_average_small{,_discrete}, src/jit_kernels/window_average_small.cu:50-136 */
+mb_status mb_launch_window_average_stats(mb_stats st, void* stream, int n, int stride, int traj_len,
+                                         const uint32_t* traj_states, const float* traj_times,
+                                         const float* traj_entropies);
+/* final_states, src/jit_kernels/final_states.cu:9-21 */
+mb_status mb_launch_final_states_stats(mb_stats st, void* stream, int n, int stride,
+                                       const uint32_t* last_states, const uint8_t* statuses);
+/* fixed_states_stats::process_batch, src/statistics/fixed_states.cu:84-125 */
+mb_status mb_launch_fixed_states_stats(mb_stats st, void* stream, int n, int stride,
+                                       const uint32_t* last_states, const uint8_t* statuses);
+/* stats::finalize (device -> host); the result is independent of the stats object. */
+mb_status mb_stats_finalize(mb_stats st, long long n_trajectories, mb_result* out);
+
+/* ------------------------------------------------------------------ whole runs (simulation_runner) */
+
+typedef struct mb_run_config_s
+{
+    int mode;                      /* MB_MODE_* */
+    long long sample_count;        /* number of trajectories */
+    unsigned long long seed;       /* seed_pseudorandom */
+    unsigned long long first_traj; /* random-stream id of trajectory 0 (sharding / replicas) */
+    int traj_len;                  /* epoch length (reference: trajectory_len_limit = 100) */
+    int batch_limit;               /* epoch batch (reference: trajectory_batch_limit = 1e6) */
+    int block;                     /* threads per block (multiple of 32, <= 256) */
+    int blocks_per_sm;             /* 0 = occupancy calculator */
+    int fixed_capacity_log2;       /* fixed-point table capacity, 0 = automatic */
+} mb_run_config;
+
+/* Defaults from the model's .cfg constants: mode FUSED_EXACT, traj_len 100, batch 1e6. */
+mb_status mb_run_config_default(mb_model m, mb_run_config* cfg);
+
+/* simulation_runner(n, N, seed, initial_probs).run_simulation(...) with the three built-in stats
+ * plugins (src/main.cpp:54-83). The module must come from mb_module_compile_model. */
+mb_status mb_run(mb_module mod, const mb_run_config* cfg, mb_result* out);
+
+/* A run with device buffers allocated once (the reference allocates them per
+ * simulation_runner::run_simulation, simulation_runner.cu:65-82). mb_runner_launch clears the
+ * accumulators and enqueues the simulation on `stream` without synchronising (fused modes; the
+ * epoch mode synchronises once per epoch); mb_runner_result waits and copies the statistics back. */
+typedef struct mb_runner_s* mb_runner;
+mb_status mb_runner_create(mb_module mod, const mb_run_config* cfg, mb_runner* out);
+mb_status mb_runner_launch(mb_runner r, void* stream);
+mb_status mb_runner_result(mb_runner r, void* stream, mb_result* out);
+/* number of engine kernels one mb_runner_launch enqueues (fused modes) */
+mb_status mb_runner_kernel_launches(mb_runner r, unsigned* n);
+mb_status mb_runner_free(mb_runner r);
+
+/* ------------------------------------------------------------------ results */
+mb_status mb_result_free(mb_result r);
+/* dims: windows, bins (2^k), non-internal count k, state words W, node count N */
+mb_status mb_result_dims(mb_result r, int* windows, int* bins, int* noninternal, int* state_words, int* nodes);
+mb_status mb_result_transitions(mb_result r, unsigned long long* transitions);
+/* kernel_ms: simulation + statistics kernels; total_ms: the whole run on the device */
+mb_status mb_result_timing(mb_result r, float* kernel_ms, float* total_ms, int* epochs);
+/* Window probabilities [windows * bins] (window_average_small.cpp:126-140) and TH [windows]. */
+mb_status mb_result_window_probs(mb_result r, double* probs);
+mb_status mb_result_window_entropy(mb_result r, double* th);
+/* Raw accumulators: continuous occupancy in fixed point (value * 2^exponent) or discrete counts. */
+mb_status mb_result_window_raw(mb_result r, long long* occupancy, unsigned* counts, long long* entropy,
+                               int* occupancy_exponent, int* entropy_exponent);
+mb_status mb_result_final_counts(mb_result r, unsigned* counts);
+mb_status mb_result_num_fixed(mb_result r, int* n, unsigned* overflow);
+mb_status mb_result_fixed(mb_result r, int i, uint32_t* state_words, unsigned* count);
+
+/* Output writers: <prefix>_probtraj.csv (window_average_small.cpp:181-250) and <prefix>_fp.csv
+ * (fixed_states.cu:154-187); visualize() text of all three plugins (stdout format of
+ * src/main.cpp:85-99). Node names come from the model. */
+mb_status mb_result_write_csv(mb_result r, mb_model m, const char* prefix);
+mb_status mb_result_visualize(mb_result r, mb_model m, char* buf, size_t cap, size_t* len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MABOSS_B200_H */

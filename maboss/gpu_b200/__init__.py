@@ -1,0 +1,11 @@
+"""B200 (sm_100a) trajectory engine for stochastic Boolean networks (MaBoSS semantics).
+
+The engine is the C-ABI library libmaboss_b200.so (include/maboss_b200.h); this package is a
+thin ctypes binding over it. Nothing here computes trajectories: without the library every
+entry point raises.
+"""
+from ._lib import EngineError, build, lib
+from .engine import Context, Model, Module, Result, RunConfig, Stats, rand_state_size
+
+__all__ = ["EngineError", "build", "lib", "Context", "Model", "Module", "Result", "RunConfig", "Stats",
+           "rand_state_size"]

@@ -1,0 +1,701 @@
+// C ABI (include/maboss_b200.h) over the C++ runtime. Every entry point catches exceptions
+// and turns them into status codes with a thread-local message.
+#include "maboss_b200.h"
+
+#include <curand_kernel.h>
+
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <string>
+
+#include "codegen.h"
+#include "model.h"
+#include "output.h"
+#include "runtime.h"
+
+struct mb_model_s
+{
+	mb::model_t model;
+};
+struct mb_context_s
+{
+	std::unique_ptr<mb::context> ctx;
+};
+struct mb_module_s
+{
+	std::unique_ptr<mb::module> mod;
+};
+struct mb_result_s
+{
+	std::unique_ptr<mb::result> res;
+};
+struct mb_stats_s
+{
+	mb::stats_state st;
+};
+struct mb_runner_s
+{
+	std::unique_ptr<mb::runner> rn;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <typename F>
+mb_status guard(F&& f)
+{
+	try
+	{
+		g_last_error.clear();
+		f();
+		return MB_OK;
+	}
+	catch (const mb::engine_error& e)
+	{
+		g_last_error = e.what();
+		return e.code;
+	}
+	catch (const mb::model_error& e)
+	{
+		g_last_error = e.what();
+		return MB_ERR_PARSE;
+	}
+	catch (const std::bad_alloc&)
+	{
+		g_last_error = "out of host memory";
+		return MB_ERR_LIMIT;
+	}
+	catch (const std::exception& e)
+	{
+		g_last_error = e.what();
+		return MB_ERR_INTERNAL;
+	}
+	catch (...)
+	{
+		g_last_error = "unknown error";
+		return MB_ERR_INTERNAL;
+	}
+}
+
+void need(bool cond, const char* msg)
+{
+	if (!cond)
+		throw mb::engine_error(MB_ERR_INVALID, msg);
+}
+
+void copy_out(const std::string& s, char* buf, size_t cap, size_t* len)
+{
+	if (len)
+		*len = s.size();
+	if (buf && cap)
+	{
+		size_t n = std::min(cap - 1, s.size());
+		std::memcpy(buf, s.data(), n);
+		buf[n] = '\0';
+	}
+}
+
+cudaStream_t stream_of(mb::context* ctx, void* s) { return s ? (cudaStream_t)s : ctx->stream; }
+
+std::vector<std::string> names_of(const mb::model_t& m)
+{
+	std::vector<std::string> n;
+	for (auto& x : m.nodes)
+		n.push_back(x.name);
+	return n;
+}
+
+} // namespace
+
+extern "C" {
+
+const char* mb_version(void) { return "maboss_b200 0.1 (sm_100a)"; }
+const char* mb_last_error(void) { return g_last_error.c_str(); }
+
+// ------------------------------------------------------------------ models
+
+mb_status mb_model_parse_files(const char* bnd_path, const char* cfg_path, mb_model* out)
+{
+	return guard([&] {
+		need(bnd_path && cfg_path && out, "null argument");
+		auto m = std::make_unique<mb_model_s>();
+		mb::parse_model_files(m->model, bnd_path, cfg_path);
+		*out = m.release();
+	});
+}
+
+mb_status mb_model_parse_text(const char* bnd_text, const char* cfg_text, mb_model* out)
+{
+	return guard([&] {
+		need(bnd_text && cfg_text && out, "null argument");
+		auto m = std::make_unique<mb_model_s>();
+		mb::parse_bnd(m->model, bnd_text, "<bnd>");
+		mb::parse_cfg(m->model, cfg_text, "<cfg>");
+		*out = m.release();
+	});
+}
+
+mb_status mb_model_free(mb_model m)
+{
+	delete m;
+	return MB_OK;
+}
+
+mb_status mb_model_num_nodes(mb_model m, int* n)
+{
+	return guard([&] {
+		need(m && n, "null argument");
+		*n = (int)m->model.nodes.size();
+	});
+}
+
+mb_status mb_model_node_name(mb_model m, int i, char* buf, size_t cap, size_t* len)
+{
+	return guard([&] {
+		need(m && i >= 0 && i < (int)m->model.nodes.size(), "bad node index");
+		copy_out(m->model.nodes[i].name, buf, cap, len);
+	});
+}
+
+mb_status mb_model_node_info(mb_model m, int i, float* istate, int* is_internal)
+{
+	return guard([&] {
+		need(m && i >= 0 && i < (int)m->model.nodes.size(), "bad node index");
+		if (istate)
+			*istate = m->model.nodes[i].istate;
+		if (is_internal)
+			*is_internal = m->model.is_internal(i) ? 1 : 0;
+	});
+}
+
+mb_status mb_model_set_istate(mb_model m, int i, float istate)
+{
+	return guard([&] {
+		need(m && i >= 0 && i < (int)m->model.nodes.size(), "bad node index");
+		m->model.nodes[i].istate = istate;
+	});
+}
+
+mb_status mb_model_get_constant(mb_model m, const char* name, float* value)
+{
+	return guard([&] {
+		need(m && name && value, "null argument");
+		*value = m->model.constant(name);
+	});
+}
+
+mb_status mb_model_set_constant(mb_model m, const char* name, float value)
+{
+	return guard([&] {
+		need(m && name, "null argument");
+		m->model.constants[name] = value;
+	});
+}
+
+mb_status mb_model_get_variable(mb_model m, const char* name, float* value)
+{
+	return guard([&] {
+		need(m && name && value, "null argument");
+		auto it = m->model.variables.find(name);
+		if (it == m->model.variables.end())
+			throw mb::engine_error(MB_ERR_INVALID, std::string("unknown variable ") + name);
+		*value = it->second;
+	});
+}
+
+mb_status mb_model_set_variable(mb_model m, const char* name, float value)
+{
+	return guard([&] {
+		need(m && name && name[0] == '$', "variable names start with '$'");
+		m->model.variables[name] = value;
+	});
+}
+
+mb_status mb_model_num_variables(mb_model m, int* n)
+{
+	return guard([&] {
+		need(m && n, "null argument");
+		*n = (int)m->model.variables.size();
+	});
+}
+
+mb_status mb_model_variable_name(mb_model m, int i, char* buf, size_t cap, size_t* len)
+{
+	return guard([&] {
+		need(m && i >= 0 && i < (int)m->model.variables.size(), "bad variable index");
+		auto it = m->model.variables.begin();
+		std::advance(it, i);
+		copy_out(it->first, buf, cap, len);
+	});
+}
+
+mb_status mb_model_generate_code(mb_model m, char* buf, size_t cap, size_t* len)
+{
+	return guard([&] {
+		need(m, "null model");
+		copy_out(mb::generate_code(m->model), buf, cap, len);
+	});
+}
+
+// ------------------------------------------------------------------ context / modules
+
+mb_status mb_context_create(int device, mb_context* out)
+{
+	return guard([&] {
+		need(out, "null argument");
+		auto c = std::make_unique<mb_context_s>();
+		c->ctx = std::make_unique<mb::context>(device);
+		*out = c.release();
+	});
+}
+
+mb_status mb_context_free(mb_context c)
+{
+	delete c;
+	return MB_OK;
+}
+
+mb_status mb_context_stream(mb_context c, void** stream)
+{
+	return guard([&] {
+		need(c && stream, "null argument");
+		*stream = (void*)c->ctx->stream;
+	});
+}
+
+mb_status mb_context_sm_count(mb_context c, int* sm_count)
+{
+	return guard([&] {
+		need(c && sm_count, "null argument");
+		*sm_count = c->ctx->sm_count;
+	});
+}
+
+mb_status mb_module_compile(mb_context c, const char* code, mb_module* out)
+{
+	return guard([&] {
+		need(c && code && out, "null argument");
+		auto m = std::make_unique<mb_module_s>();
+		m->mod = mb::compile_module(*c->ctx, code);
+		*out = m.release();
+	});
+}
+
+mb_status mb_module_compile_model(mb_context c, mb_model model, mb_module* out)
+{
+	return guard([&] {
+		need(c && model && out, "null argument");
+		auto m = std::make_unique<mb_module_s>();
+		mb::model_layout L = mb::analyze_model(model->model);
+		m->mod = mb::compile_module(*c->ctx, mb::generate_code(model->model));
+		m->mod->layout = std::move(L);
+		m->mod->has_layout = true;
+		*out = m.release();
+	});
+}
+
+mb_status mb_jit_check(const char* generated_code, size_t* cubin_size, char* log, size_t cap)
+{
+	return guard([&] {
+		need(generated_code, "null code");
+		std::string lg;
+		auto cubin = mb::compile_cubin(generated_code, lg);
+		if (cubin_size)
+			*cubin_size = cubin.size();
+		copy_out(lg, log, cap, nullptr);
+	});
+}
+
+mb_status mb_module_free(mb_module mod)
+{
+	delete mod;
+	return MB_OK;
+}
+
+mb_status mb_module_state_size(mb_module mod, int* state_size, int* state_words)
+{
+	return guard([&] {
+		need(mod, "null module");
+		if (state_size)
+			*state_size = mod->mod->state_size;
+		if (state_words)
+			*state_words = mod->mod->state_words;
+	});
+}
+
+mb_status mb_module_log(mb_module mod, char* buf, size_t cap, size_t* len)
+{
+	return guard([&] {
+		need(mod, "null module");
+		copy_out(mod->mod->log, buf, cap, len);
+	});
+}
+
+// ------------------------------------------------------------------ kernel entry points
+
+size_t mb_rand_state_size(void) { return sizeof(curandState); }
+
+mb_status mb_launch_initialize_random(mb_module mod, void* stream, int n, unsigned long long seed,
+									  unsigned long long first, void* rands)
+{
+	return guard([&] {
+		need(mod && n >= 0 && (rands || n == 0), "bad argument");
+		if (n == 0)
+			return;
+		mb::module& m = *mod->mod;
+		MB_CUDA(cudaSetDevice(m.ctx->device));
+		void* a[] = { &n, &seed, &first, &rands };
+		mb::launch(m.init_random, (n + 255) / 256, 256, 0, stream_of(m.ctx, stream), a);
+	});
+}
+
+mb_status mb_launch_initialize_initial_state(mb_module mod, void* stream, int n, int stride,
+											 const float* initial_probs, uint32_t* last_states, float* last_times,
+											 void* rands)
+{
+	return guard([&] {
+		need(mod && n >= 0 && stride >= n, "bad argument");
+		if (n == 0)
+			return;
+		need(initial_probs && last_states && last_times && rands, "null buffer");
+		mb::module& m = *mod->mod;
+		MB_CUDA(cudaSetDevice(m.ctx->device));
+		void* a[] = { &n, &stride, &initial_probs, &last_states, &last_times, &rands };
+		mb::launch(m.init_state, (n + 255) / 256, 256, 0, stream_of(m.ctx, stream), a);
+	});
+}
+
+mb_status mb_launch_simulate(mb_module mod, void* stream, int n, int stride, int traj_len, uint32_t* last_states,
+							 float* last_times, void* rands, uint32_t* traj_states, float* traj_times,
+							 float* traj_entropies, uint8_t* statuses, unsigned long long* transitions)
+{
+	return guard([&] {
+		need(mod && n >= 0 && stride >= n && traj_len >= 2, "bad argument");
+		if (n == 0)
+			return;
+		need(last_states && last_times && rands && traj_states && traj_times && traj_entropies && statuses &&
+				 transitions,
+			 "null buffer");
+		mb::module& m = *mod->mod;
+		MB_CUDA(cudaSetDevice(m.ctx->device));
+		void* a[] = { &n,		   &stride,		 &traj_len,		  &last_states, &last_times,  &rands,
+					  &traj_states, &traj_times, &traj_entropies, &statuses,	&transitions };
+		mb::launch(m.sim_epoch, (n + 255) / 256, 256, 0, stream_of(m.ctx, stream), a);
+	});
+}
+
+mb_status mb_stats_create(mb_module mod, float time_tick, float max_time, int discrete_time,
+						  const int* noninternal_nodes, int n_noninternal, long long sample_count, mb_stats* out)
+{
+	return guard([&] {
+		need(mod && out && n_noninternal >= 0 && (noninternal_nodes || n_noninternal == 0), "bad argument");
+		mb::module& m = *mod->mod;
+		MB_CUDA(cudaSetDevice(m.ctx->device));
+		auto s = std::make_unique<mb_stats_s>();
+		std::vector<int> ni(noninternal_nodes, noninternal_nodes + n_noninternal);
+		s->st.init(m, time_tick, max_time, discrete_time != 0, ni, sample_count, 0, m.ctx->stream);
+		MB_CUDA(cudaStreamSynchronize(m.ctx->stream));
+		*out = s.release();
+	});
+}
+
+mb_status mb_stats_free(mb_stats st)
+{
+	delete st;
+	return MB_OK;
+}
+
+mb_status mb_launch_window_average_stats(mb_stats st, void* stream, int n, int stride, int traj_len,
+										 const uint32_t* traj_states, const float* traj_times,
+										 const float* traj_entropies)
+{
+	return guard([&] {
+		need(st && n >= 0 && stride >= n && traj_len >= 2, "bad argument");
+		if (n == 0)
+			return;
+		need(traj_states && traj_times && traj_entropies, "null buffer");
+		MB_CUDA(cudaSetDevice(st->st.mod->ctx->device));
+		st->st.window_batch(stream_of(st->st.mod->ctx, stream), n, stride, traj_len, traj_states, traj_times,
+							traj_entropies);
+	});
+}
+
+mb_status mb_launch_final_states_stats(mb_stats st, void* stream, int n, int stride, const uint32_t* last_states,
+									   const uint8_t* statuses)
+{
+	return guard([&] {
+		need(st && n >= 0 && stride >= n, "bad argument");
+		if (n == 0)
+			return;
+		need(last_states && statuses, "null buffer");
+		MB_CUDA(cudaSetDevice(st->st.mod->ctx->device));
+		st->st.final_batch(stream_of(st->st.mod->ctx, stream), n, stride, last_states, statuses);
+	});
+}
+
+mb_status mb_launch_fixed_states_stats(mb_stats st, void* stream, int n, int stride, const uint32_t* last_states,
+									   const uint8_t* statuses)
+{
+	return guard([&] {
+		need(st && n >= 0 && stride >= n, "bad argument");
+		if (n == 0)
+			return;
+		need(last_states && statuses, "null buffer");
+		MB_CUDA(cudaSetDevice(st->st.mod->ctx->device));
+		st->st.fixed_batch(stream_of(st->st.mod->ctx, stream), n, stride, last_states, statuses);
+	});
+}
+
+mb_status mb_stats_finalize(mb_stats st, long long n_trajectories, mb_result* out)
+{
+	return guard([&] {
+		need(st && out, "null argument");
+		MB_CUDA(cudaSetDevice(st->st.mod->ctx->device));
+		MB_CUDA(cudaDeviceSynchronize());
+		auto r = std::make_unique<mb_result_s>();
+		r->res = st->st.finalize(n_trajectories, st->st.mod->ctx->stream);
+		*out = r.release();
+	});
+}
+
+// ------------------------------------------------------------------ whole runs
+
+mb_status mb_run_config_default(mb_model m, mb_run_config* cfg)
+{
+	return guard([&] {
+		need(m && cfg, "null argument");
+		mb_run_config c{};
+		c.mode = MB_MODE_FUSED_EXACT;
+		c.sample_count = (long long)m->model.constant("sample_count");
+		c.seed = (unsigned long long)m->model.constant("seed_pseudorandom");
+		c.first_traj = 0;
+		c.traj_len = 100;
+		c.batch_limit = 1000000;
+		c.block = 256;
+		c.blocks_per_sm = 0;
+		c.fixed_capacity_log2 = 0;
+		*cfg = c;
+	});
+}
+
+namespace {
+mb::run_config to_config(mb_module mod, const mb_run_config* cfg)
+{
+	need(mod->mod->has_layout, "whole runs need a module from mb_module_compile_model");
+	mb::run_config c = mb::config_from_layout(mod->mod->layout, cfg->mode);
+	c.sample_count = cfg->sample_count;
+	c.seed = cfg->seed;
+	c.first_traj = cfg->first_traj;
+	c.traj_len = cfg->traj_len > 0 ? cfg->traj_len : 100;
+	c.batch_limit = cfg->batch_limit > 0 ? cfg->batch_limit : 1000000;
+	c.block = cfg->block > 0 ? cfg->block : 256;
+	c.blocks_per_sm = cfg->blocks_per_sm;
+	c.fixed_capacity_log2 = cfg->fixed_capacity_log2;
+	return c;
+}
+} // namespace
+
+mb_status mb_runner_create(mb_module mod, const mb_run_config* cfg, mb_runner* out)
+{
+	return guard([&] {
+		need(mod && cfg && out, "null argument");
+		auto r = std::make_unique<mb_runner_s>();
+		r->rn = std::make_unique<mb::runner>(*mod->mod, to_config(mod, cfg));
+		*out = r.release();
+	});
+}
+
+mb_status mb_runner_launch(mb_runner r, void* stream)
+{
+	return guard([&] {
+		need(r, "null runner");
+		r->rn->launch(stream_of(r->rn->mod->ctx, stream));
+	});
+}
+
+mb_status mb_runner_result(mb_runner r, void* stream, mb_result* out)
+{
+	return guard([&] {
+		need(r && out, "null argument");
+		auto res = std::make_unique<mb_result_s>();
+		res->res = r->rn->collect(stream_of(r->rn->mod->ctx, stream));
+		*out = res.release();
+	});
+}
+
+mb_status mb_runner_kernel_launches(mb_runner r, unsigned* n)
+{
+	return guard([&] {
+		need(r && n, "null argument");
+		*n = r->rn->kernel_launches();
+	});
+}
+
+mb_status mb_runner_free(mb_runner r)
+{
+	delete r;
+	return MB_OK;
+}
+
+mb_status mb_run(mb_module mod, const mb_run_config* cfg, mb_result* out)
+{
+	return guard([&] {
+		need(mod && cfg && out, "null argument");
+		mb::run_config c = to_config(mod, cfg);
+		auto r = std::make_unique<mb_result_s>();
+		r->res = mb::run(*mod->mod, c);
+		*out = r.release();
+	});
+}
+
+// ------------------------------------------------------------------ results
+
+mb_status mb_result_free(mb_result r)
+{
+	delete r;
+	return MB_OK;
+}
+
+mb_status mb_result_dims(mb_result r, int* windows, int* bins, int* noninternal, int* state_words, int* nodes)
+{
+	return guard([&] {
+		need(r, "null result");
+		const mb::result& x = *r->res;
+		if (windows)
+			*windows = x.n_windows;
+		if (bins)
+			*bins = (int)x.n_bins;
+		if (noninternal)
+			*noninternal = (int)x.noninternal_nodes.size();
+		if (state_words)
+			*state_words = x.state_words;
+		if (nodes)
+			*nodes = x.state_size;
+	});
+}
+
+mb_status mb_result_transitions(mb_result r, unsigned long long* t)
+{
+	return guard([&] {
+		need(r && t, "null argument");
+		*t = r->res->transitions;
+	});
+}
+
+mb_status mb_result_timing(mb_result r, float* kernel_ms, float* total_ms, int* epochs)
+{
+	return guard([&] {
+		need(r, "null result");
+		if (kernel_ms)
+			*kernel_ms = r->res->kernel_ms;
+		if (total_ms)
+			*total_ms = r->res->total_ms;
+		if (epochs)
+			*epochs = r->res->epochs;
+	});
+}
+
+mb_status mb_result_window_probs(mb_result r, double* probs)
+{
+	return guard([&] {
+		need(r && probs, "null argument");
+		const mb::result& x = *r->res;
+		for (int w = 0; w < x.n_windows; w++)
+			for (unsigned b = 0; b < x.n_bins; b++)
+				probs[(size_t)w * x.n_bins + b] = x.n_traj > 0 ? x.window_prob(w, b) : 0.0;
+	});
+}
+
+mb_status mb_result_window_entropy(mb_result r, double* th)
+{
+	return guard([&] {
+		need(r && th, "null argument");
+		const mb::result& x = *r->res;
+		for (int w = 0; w < x.n_windows; w++)
+			th[w] = x.n_traj > 0 ? x.window_th(w) : 0.0;
+	});
+}
+
+mb_status mb_result_window_raw(mb_result r, long long* occupancy, unsigned* counts, long long* entropy, int* occ_exp,
+							   int* ent_exp)
+{
+	return guard([&] {
+		need(r, "null result");
+		const mb::result& x = *r->res;
+		if (occupancy && !x.win_occ.empty())
+			std::memcpy(occupancy, x.win_occ.data(), x.win_occ.size() * sizeof(long long));
+		if (counts && !x.win_cnt.empty())
+			std::memcpy(counts, x.win_cnt.data(), x.win_cnt.size() * sizeof(unsigned));
+		if (entropy && !x.win_h.empty())
+			std::memcpy(entropy, x.win_h.data(), x.win_h.size() * sizeof(long long));
+		if (occ_exp)
+			*occ_exp = (int)std::lround(std::log2(x.fx));
+		if (ent_exp)
+			*ent_exp = (int)std::lround(std::log2(x.fx_h));
+	});
+}
+
+mb_status mb_result_final_counts(mb_result r, unsigned* counts)
+{
+	return guard([&] {
+		need(r && counts, "null argument");
+		std::memcpy(counts, r->res->final_cnt.data(), r->res->final_cnt.size() * sizeof(unsigned));
+	});
+}
+
+mb_status mb_result_num_fixed(mb_result r, int* n, unsigned* overflow)
+{
+	return guard([&] {
+		need(r, "null result");
+		if (n)
+			*n = (int)r->res->fixed_counts.size();
+		if (overflow)
+			*overflow = r->res->fixed_overflow;
+	});
+}
+
+mb_status mb_result_fixed(mb_result r, int i, uint32_t* state_words, unsigned* count)
+{
+	return guard([&] {
+		need(r && i >= 0 && i < (int)r->res->fixed_counts.size(), "bad fixed-point index");
+		const mb::result& x = *r->res;
+		if (state_words)
+			std::memcpy(state_words, x.fixed_states.data() + (size_t)i * x.state_words, x.state_words * sizeof(uint32_t));
+		if (count)
+			*count = x.fixed_counts[i];
+	});
+}
+
+mb_status mb_result_write_csv(mb_result r, mb_model m, const char* prefix)
+{
+	return guard([&] {
+		need(r && m && prefix, "null argument");
+		need((int)m->model.nodes.size() == r->res->state_size, "model does not match the result");
+		const auto names = names_of(m->model);
+		{
+			std::ofstream f(std::string(prefix) + "_probtraj.csv");
+			if (!f)
+				throw mb::engine_error(MB_ERR_INVALID, std::string("cannot write ") + prefix + "_probtraj.csv");
+			f << mb::format_probtraj_csv(*r->res, names);
+		}
+		{
+			std::ofstream f(std::string(prefix) + "_fp.csv");
+			if (!f)
+				throw mb::engine_error(MB_ERR_INVALID, std::string("cannot write ") + prefix + "_fp.csv");
+			f << mb::format_fp_csv(*r->res, names);
+		}
+	});
+}
+
+mb_status mb_result_visualize(mb_result r, mb_model m, char* buf, size_t cap, size_t* len)
+{
+	return guard([&] {
+		need(r && m, "null argument");
+		need((int)m->model.nodes.size() == r->res->state_size, "model does not match the result");
+		copy_out(mb::format_visualize(*r->res, names_of(m->model)), buf, cap, len);
+	});
+}
+
+} // extern "C"

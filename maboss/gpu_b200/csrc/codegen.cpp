@@ -1,0 +1,549 @@
+// Model -> CUDA source. See codegen.h.
+#include "codegen.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <set>
+#include <sstream>
+
+namespace mb {
+
+namespace {
+
+// Value of a printed literal as the CUDA compiler sees it: the text decides int vs
+// double, and the value is the text parsed back.
+struct cval
+{
+	bool is_double = false;
+	double d = 0;
+	long long i = 0;
+	double as_double() const { return is_double ? d : (double)i; }
+	bool truthy() const { return is_double ? d != 0 : i != 0; }
+};
+
+cval literal_cval(float v)
+{
+	std::string s = print_float(v);
+	cval r;
+	if (s.find_first_of(".eEnNiI") != std::string::npos)
+	{
+		r.is_double = true;
+		r.d = std::strtod(s.c_str(), nullptr);
+	}
+	else
+		r.i = std::strtoll(s.c_str(), nullptr, 10);
+	return r;
+}
+
+struct not_evaluable : std::runtime_error
+{
+	not_evaluable() : std::runtime_error("not evaluable") {}
+};
+
+// Evaluate an emitted expression with C++ typing rules for a given node-state assignment.
+// `bit(i)` returns the value of node i. Throws not_evaluable for forms whose emitted code
+// would not compile (bitwise ops on doubles) or has undefined behaviour (int division by 0).
+template <typename BitFn>
+cval eval_c(const model_t& m, const expr& e, const std::string& current, BitFn&& bit)
+{
+	using K = expr::kind_t;
+	switch (e.kind)
+	{
+		case K::literal: return literal_cval(e.value);
+		case K::variable: return literal_cval(m.variables.at(e.name));
+		case K::identifier:
+		{
+			int i = m.node_index(e.name);
+			if (i < 0)
+				throw model_error("unknown node name: " + e.name);
+			cval r;
+			r.i = bit(i) ? 1 : 0;
+			return r;
+		}
+		case K::alias:
+		{
+			int i = m.node_index(current);
+			return eval_c(m, m.nodes[i].get_attr(e.name.substr(1)), current, bit);
+		}
+		case K::paren: return eval_c(m, *e.a, current, bit);
+		case K::ternary:
+		{
+			cval c = eval_c(m, *e.a, current, bit);
+			cval x = eval_c(m, *e.b, current, bit);
+			cval y = eval_c(m, *e.c, current, bit);
+			cval r = c.truthy() ? x : y;
+			if (x.is_double || y.is_double)
+			{
+				r.d = r.as_double();
+				r.is_double = true;
+			}
+			return r;
+		}
+		case K::unary:
+		{
+			cval v = eval_c(m, *e.a, current, bit);
+			cval r = v;
+			if (e.op == op_t::MINUS)
+			{
+				r.d = -v.d;
+				r.i = -v.i;
+			}
+			else if (e.op == op_t::NOT)
+			{
+				r.is_double = false;
+				r.i = v.truthy() ? 0 : 1;
+			}
+			return r;
+		}
+		case K::binary:
+		{
+			cval a = eval_c(m, *e.a, current, bit);
+			cval b = eval_c(m, *e.b, current, bit);
+			cval r;
+			const bool dbl = a.is_double || b.is_double;
+			switch (e.op)
+			{
+				case op_t::PLUS:
+				case op_t::MINUS:
+				case op_t::STAR:
+				case op_t::SLASH:
+					if (dbl)
+					{
+						r.is_double = true;
+						double x = a.as_double(), y = b.as_double();
+						r.d = e.op == op_t::PLUS ? x + y : e.op == op_t::MINUS ? x - y : e.op == op_t::STAR ? x * y : x / y;
+					}
+					else
+					{
+						if (e.op == op_t::SLASH && b.i == 0)
+							throw not_evaluable();
+						r.i = e.op == op_t::PLUS ? a.i + b.i
+							  : e.op == op_t::MINUS ? a.i - b.i
+							  : e.op == op_t::STAR ? a.i * b.i
+												   : a.i / b.i;
+					}
+					return r;
+				case op_t::AND:
+				case op_t::OR:
+				case op_t::XOR:
+					if (dbl)
+						throw not_evaluable();
+					r.i = e.op == op_t::AND ? (a.i & b.i) : e.op == op_t::OR ? (a.i | b.i) : (a.i ^ b.i);
+					return r;
+				default:
+				{
+					double x = a.as_double(), y = b.as_double();
+					bool v = false;
+					if (!dbl)
+					{
+						long long p = a.i, q = b.i;
+						v = e.op == op_t::EQ ? p == q : e.op == op_t::NE ? p != q : e.op == op_t::LE ? p <= q
+							: e.op == op_t::LT ? p < q : e.op == op_t::GE ? p >= q : p > q;
+					}
+					else
+						v = e.op == op_t::EQ ? x == y : e.op == op_t::NE ? x != y : e.op == op_t::LE ? x <= y
+							: e.op == op_t::LT ? x < y : e.op == op_t::GE ? x >= y : x > y;
+					r.i = v ? 1 : 0;
+					return r;
+				}
+			}
+		}
+	}
+	throw not_evaluable();
+}
+
+void collect_nodes(const model_t& m, const expr& e, const std::string& current, std::set<int>& out, int depth = 0)
+{
+	using K = expr::kind_t;
+	if (depth > 64)
+		throw model_error("alias recursion too deep in node " + current);
+	switch (e.kind)
+	{
+		case K::identifier:
+		{
+			int i = m.node_index(e.name);
+			if (i < 0)
+				throw model_error("unknown node name: " + e.name);
+			out.insert(i);
+			return;
+		}
+		case K::alias:
+		{
+			int i = m.node_index(current);
+			collect_nodes(m, m.nodes[i].get_attr(e.name.substr(1)), current, out, depth + 1);
+			return;
+		}
+		default:
+			if (e.a)
+				collect_nodes(m, *e.a, current, out, depth);
+			if (e.b)
+				collect_nodes(m, *e.b, current, out, depth);
+			if (e.c)
+				collect_nodes(m, *e.c, current, out, depth);
+	}
+}
+
+// generator.cpp:57-82 (is_logic_ternary_expression). The reference evaluates the branches
+// unconditionally and aborts on non-constant ones; here such nodes use the general form.
+bool is_logic_ternary(const model_t& m, const expr* e, bool up, float& val)
+{
+	if (!e || e->kind != expr::kind_t::ternary)
+		return false;
+	if (e->a->kind != expr::kind_t::alias || e->a->name != "@logic")
+		return false;
+	if (!is_constant_expr(m, *e->b) || !is_constant_expr(m, *e->c))
+		return false;
+	float l = evaluate(m, *e->b), r = evaluate(m, *e->c);
+	float zero = up ? r : l;
+	val = up ? l : r;
+	return zero == 0.f;
+}
+
+float compiled_literal(float v) { return (float)literal_cval(v).as_double(); }
+
+std::string flit(float v)
+{
+	// exact float literal for engine-side constants
+	char buf[64];
+	std::snprintf(buf, sizeof buf, "%.9gf", v);
+	std::string s = buf;
+	if (s.find_first_of(".eEn") == std::string::npos)
+		s.insert(s.size() - 1, ".0");
+	return s;
+}
+
+std::string ident(const std::string& node_name) { return node_name; }
+
+void emit_bit(std::ostream& os, int i) { os << "((state[" << i / 32 << "] & " << (1u << (i % 32)) << "u) != 0)"; }
+
+} // namespace
+
+int model_layout::windows() const
+{
+	// window_average_small.cpp:305: std::ceil(max_time / window_size) with float operands
+	float q = max_time / time_tick;
+	return (int)std::ceil(q);
+}
+
+model_layout analyze_model(const model_t& m)
+{
+	model_layout L;
+	const int N = (int)m.nodes.size();
+	L.state_size = N;
+	L.state_words = (N + 31) / 32;
+	L.discrete_time = m.constant("discrete_time") != 0;
+	L.max_time = m.constant("max_time");
+	L.time_tick = m.constant("time_tick");
+	L.sample_count = (int)m.constant("sample_count");
+	L.seed = (unsigned long long)m.constant("seed_pseudorandom");
+	std::set<int> ni_words;
+	for (int i = 0; i < N; i++)
+	{
+		L.names.push_back(m.nodes[i].name);
+		L.istate.push_back(m.nodes[i].istate);
+		if (!m.is_internal(i))
+		{
+			L.noninternal_nodes.push_back(i);
+			ni_words.insert(i / 32);
+		}
+	}
+	L.noninternal_words = (int)ni_words.size();
+
+	L.fast_path.assign(N, 0);
+	L.up.assign(N, 0.f);
+	L.down.assign(N, 0.f);
+	L.all_fast_path = N > 0;
+	L.rates_nonnegative = true;
+	for (int i = 0; i < N; i++)
+	{
+		const node_t& node = m.nodes[i];
+		float u = 0, d = 0;
+		bool fp = is_logic_ternary(m, node.find_attr("rate_up"), true, u)
+				  && is_logic_ternary(m, node.find_attr("rate_down"), false, d) && node.find_attr("logic");
+		L.fast_path[i] = fp;
+		if (fp)
+		{
+			L.up[i] = compiled_literal(u);
+			L.down[i] = compiled_literal(d);
+			if (!(L.up[i] >= 0.f) || !(L.down[i] >= 0.f))
+				L.rates_nonnegative = false;
+		}
+		else
+		{
+			L.all_fast_path = false;
+			L.rates_nonnegative = false;
+		}
+	}
+
+	// incremental tables (fast-path models with small logic fan-in only)
+	L.incremental_ok = L.all_fast_path;
+	constexpr int max_inputs = 12;
+	if (L.incremental_ok)
+	{
+		std::vector<std::set<int>> inputs(N);
+		for (int i = 0; i < N && L.incremental_ok; i++)
+		{
+			collect_nodes(m, m.nodes[i].get_attr("logic"), m.nodes[i].name, inputs[i]);
+			if ((int)inputs[i].size() > max_inputs)
+				L.incremental_ok = false;
+		}
+		if (L.incremental_ok)
+		{
+			L.in_ptr.push_back(0);
+			L.tt_ptr.push_back(0);
+			std::vector<std::vector<int>> deps(N);
+			for (int i = 0; i < N; i++)
+				deps[i].push_back(i);
+			for (int i = 0; i < N && L.incremental_ok; i++)
+			{
+				std::vector<int> in(inputs[i].begin(), inputs[i].end());
+				for (int j : in)
+				{
+					L.in_idx.push_back(j);
+					if (j != i)
+						deps[j].push_back(i);
+				}
+				L.in_ptr.push_back((int)L.in_idx.size());
+				const int mi = (int)in.size();
+				const int patterns = 1 << mi;
+				const int words = (patterns + 31) / 32;
+				std::vector<unsigned> tt(words, 0u);
+				try
+				{
+					for (int p = 0; p < patterns; p++)
+					{
+						auto bit = [&](int node) {
+							auto it = std::find(in.begin(), in.end(), node);
+							return ((p >> (it - in.begin())) & 1) != 0;
+						};
+						cval v = eval_c(m, m.nodes[i].get_attr("logic"), m.nodes[i].name, bit);
+						if (v.truthy())
+							tt[p / 32] |= 1u << (p % 32);
+					}
+				}
+				catch (const not_evaluable&)
+				{
+					L.incremental_ok = false;
+				}
+				L.tt_words.insert(L.tt_words.end(), tt.begin(), tt.end());
+				L.tt_ptr.push_back((int)L.tt_words.size());
+			}
+			L.dep_ptr.push_back(0);
+			for (int j = 0; j < N; j++)
+			{
+				std::sort(deps[j].begin(), deps[j].end());
+				deps[j].erase(std::unique(deps[j].begin(), deps[j].end()), deps[j].end());
+				L.dep_idx.insert(L.dep_idx.end(), deps[j].begin(), deps[j].end());
+				L.dep_ptr.push_back((int)L.dep_idx.size());
+			}
+		}
+		if (!L.incremental_ok)
+		{
+			L.in_ptr.clear();
+			L.in_idx.clear();
+			L.tt_ptr.clear();
+			L.tt_words.clear();
+			L.dep_ptr.clear();
+			L.dep_idx.clear();
+		}
+	}
+	return L;
+}
+
+std::string generate_code(const model_t& m)
+{
+	const model_layout L = analyze_model(m);
+	const int N = L.state_size;
+	std::ostringstream ss;
+
+	// ---- reference-form prologue (generator.cpp:17-29)
+	ss << "using uint8_t = unsigned char;" << std::endl;
+	ss << "using uint32_t = unsigned int;" << std::endl << std::endl;
+	ss << "constexpr int state_size = " << N << ";" << std::endl;
+	ss << "constexpr int state_words = " << L.state_words << ";" << std::endl;
+	ss << "constexpr bool discrete_time = " << (L.discrete_time ? 1 : 0) << ";" << std::endl;
+	ss << "constexpr float max_time = " << print_float(m.constant("max_time")) << ";" << std::endl;
+	ss << "constexpr float time_tick = " << print_float(m.constant("time_tick")) << ";" << std::endl;
+	ss << "using state_word_t = uint32_t;" << std::endl << std::endl;
+
+	// ---- per-node rate functions (generator.cpp:84-122)
+	for (int i = 0; i < N; i++)
+	{
+		const node_t& node = m.nodes[i];
+		ss << "__device__ float " << ident(node.name) << "_rate(const state_word_t* __restrict__ state) " << std::endl;
+		ss << "{" << std::endl;
+		if (L.fast_path[i])
+		{
+			float up_val = 0, down_val = 0;
+			is_logic_ternary(m, node.find_attr("rate_up"), true, up_val);
+			is_logic_ternary(m, node.find_attr("rate_down"), false, down_val);
+			ss << "    const bool is_up = ";
+			emit_bit(ss, i);
+			ss << ";" << std::endl;
+			ss << "    const bool logic = ";
+			emit_code(m, node.get_attr("logic"), node.name, ss);
+			ss << ";" << std::endl;
+			if (up_val == down_val)
+				ss << "    return is_up == logic ? 0 : " << print_float(up_val) << ";" << std::endl;
+			else
+				ss << "    return is_up == logic ? 0 : (is_up ? " << print_float(down_val) << " : "
+				   << print_float(up_val) << ");" << std::endl;
+		}
+		else
+		{
+			ss << "    return ";
+			emit_bit(ss, i);
+			ss << " ?" << std::endl;
+			ss << "          (";
+			emit_code(m, node.get_attr("rate_down"), node.name, ss);
+			ss << ")" << std::endl;
+			ss << "        : (";
+			emit_code(m, node.get_attr("rate_up"), node.name, ss);
+			ss << ");" << std::endl;
+		}
+		ss << "}" << std::endl << std::endl;
+	}
+
+	// ---- compute_transition_rates (generator.cpp:124-144)
+	ss << "__device__ float compute_transition_rates(float* __restrict__ transition_rates, const state_word_t* "
+		  "__restrict__ state)"
+	   << std::endl;
+	ss << "{" << std::endl << "    float sum = 0;" << std::endl << "    float tmp;" << std::endl << std::endl;
+	for (int i = 0; i < N; i++)
+	{
+		ss << "    tmp = " << ident(m.nodes[i].name) << "_rate(state);" << std::endl;
+		ss << "    transition_rates[" << i << "] = tmp;" << std::endl;
+		ss << "    sum += tmp;" << std::endl << std::endl;
+	}
+	ss << "    return sum;" << std::endl << "}" << std::endl << std::endl;
+
+	// ---- compute_transition_entropy (generator.cpp:146-175)
+	ss << "__device__ float compute_transition_entropy(const float* __restrict__ transition_rates)" << std::endl;
+	ss << "{" << std::endl;
+	ss << "    float entropy = 0.f;" << std::endl;
+	ss << "    float non_internal_total_rate = 0.f;" << std::endl;
+	ss << "    float tmp_prob;" << std::endl << std::endl;
+	for (int i : L.noninternal_nodes)
+		ss << "    non_internal_total_rate += transition_rates[" << i << "];" << std::endl;
+	ss << "    if (non_internal_total_rate == 0.f) return 0.f;" << std::endl << std::endl;
+	for (int i : L.noninternal_nodes)
+	{
+		ss << "    tmp_prob = transition_rates[" << i << "] / non_internal_total_rate;" << std::endl;
+		ss << "    entropy -= (tmp_prob == 0.f) ? 0.f : log2f(tmp_prob) * tmp_prob;" << std::endl;
+	}
+	ss << "    return entropy;" << std::endl << "}" << std::endl << std::endl;
+
+	// ---- get_non_internal_index (generator.cpp:207-235)
+	ss << "__device__ uint32_t get_non_internal_index(const state_word_t* __restrict__ state)" << std::endl;
+	ss << "{" << std::endl;
+	if (L.noninternal_nodes.empty() || L.noninternal_nodes.size() > 32)
+		ss << "    return 0u;" << std::endl;
+	else
+	{
+		ss << "    return" << std::endl << "\t\t\t";
+		int k = 0;
+		const int kc = (int)L.noninternal_nodes.size();
+		for (int i : L.noninternal_nodes)
+		{
+			ss << "((state[" << i / 32 << "] & " << (1u << (i % 32)) << "u)";
+			int shift = (i % 32) - k++;
+			if (shift > 0)
+				ss << " >> " << shift;
+			else if (shift < 0)
+				ss << " << " << -shift;
+			ss << ")";
+			if (k != kc)
+				ss << " | ";
+		}
+		ss << ";" << std::endl;
+	}
+	ss << "}" << std::endl << std::endl;
+
+	// ---- engine helpers (not part of the reference's generated text)
+	ss << "// ---- B200 engine helpers" << std::endl;
+	ss << "constexpr int mbg_noninternal_count = " << L.noninternal_nodes.size() << ";" << std::endl;
+	ss << "constexpr bool mbg_rates_nonnegative = " << (L.rates_nonnegative ? "true" : "false") << ";" << std::endl;
+	ss << "constexpr bool mbg_all_fast_path = " << (L.all_fast_path ? "true" : "false") << ";" << std::endl;
+	ss << "constexpr bool mbg_incremental = " << (L.incremental_ok ? "true" : "false") << ";" << std::endl
+	   << std::endl;
+
+	// total rate in node order: the same fp32 sum sequence as compute_transition_rates
+	ss << "__device__ __forceinline__ float mbg_total_rate(const state_word_t* __restrict__ state)" << std::endl;
+	ss << "{" << std::endl << "    float sum = 0;" << std::endl;
+	for (int i = 0; i < N; i++)
+		ss << "    sum += " << ident(m.nodes[i].name) << "_rate(state);" << std::endl;
+	ss << "    return sum;" << std::endl << "}" << std::endl << std::endl;
+
+	// flip selection: idx = #{i : prefix_i < r} (simulation.cu:9-21). With non-negative rates
+	// the prefix sums are monotone, so the count equals the first index reaching r.
+	ss << "__device__ __forceinline__ int mbg_select_flip(const state_word_t* __restrict__ state, float r)"
+	   << std::endl;
+	ss << "{" << std::endl << "    float sum = 0;" << std::endl;
+	if (L.rates_nonnegative)
+	{
+		for (int i = 0; i < N; i++)
+			ss << "    sum += " << ident(m.nodes[i].name) << "_rate(state); if (!(sum < r)) return " << i << ";"
+			   << std::endl;
+		ss << "    return " << (N - 1) << ";" << std::endl;
+	}
+	else
+	{
+		ss << "    int idx = 0;" << std::endl;
+		for (int i = 0; i < N; i++)
+			ss << "    sum += " << ident(m.nodes[i].name) << "_rate(state); idx += (sum < r) ? 1 : 0;" << std::endl;
+		ss << "    return idx < " << N << " ? idx : " << (N - 1) << ";" << std::endl;
+	}
+	ss << "}" << std::endl << std::endl;
+
+	// transition entropy with the same arithmetic as compute_transition_entropy
+	ss << "__device__ __forceinline__ float mbg_entropy(const state_word_t* __restrict__ state)" << std::endl;
+	ss << "{" << std::endl;
+	for (int i : L.noninternal_nodes)
+		ss << "    const float r" << i << " = " << ident(m.nodes[i].name) << "_rate(state);" << std::endl;
+	ss << "    float entropy = 0.f;" << std::endl;
+	ss << "    float non_internal_total_rate = 0.f;" << std::endl;
+	ss << "    float tmp_prob;" << std::endl;
+	for (int i : L.noninternal_nodes)
+		ss << "    non_internal_total_rate += r" << i << ";" << std::endl;
+	ss << "    if (non_internal_total_rate == 0.f) return 0.f;" << std::endl;
+	for (int i : L.noninternal_nodes)
+	{
+		ss << "    tmp_prob = r" << i << " / non_internal_total_rate;" << std::endl;
+		ss << "    entropy -= (tmp_prob == 0.f) ? 0.f : log2f(tmp_prob) * tmp_prob;" << std::endl;
+	}
+	ss << "    (void)tmp_prob;" << std::endl;
+	ss << "    return entropy;" << std::endl << "}" << std::endl << std::endl;
+
+	// fast-mode entropy: h = log2(S) - (sum r log2 r) / S with r log2 r folded into constants
+	ss << "__device__ __forceinline__ float mbg_entropy_fast(const state_word_t* __restrict__ state)" << std::endl;
+	ss << "{" << std::endl << "    float t = 0.f, tl = 0.f;" << std::endl;
+	for (int i : L.noninternal_nodes)
+	{
+		if (L.fast_path[i])
+		{
+			const double u = L.up[i], d = L.down[i];
+			const float ul = u > 0 ? (float)(u * std::log2(u)) : 0.f;
+			const float dl = d > 0 ? (float)(d * std::log2(d)) : 0.f;
+			ss << "    { const bool up = ";
+			emit_bit(ss, i);
+			ss << "; const bool lg = ";
+			emit_code(m, m.nodes[i].get_attr("logic"), m.nodes[i].name, ss);
+			ss << "; if (up != lg) { t += up ? " << flit(L.down[i]) << " : " << flit(L.up[i]) << "; tl += up ? "
+			   << flit(dl) << " : " << flit(ul) << "; } }" << std::endl;
+		}
+		else
+		{
+			ss << "    { const float r = " << ident(m.nodes[i].name)
+			   << "_rate(state); t += r; tl += (r > 0.f) ? r * log2f(r) : 0.f; }" << std::endl;
+		}
+	}
+	ss << "    if (!(t > 0.f)) return 0.f;" << std::endl;
+	ss << "    const float h = log2f(t) - tl / t;" << std::endl;
+	ss << "    return h > 0.f ? h : 0.f;" << std::endl << "}" << std::endl;
+
+	return ss.str();
+}
+
+} // namespace mb

@@ -1,0 +1,57 @@
+// Code generator: model -> CUDA source compiled by NVRTC together with the engine kernels.
+//
+// The emitted per-node rate functions, `compute_transition_rates`,
+// `compute_transition_entropy` and `get_non_internal_index` reproduce the text of the
+// reference generator (src/generator.cpp:84-235) so that the compiled rate arithmetic is
+// identical. On top of them it emits straight-line helpers (`mbg_*`) that the engine
+// kernels call instead of materialising a `float rates[N]` array per thread.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "model.h"
+
+namespace mb {
+
+// Static facts about a model that the host runtime needs next to the compiled module.
+struct model_layout
+{
+	int state_size = 0;					// N
+	int state_words = 0;				// W = ceil(N/32)
+	std::vector<int> noninternal_nodes; // node indices in node order
+	int noninternal_words = 0;			// number of distinct state words holding non-internal bits
+	bool discrete_time = false;
+	float max_time = 0.f;  // exact float constant (host side, window statistics)
+	float time_tick = 0.f; // exact float constant (host side, window statistics)
+	int sample_count = 0;
+	unsigned long long seed = 0;
+	std::vector<float> istate;
+	std::vector<std::string> names;
+
+	// Fast-path form `rate_up = @logic ? U : 0; rate_down = @logic ? 0 : D;` for every
+	// node (generator.cpp:57-82). When true, `up`/`down` hold the rate values exactly as
+	// the compiled code sees them (6-significant-digit literals converted to float).
+	bool all_fast_path = false;
+	std::vector<char> fast_path;
+	std::vector<float> up, down;
+	bool rates_nonnegative = false;
+
+	// Incremental engine tables (valid when `incremental_ok`): node -> inputs of its logic
+	// (CSR), the logic truth table over those inputs, and node -> dependents (CSR).
+	bool incremental_ok = false;
+	std::vector<int> in_ptr, in_idx;
+	std::vector<int> tt_ptr;				// offset (in 32-bit words) of each node's truth table
+	std::vector<unsigned> tt_words;			// truth tables, bit b = logic value for input pattern b
+	std::vector<int> dep_ptr, dep_idx;		// nodes whose rate must be re-evaluated after a flip
+
+	int windows() const; // ceil(max_time / time_tick) in float, window_average_small.cpp:305
+};
+
+// Analyse a parsed model (throws model_error on semantic errors such as unknown nodes).
+model_layout analyze_model(const model_t& m);
+
+// The generated CUDA source for a model (model-specific part only).
+std::string generate_code(const model_t& m);
+
+} // namespace mb

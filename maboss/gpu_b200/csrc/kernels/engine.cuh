@@ -1,0 +1,627 @@
+// B200 trajectory engine: hand-written device code, compiled by NVRTC for sm_100a in one
+// translation unit after the generated model code (which defines state_size, state_words,
+// discrete_time, max_time, time_tick, the per-node rate functions, get_non_internal_index
+// and the mbg_* helpers).
+//
+// Two execution shapes share the same per-step semantics (src/jit_kernels/simulation.cu:77-164):
+//  * fused persistent kernel: one thread runs whole trajectories taken from a work counter and
+//    accumulates window occupancy, transition entropy, final states and fixed points in place,
+//    so no trajectory buffer is written;
+//  * buffered epoch kernels: the reference's simulate -> stats -> partition/refill epochs over
+//    SoA buffers [slot][word][trajectory], for the stats-plugin API.
+// Window sums are int64 fixed point (value * 2^e, round to nearest even): integer atomics make
+// every sum independent of thread order, so results are reproducible bit for bit.
+#include <curand_kernel.h>
+
+enum class trajectory_status : uint8_t
+{
+	CONTINUE,
+	FINISHED,
+	FIXED_POINT
+};
+
+// ---------------------------------------------------------------- small helpers
+
+__device__ __forceinline__ void mb_flip(state_word_t* st, int f)
+{
+	const int fw = f >> 5;
+	const uint32_t m = 1u << (f & 31);
+#pragma unroll
+	for (int w = 0; w < state_words; w++)
+		st[w] ^= (w == fw) ? m : 0u;
+}
+
+// Initial state: bit i set iff uniform_i <= istate[i], uniforms drawn in node order
+// (simulation.cu:34-71).
+template <typename RNG>
+__device__ __forceinline__ void mb_init_state(state_word_t* st, RNG& rng, const float* __restrict__ istate)
+{
+#pragma unroll
+	for (int w = 0; w < state_words; w++)
+	{
+		uint32_t s = 0;
+		const int nb = (w == state_words - 1) ? state_size - 32 * w : 32;
+		for (int b = 0; b < nb; b++)
+			if (curand_uniform(&rng) <= __ldg(istate + 32 * w + b))
+				s |= 1u << b;
+		st[w] = s;
+	}
+}
+
+__device__ __forceinline__ unsigned long long mb_mix64(unsigned long long x)
+{
+	x ^= x >> 30;
+	x *= 0xbf58476d1ce4e5b9ull;
+	x ^= x >> 27;
+	x *= 0x94d049bb133111ebull;
+	x ^= x >> 31;
+	return x;
+}
+
+// 128-bit fixed-point key: the state itself when it fits in 96 bits, else two independent
+// 64-bit hashes. The top bit is always set so that 0 marks an empty slot.
+__device__ __forceinline__ mb_key128 mb_state_key(const state_word_t* st)
+{
+	mb_key128 k;
+	if (state_words <= 3)
+	{
+		k.lo = (unsigned long long)st[0] | (state_words > 1 ? ((unsigned long long)st[state_words > 1 ? 1 : 0] << 32) : 0ull);
+		k.hi = (state_words > 2 ? (unsigned long long)st[state_words > 2 ? 2 : 0] : 0ull) | (1ull << 63);
+	}
+	else
+	{
+		unsigned long long a = 0x243f6a8885a308d3ull, b = 0x13198a2e03707344ull;
+#pragma unroll
+		for (int w = 0; w < state_words; w++)
+		{
+			a = mb_mix64(a ^ ((unsigned long long)st[w] + 0x9e3779b97f4a7c15ull * (w + 1)));
+			b = mb_mix64(b + ((unsigned long long)st[w] ^ (0xc2b2ae3d27d4eb4full * (w + 7))));
+		}
+		k.lo = a;
+		k.hi = b | (1ull << 63);
+	}
+	return k;
+}
+
+// Open-addressing insert of a fixed point (bounded probing; overflow is counted, never waited on).
+__device__ void mb_fixed_insert(const mb_stats_params& p, const state_word_t* st)
+{
+	const mb_key128 key = mb_state_key(st);
+	const unsigned h = (unsigned)mb_mix64(key.lo ^ mb_mix64(key.hi));
+	mb_key128 empty;
+	empty.lo = 0;
+	empty.hi = 0;
+	for (unsigned probe = 0; probe <= p.fp_mask; probe++)
+	{
+		const unsigned slot = (h + probe) & p.fp_mask;
+		const mb_key128 prev = atomicCAS(p.fp_keys + slot, empty, key);
+		if (prev.lo == 0ull && prev.hi == 0ull)
+		{
+#pragma unroll
+			for (int w = 0; w < state_words; w++)
+				p.fp_states[(size_t)slot * state_words + w] = st[w];
+			atomicAdd(p.fp_counts + slot, 1u);
+			return;
+		}
+		if (prev.lo == key.lo && prev.hi == key.hi)
+		{
+			atomicAdd(p.fp_counts + slot, 1u);
+			return;
+		}
+	}
+	atomicAdd(p.fp_overflow, 1u);
+}
+
+// ---------------------------------------------------------------- window accumulation
+
+// Per-thread run-length accumulator: consecutive slices that fall into the same
+// (window, non-internal state) bin are summed in a register before one atomic.
+struct mb_win_acc
+{
+	int ow;
+	uint32_t oi;
+	long long oq;
+	int hw;
+	long long hq;
+};
+
+__device__ __forceinline__ void mb_acc_init(mb_win_acc& a)
+{
+	a.ow = -1;
+	a.oi = 0;
+	a.oq = 0;
+	a.hw = -1;
+	a.hq = 0;
+}
+
+__device__ __forceinline__ void mb_add_h(long long* hsink, int w, long long v)
+{
+	if (v != 0)
+		atomicAdd(reinterpret_cast<unsigned long long*>(hsink + w), (unsigned long long)v);
+}
+
+__device__ __forceinline__ void mb_acc_flush(mb_win_acc& a, const mb_stats_params& p, long long* hsink)
+{
+	if (a.ow >= 0 && a.oq != 0)
+		atomicAdd(reinterpret_cast<unsigned long long*>(p.win_occ + (size_t)a.ow * p.n_bins + a.oi),
+				  (unsigned long long)a.oq);
+	if (a.hw >= 0)
+		mb_add_h(hsink, a.hw, a.hq);
+	mb_acc_init(a);
+}
+
+// Continuous time: the state `idx` occupies (t0, t1]; split it over windows exactly like
+// window_average_small.cu:66-92 and add each slice (and h * slice) to its window.
+__device__ __forceinline__ void mb_record_cont(mb_win_acc& a, const mb_stats_params& p, long long* hsink,
+											   uint32_t idx, float t0, float t1, float h)
+{
+	float sb = t0;
+	int w = (int)floorf(sb / p.win_tick);
+	for (int guard = 0; t1 > sb && guard <= p.n_windows + 2; guard++)
+	{
+		const float we = (float)(w + 1) * p.win_tick;
+		const float se = fminf(t1, we);
+		const float sl = se - sb;
+		if (w >= 0 && w < p.n_windows)
+		{
+			const long long q = __double2ll_rn((double)sl * p.fx);
+			if (w == a.ow && idx == a.oi)
+				a.oq += q;
+			else
+			{
+				if (a.ow >= 0 && a.oq != 0)
+					atomicAdd(reinterpret_cast<unsigned long long*>(p.win_occ + (size_t)a.ow * p.n_bins + a.oi),
+							  (unsigned long long)a.oq);
+				a.ow = w;
+				a.oi = idx;
+				a.oq = q;
+			}
+			const long long hq = __double2ll_rn((double)__fmul_rn(h, sl) * p.fx_h);
+			if (w == a.hw)
+				a.hq += hq;
+			else
+			{
+				if (a.hw >= 0)
+					mb_add_h(hsink, a.hw, a.hq);
+				a.hw = w;
+				a.hq = hq;
+			}
+		}
+		w++;
+		sb = se;
+	}
+}
+
+// Discrete time: count the state at window lround(t0 / tick) (window_average_small.cu:117-130).
+__device__ __forceinline__ void mb_record_disc(const mb_stats_params& p, long long* hsink, uint32_t idx, float t0,
+											   float h)
+{
+	const int w = (int)lroundf(t0 / p.win_tick);
+	if (w >= 0 && w < p.n_windows)
+	{
+		atomicAdd(p.win_cnt + (size_t)w * p.n_bins + idx, 1u);
+		mb_add_h(hsink, w, __double2ll_rn((double)h * p.fx_h));
+	}
+}
+
+__device__ __forceinline__ void mb_record(mb_win_acc& a, const mb_stats_params& p, long long* hsink,
+										  const state_word_t* st, float t0, float t1, float h)
+{
+	if (t1 == 0.f) // zero-time slots are empty (window_average_small.cu:68)
+		return;
+	const uint32_t idx = get_non_internal_index(st);
+	if (discrete_time)
+		mb_record_disc(p, hsink, idx, t0, h);
+	else
+		mb_record_cont(a, p, hsink, idx, t0, t1, h);
+}
+
+// ---------------------------------------------------------------- fused persistent kernel
+
+// One whole trajectory. EXACT reproduces the reference bit for bit: XORWOW streams seeded by
+// curand_init(seed, trajectory id, 0), the reference's fp32 operation order, and the 100-slot
+// epoch boundary at which the reference stops without flipping and redraws the waiting time
+// of the same state in the next epoch (simulation.cu:137-147 with simulation_runner.cu:104-162).
+template <bool EXACT, typename RNG>
+__device__ __forceinline__ void mb_trajectory(const mb_fused_params& P, RNG& rng, long long* hsink,
+											  unsigned long long& trans, mb_win_acc& acc)
+{
+	state_word_t st[state_words];
+	mb_init_state(st, rng, P.istate);
+	float time = 0.f;
+	int slot = 1;
+	bool fixed = false;
+	for (;;)
+	{
+		const float total = mbg_total_rate(st);
+		float h = 0.f, tn;
+		if (isinf(total))
+		{
+			// an infinite total rate gives zero waiting times forever: stop this trajectory
+			atomicAdd(P.errors, 1u);
+			break;
+		}
+		if (total == 0.f)
+		{
+			fixed = true;
+			tn = max_time;
+		}
+		else
+		{
+			if (discrete_time)
+			{
+				tn = time + time_tick;
+				tn = max_time - time_tick < tn ? max_time : tn;
+			}
+			else
+				tn = time + -logf(curand_uniform(&rng)) / total;
+			tn = fminf(tn, max_time);
+			h = EXACT ? mbg_entropy(st) : mbg_entropy_fast(st);
+		}
+		trans += (tn != 0.f) ? 1ull : 0ull;
+		mb_record(acc, P.st, hsink, st, time, tn, h);
+		time = tn;
+		if (time >= max_time)
+			break;
+		if (EXACT && P.traj_len > 1)
+		{
+			if (++slot >= P.traj_len)
+			{
+				slot = 1;
+				continue;
+			}
+		}
+		const float r = curand_uniform(&rng) * total;
+		mb_flip(st, mbg_select_flip(st, r));
+	}
+	atomicAdd(P.st.final_cnt + get_non_internal_index(st), 1u);
+	if (fixed)
+		mb_fixed_insert(P.st, st);
+}
+
+template <bool EXACT>
+__device__ __forceinline__ void mb_fused_body(const mb_fused_params& P)
+{
+	extern __shared__ long long mb_smem_h[];
+	long long* hsink = P.st.win_h;
+	if (P.st.h_in_smem)
+	{
+		for (int i = threadIdx.x; i < P.st.n_windows; i += blockDim.x)
+			mb_smem_h[i] = 0;
+		__syncthreads();
+		hsink = mb_smem_h;
+	}
+
+	unsigned long long trans = 0;
+	mb_win_acc acc;
+	mb_acc_init(acc);
+	for (;;)
+	{
+		const unsigned long long t = atomicAdd(P.next_traj, 1ull);
+		if (t >= P.n_traj)
+			break;
+		const unsigned long long id = P.first_traj + t;
+		if (EXACT)
+		{
+			curandState rng;
+			curand_init(P.seed, id, 0ull, &rng);
+			mb_trajectory<true>(P, rng, hsink, trans, acc);
+		}
+		else
+		{
+			curandStatePhilox4_32_10_t rng;
+			curand_init(P.seed, id, 0ull, &rng);
+			mb_trajectory<false>(P, rng, hsink, trans, acc);
+		}
+	}
+	mb_acc_flush(acc, P.st, hsink);
+
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+		trans += __shfl_down_sync(0xffffffffu, trans, o);
+	if ((threadIdx.x & 31) == 0 && trans)
+		atomicAdd(P.transitions, trans);
+
+	if (P.st.h_in_smem)
+	{
+		__syncthreads();
+		for (int i = threadIdx.x; i < P.st.n_windows; i += blockDim.x)
+			if (mb_smem_h[i] != 0)
+				atomicAdd(reinterpret_cast<unsigned long long*>(P.st.win_h + i), (unsigned long long)mb_smem_h[i]);
+	}
+}
+
+extern "C" __global__ void __launch_bounds__(256) mb_fused_exact(mb_fused_params P) { mb_fused_body<true>(P); }
+extern "C" __global__ void __launch_bounds__(256) mb_fused_fast(mb_fused_params P) { mb_fused_body<false>(P); }
+
+// ---------------------------------------------------------------- buffered epoch kernels (SoA)
+// Layouts (stride = batch capacity B):
+//   last_states[w * B + i], last_times[i], rands[i] (curandState), statuses[i]
+//   traj_states[(s * W + w) * B + i], traj_times[s * B + i], traj_h[s * B + i]
+
+extern "C" __global__ void mb_initialize_random(int n, unsigned long long seed, unsigned long long first,
+												 curandState* __restrict__ rands)
+{
+	const int id = blockIdx.x * blockDim.x + threadIdx.x;
+	if (id >= n)
+		return;
+	curand_init(seed, first + id, 0ull, rands + id); // simulation.cu:23-32
+}
+
+extern "C" __global__ void mb_initialize_initial_state(int n, int stride, const float* __restrict__ istate,
+														uint32_t* __restrict__ states, float* __restrict__ times,
+														curandState* __restrict__ rands)
+{
+	const int id = blockIdx.x * blockDim.x + threadIdx.x;
+	if (id >= n)
+		return;
+	curandState r = rands[id];
+	state_word_t st[state_words];
+	mb_init_state(st, r, istate);
+#pragma unroll
+	for (int w = 0; w < state_words; w++)
+		states[(size_t)w * stride + id] = st[w];
+	times[id] = 0.f;
+	rands[id] = r;
+}
+
+// One epoch of at most L-1 recorded steps per trajectory (simulation.cu:77-164).
+extern "C" __global__ void __launch_bounds__(256)
+	mb_simulate_epoch(int n, int stride, int L, uint32_t* __restrict__ last_states, float* __restrict__ last_times,
+					  curandState* __restrict__ rands, uint32_t* __restrict__ traj_states,
+					  float* __restrict__ traj_times, float* __restrict__ traj_h, uint8_t* __restrict__ statuses,
+					  unsigned long long* __restrict__ transitions)
+{
+	const int id = blockIdx.x * blockDim.x + threadIdx.x;
+	unsigned long long trans = 0;
+	if (id < n)
+	{
+		state_word_t st[state_words];
+#pragma unroll
+		for (int w = 0; w < state_words; w++)
+			st[w] = last_states[(size_t)w * stride + id];
+		curandState rng = rands[id];
+		float time = last_times[id];
+		trajectory_status status = trajectory_status::CONTINUE;
+		int step = 0;
+		traj_times[(size_t)step * stride + id] = time;
+		step++;
+		for (;;)
+		{
+			const float total = mbg_total_rate(st);
+			float h = 0.f;
+			if (isinf(total))
+			{
+				// an infinite total rate gives zero waiting times forever: end the trajectory
+				time = max_time;
+				break;
+			}
+			if (total == 0.f)
+			{
+				status = trajectory_status::FIXED_POINT;
+				time = max_time;
+			}
+			else
+			{
+				if (discrete_time)
+				{
+					time += time_tick;
+					time = max_time - time_tick < time ? max_time : time;
+				}
+				else
+					time += -logf(curand_uniform(&rng)) / total;
+				time = fminf(time, max_time);
+				h = mbg_entropy(st);
+			}
+#pragma unroll
+			for (int w = 0; w < state_words; w++)
+				traj_states[((size_t)step * state_words + w) * stride + id] = st[w];
+			traj_times[(size_t)step * stride + id] = time;
+			traj_h[(size_t)step * stride + id] = h;
+			trans += (time != 0.f) ? 1ull : 0ull;
+			step++;
+			if (time >= max_time || step >= L)
+				break;
+			const float r = curand_uniform(&rng) * total;
+			mb_flip(st, mbg_select_flip(st, r));
+		}
+		for (int s = step; s < L; s++) // empty slots carry the zero-time sentinel
+			traj_times[(size_t)s * stride + id] = 0.f;
+#pragma unroll
+		for (int w = 0; w < state_words; w++)
+			last_states[(size_t)w * stride + id] = st[w];
+		rands[id] = rng;
+		last_times[id] = time;
+		if (status != trajectory_status::FIXED_POINT)
+			status = (time >= max_time) ? trajectory_status::FINISHED : trajectory_status::CONTINUE;
+		statuses[id] = (uint8_t)status;
+	}
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+		trans += __shfl_down_sync(0xffffffffu, trans, o);
+	if ((threadIdx.x & 31) == 0 && trans)
+		atomicAdd(transitions, trans);
+}
+
+// Window statistics over one epoch's buffer, one thread per trajectory walking its slots
+// (coalesced across threads for every slot).
+extern "C" __global__ void __launch_bounds__(256)
+	mb_window_epoch(int n, int stride, int L, const uint32_t* __restrict__ traj_states,
+					const float* __restrict__ traj_times, const float* __restrict__ traj_h, mb_stats_params p)
+{
+	extern __shared__ long long mb_smem_h[];
+	long long* hsink = p.win_h;
+	if (p.h_in_smem)
+	{
+		for (int i = threadIdx.x; i < p.n_windows; i += blockDim.x)
+			mb_smem_h[i] = 0;
+		__syncthreads();
+		hsink = mb_smem_h;
+	}
+	const int id = blockIdx.x * blockDim.x + threadIdx.x;
+	if (id < n)
+	{
+		mb_win_acc acc;
+		mb_acc_init(acc);
+		float t0 = traj_times[id];
+		for (int s = 1; s < L; s++)
+		{
+			const float t1 = traj_times[(size_t)s * stride + id];
+			if (t1 != 0.f)
+			{
+				state_word_t st[state_words];
+#pragma unroll
+				for (int w = 0; w < state_words; w++)
+					st[w] = traj_states[((size_t)s * state_words + w) * stride + id];
+				mb_record(acc, p, hsink, st, t0, t1, traj_h[(size_t)s * stride + id]);
+			}
+			t0 = t1;
+		}
+		mb_acc_flush(acc, p, hsink);
+	}
+	if (p.h_in_smem)
+	{
+		__syncthreads();
+		for (int i = threadIdx.x; i < p.n_windows; i += blockDim.x)
+			if (mb_smem_h[i] != 0)
+				atomicAdd(reinterpret_cast<unsigned long long*>(p.win_h + i), (unsigned long long)mb_smem_h[i]);
+	}
+}
+
+// Final states of FINISHED / FIXED_POINT trajectories (final_states.cu:9-21).
+extern "C" __global__ void mb_final_epoch(int n, int stride, const uint32_t* __restrict__ last_states,
+										   const uint8_t* __restrict__ statuses, unsigned* __restrict__ final_cnt)
+{
+	const int id = blockIdx.x * blockDim.x + threadIdx.x;
+	if (id >= n)
+		return;
+	const uint8_t s = statuses[id];
+	if (s == (uint8_t)trajectory_status::FINISHED || s == (uint8_t)trajectory_status::FIXED_POINT)
+	{
+		state_word_t st[state_words];
+#pragma unroll
+		for (int w = 0; w < state_words; w++)
+			st[w] = last_states[(size_t)w * stride + id];
+		atomicAdd(final_cnt + get_non_internal_index(st), 1u);
+	}
+}
+
+// Fixed points of one epoch (replaces the CUB select/sort/run-length pipeline of
+// fixed_states.cu:84-125 with a device hash table).
+extern "C" __global__ void mb_fixed_epoch(int n, int stride, const uint32_t* __restrict__ last_states,
+										   const uint8_t* __restrict__ statuses, mb_stats_params p)
+{
+	const int id = blockIdx.x * blockDim.x + threadIdx.x;
+	if (id >= n)
+		return;
+	if (statuses[id] == (uint8_t)trajectory_status::FIXED_POINT)
+	{
+		state_word_t st[state_words];
+#pragma unroll
+		for (int w = 0; w < state_words; w++)
+			st[w] = last_states[(size_t)w * stride + id];
+		mb_fixed_insert(p, st);
+	}
+}
+
+// ---- stable partition of CONTINUE trajectories to the front (simulation_runner.cu:129-137)
+constexpr int MB_SCAN_BLOCK = 1024;
+
+extern "C" __global__ void __launch_bounds__(MB_SCAN_BLOCK)
+	mb_compact_count(int n, const uint8_t* __restrict__ statuses, unsigned* __restrict__ block_counts)
+{
+	const int id = blockIdx.x * MB_SCAN_BLOCK + threadIdx.x;
+	const bool keep = id < n && statuses[id] == (uint8_t)trajectory_status::CONTINUE;
+	const int c = __syncthreads_count(keep);
+	if (threadIdx.x == 0)
+		block_counts[blockIdx.x] = (unsigned)c;
+}
+
+// Exclusive scan of up to 1024 * 1024 block counts in one block; writes the total last.
+extern "C" __global__ void __launch_bounds__(MB_SCAN_BLOCK)
+	mb_compact_scan(int nblocks, const unsigned* __restrict__ block_counts, unsigned* __restrict__ block_offsets)
+{
+	__shared__ unsigned part[MB_SCAN_BLOCK];
+	const int per = (nblocks + MB_SCAN_BLOCK - 1) / MB_SCAN_BLOCK;
+	const int b0 = threadIdx.x * per;
+	unsigned s = 0;
+	for (int i = 0; i < per; i++)
+		if (b0 + i < nblocks)
+			s += block_counts[b0 + i];
+	part[threadIdx.x] = s;
+	__syncthreads();
+	for (int o = 1; o < MB_SCAN_BLOCK; o <<= 1)
+	{
+		unsigned v = threadIdx.x >= o ? part[threadIdx.x - o] : 0u;
+		__syncthreads();
+		part[threadIdx.x] += v;
+		__syncthreads();
+	}
+	unsigned run = part[threadIdx.x] - s;
+	for (int i = 0; i < per; i++)
+		if (b0 + i < nblocks)
+		{
+			block_offsets[b0 + i] = run;
+			run += block_counts[b0 + i];
+		}
+	if (threadIdx.x == MB_SCAN_BLOCK - 1)
+		block_offsets[nblocks] = part[MB_SCAN_BLOCK - 1];
+}
+
+extern "C" __global__ void __launch_bounds__(MB_SCAN_BLOCK)
+	mb_compact_scatter(int n, int stride, const uint8_t* __restrict__ statuses,
+					   const unsigned* __restrict__ block_offsets, const uint32_t* __restrict__ src_states,
+					   const float* __restrict__ src_times, const curandState* __restrict__ src_rands,
+					   uint32_t* __restrict__ dst_states, float* __restrict__ dst_times, curandState* __restrict__ dst_rands)
+{
+	__shared__ unsigned warp_sums[MB_SCAN_BLOCK / 32];
+	const int id = blockIdx.x * MB_SCAN_BLOCK + threadIdx.x;
+	const bool keep = id < n && statuses[id] == (uint8_t)trajectory_status::CONTINUE;
+	const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	if (lane == 0)
+		warp_sums[warp] = __popc(ballot);
+	__syncthreads();
+	if (warp == 0)
+	{
+		unsigned v = warp_sums[lane];
+		unsigned inc = v;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1)
+		{
+			unsigned t = __shfl_up_sync(0xffffffffu, inc, o);
+			if (lane >= o)
+				inc += t;
+		}
+		warp_sums[lane] = inc - v;
+	}
+	__syncthreads();
+	if (keep)
+	{
+		const unsigned dst = block_offsets[blockIdx.x] + warp_sums[warp] + __popc(ballot & ((1u << lane) - 1u));
+#pragma unroll
+		for (int w = 0; w < state_words; w++)
+			dst_states[(size_t)w * stride + dst] = src_states[(size_t)w * stride + id];
+		dst_times[dst] = src_times[id];
+		dst_rands[dst] = src_rands[id];
+	}
+}
+
+// ---- compaction of the fixed-point table into (state, count) records
+extern "C" __global__ void mb_fixed_extract(unsigned cap, const mb_key128* __restrict__ keys,
+											 const unsigned* __restrict__ counts, const uint32_t* __restrict__ states,
+											 unsigned* __restrict__ out_n, uint32_t* __restrict__ out_states,
+											 unsigned* __restrict__ out_counts)
+{
+	const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= cap)
+		return;
+	const mb_key128 k = keys[i];
+	if (k.lo == 0ull && k.hi == 0ull)
+		return;
+	const unsigned o = atomicAdd(out_n, 1u);
+#pragma unroll
+	for (int w = 0; w < state_words; w++)
+		out_states[(size_t)o * state_words + w] = states[(size_t)i * state_words + w];
+	out_counts[o] = counts[i];
+}

@@ -1,0 +1,729 @@
+// Host runtime: NVRTC compilation, module loading through the CUDA driver API (resolved at
+// run time with cudaGetDriverEntryPointByVersion, so the library loads on hosts without a GPU
+// driver), and the run drivers.
+#include "runtime.h"
+
+#include <curand_kernel.h>
+#include <nvrtc.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <mutex>
+#include <numeric>
+#include <sstream>
+
+#include "kernels/params.cuh"
+
+namespace mb {
+
+namespace {
+
+#include "engine_src.inc" // mb_params_source, mb_engine_source (embedded kernels/*.cuh)
+
+struct driver_api
+{
+	CUresult (*ModuleLoadData)(CUmodule*, const void*) = nullptr;
+	CUresult (*ModuleUnload)(CUmodule) = nullptr;
+	CUresult (*ModuleGetFunction)(CUfunction*, CUmodule, const char*) = nullptr;
+	CUresult (*LaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, CUstream,
+							 void**, void**) = nullptr;
+	CUresult (*FuncSetAttribute)(CUfunction, CUfunction_attribute, int) = nullptr;
+	CUresult (*GetErrorString)(CUresult, const char**) = nullptr;
+	CUresult (*OccupancyMaxActiveBlocksPerMultiprocessor)(int*, CUfunction, int, size_t) = nullptr;
+};
+
+template <typename F>
+void resolve(const char* name, F& fn)
+{
+	void* p = nullptr;
+	cudaDriverEntryPointQueryResult q;
+	cudaError_t e = cudaGetDriverEntryPointByVersion(name, &p, 12000, cudaEnableDefault, &q);
+	if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p)
+		throw engine_error(MB_ERR_CUDA, std::string("cannot resolve CUDA driver entry point ") + name);
+	fn = reinterpret_cast<F>(p);
+}
+
+const driver_api& drv()
+{
+	static driver_api api;
+	static std::once_flag once;
+	static std::string failure;
+	std::call_once(once, [] {
+		try
+		{
+			resolve("cuModuleLoadData", api.ModuleLoadData);
+			resolve("cuModuleUnload", api.ModuleUnload);
+			resolve("cuModuleGetFunction", api.ModuleGetFunction);
+			resolve("cuLaunchKernel", api.LaunchKernel);
+			resolve("cuFuncSetAttribute", api.FuncSetAttribute);
+			resolve("cuGetErrorString", api.GetErrorString);
+			resolve("cuOccupancyMaxActiveBlocksPerMultiprocessor", api.OccupancyMaxActiveBlocksPerMultiprocessor);
+		}
+		catch (const std::exception& e)
+		{
+			failure = e.what();
+		}
+	});
+	if (!failure.empty())
+		throw engine_error(MB_ERR_CUDA, failure);
+	return api;
+}
+
+void cu_throw(CUresult r, const char* what)
+{
+	if (r == CUDA_SUCCESS)
+		return;
+	const char* s = nullptr;
+	if (drv().GetErrorString)
+		drv().GetErrorString(r, &s);
+	throw engine_error(MB_ERR_CUDA, std::string(what) + ": " + (s ? s : "CUDA driver error") + " (" +
+										std::to_string((int)r) + ")");
+}
+
+std::string cuda_include_dir()
+{
+	if (const char* e = std::getenv("MABOSS_CUDA_INCLUDE"))
+		return e;
+#ifdef MB_CUDA_INCLUDE
+	return MB_CUDA_INCLUDE;
+#else
+	return "/usr/local/cuda/include";
+#endif
+}
+
+int parse_constexpr(const std::string& src, const std::string& name, int fallback)
+{
+	const std::string key = "constexpr int " + name + " = ";
+	auto p = src.find(key);
+	if (p == std::string::npos)
+		return fallback;
+	return std::atoi(src.c_str() + p + key.size());
+}
+
+std::mutex cache_mu;
+std::map<size_t, std::vector<char>>& cubin_cache()
+{
+	static std::map<size_t, std::vector<char>> c;
+	return c;
+}
+
+template <typename T>
+T* ptr(const dbuf& b)
+{
+	return b.as<T>();
+}
+
+unsigned next_pow2(unsigned long long v)
+{
+	unsigned p = 1;
+	while (p < v && p < (1u << 30))
+		p <<= 1;
+	return p;
+}
+
+} // namespace
+
+void cuda_throw(cudaError_t e, const char* what)
+{
+	if (e == cudaSuccess)
+		return;
+	cudaGetLastError();
+	int code = (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? MB_ERR_NO_DEVICE
+			   : (e == cudaErrorMemoryAllocation)							 ? MB_ERR_LIMIT
+																			 : MB_ERR_CUDA;
+	throw engine_error(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+dbuf::~dbuf()
+{
+	if (p)
+		cudaFree(p);
+}
+
+void dbuf::alloc(size_t n)
+{
+	if (p)
+		cudaFree(p);
+	p = nullptr;
+	bytes = 0;
+	if (n == 0)
+		return;
+	MB_CUDA(cudaMalloc(&p, n));
+	bytes = n;
+}
+
+context::context(int dev) : device(dev)
+{
+	int count = 0;
+	MB_CUDA(cudaGetDeviceCount(&count));
+	if (dev < 0 || dev >= count)
+		throw engine_error(MB_ERR_NO_DEVICE, "CUDA device " + std::to_string(dev) + " not present");
+	MB_CUDA(cudaSetDevice(dev));
+	MB_CUDA(cudaFree(nullptr)); // make the primary context current
+	cudaDeviceProp prop;
+	MB_CUDA(cudaGetDeviceProperties(&prop, dev));
+	sm_count = prop.multiProcessorCount;
+	cc_major = prop.major;
+	cc_minor = prop.minor;
+	if (cc_major != 10)
+		throw engine_error(MB_ERR_NO_DEVICE, std::string("this engine is built for sm_100a (B200); device is ") +
+												 prop.name + " sm_" + std::to_string(cc_major) + std::to_string(cc_minor));
+	MB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+}
+
+context::~context()
+{
+	if (stream)
+	{
+		cudaSetDevice(device);
+		cudaStreamDestroy(stream);
+	}
+}
+
+module::~module()
+{
+	if (mod)
+	{
+		cudaSetDevice(ctx->device);
+		drv().ModuleUnload(mod);
+	}
+}
+
+std::vector<char> compile_cubin(const std::string& generated_code, std::string& log)
+{
+	const std::string source = generated_code + "\n// ---- engine: kernel parameter blocks\n" + mb_params_source +
+							   "\n// ---- engine: kernels\n" + mb_engine_source;
+	const int N = parse_constexpr(generated_code, "state_size", -1);
+	const int W = parse_constexpr(generated_code, "state_words", -1);
+	if (N <= 0 || W != (N + 31) / 32)
+		throw engine_error(MB_ERR_COMPILE, "generated code does not define state_size/state_words");
+	const std::string inc = "-I" + cuda_include_dir();
+	const char* opts[] = { "-arch=sm_100a", "-std=c++17", "-lineinfo", "-DNDEBUG", inc.c_str() };
+	const size_t key = std::hash<std::string>()(source + inc);
+	{
+		std::lock_guard<std::mutex> lk(cache_mu);
+		auto it = cubin_cache().find(key);
+		if (it != cubin_cache().end())
+			return it->second;
+	}
+	nvrtcProgram prog;
+	if (nvrtcCreateProgram(&prog, source.c_str(), "maboss_b200_model.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS)
+		throw engine_error(MB_ERR_COMPILE, "nvrtcCreateProgram failed");
+	nvrtcResult r = nvrtcCompileProgram(prog, (int)(sizeof opts / sizeof opts[0]), opts);
+	size_t log_size = 0;
+	nvrtcGetProgramLogSize(prog, &log_size);
+	log.assign(log_size, '\0');
+	if (log_size)
+		nvrtcGetProgramLog(prog, &log[0]);
+	if (r != NVRTC_SUCCESS)
+	{
+		nvrtcDestroyProgram(&prog);
+		throw engine_error(MB_ERR_COMPILE, std::string("NVRTC compilation failed: ") + nvrtcGetErrorString(r) + "\n" + log);
+	}
+	size_t n = 0;
+	nvrtcGetCUBINSize(prog, &n);
+	std::vector<char> cubin(n);
+	nvrtcGetCUBIN(prog, cubin.data());
+	nvrtcDestroyProgram(&prog);
+	std::lock_guard<std::mutex> lk(cache_mu);
+	cubin_cache()[key] = cubin;
+	return cubin;
+}
+
+std::unique_ptr<module> compile_module(context& ctx, const std::string& generated_code)
+{
+	MB_CUDA(cudaSetDevice(ctx.device));
+	auto m = std::make_unique<module>();
+	m->ctx = &ctx;
+	m->state_size = parse_constexpr(generated_code, "state_size", -1);
+	m->state_words = parse_constexpr(generated_code, "state_words", -1);
+	m->noninternal_count = parse_constexpr(generated_code, "mbg_noninternal_count", -1);
+	std::vector<char> cubin = compile_cubin(generated_code, m->log);
+	m->source = generated_code;
+	cu_throw(drv().ModuleLoadData(&m->mod, cubin.data()), "cuModuleLoadData");
+	auto get = [&](CUfunction& f, const char* name) { cu_throw(drv().ModuleGetFunction(&f, m->mod, name), name); };
+	get(m->fused_exact, "mb_fused_exact");
+	get(m->fused_fast, "mb_fused_fast");
+	get(m->init_random, "mb_initialize_random");
+	get(m->init_state, "mb_initialize_initial_state");
+	get(m->sim_epoch, "mb_simulate_epoch");
+	get(m->window_epoch, "mb_window_epoch");
+	get(m->final_epoch, "mb_final_epoch");
+	get(m->fixed_epoch, "mb_fixed_epoch");
+	get(m->compact_count, "mb_compact_count");
+	get(m->compact_scan, "mb_compact_scan");
+	get(m->compact_scatter, "mb_compact_scatter");
+	get(m->fixed_extract, "mb_fixed_extract");
+	return m;
+}
+
+void launch(CUfunction f, unsigned grid, unsigned block, size_t smem, cudaStream_t s, void** args)
+{
+	if (grid == 0)
+		return;
+	if (smem > 48 * 1024)
+		cu_throw(drv().FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem),
+				 "cuFuncSetAttribute");
+	cu_throw(drv().LaunchKernel(f, grid, 1, 1, block, 1, 1, (unsigned)smem, (CUstream)s, args, nullptr),
+			 "cuLaunchKernel");
+}
+
+int occupancy_blocks(CUfunction f, int block, size_t smem)
+{
+	int n = 0;
+	cu_throw(drv().OccupancyMaxActiveBlocksPerMultiprocessor(&n, f, block, smem), "cuOccupancyMaxActiveBlocks");
+	return std::max(n, 1);
+}
+
+run_config config_from_layout(const model_layout& L, int mode)
+{
+	run_config c;
+	c.mode = mode;
+	c.sample_count = L.sample_count;
+	c.seed = L.seed;
+	c.max_time = L.max_time;
+	c.time_tick = L.time_tick;
+	c.discrete_time = L.discrete_time;
+	c.istate = L.istate;
+	c.noninternal_nodes = L.noninternal_nodes;
+	return c;
+}
+
+int occupancy_exponent(long long n_traj, float tick, bool discrete)
+{
+	// per-bin sums are bounded by n * tick (continuous); discrete bins are plain counts
+	if (discrete)
+		return 0;
+	const double bound = std::max(1.0, (double)std::max(1LL, n_traj) * (double)std::max(tick, 1e-30f));
+	return std::clamp((int)std::floor(61.0 - std::log2(bound)), 0, 100);
+}
+
+int entropy_exponent(long long n_traj, float tick, bool discrete)
+{
+	// h <= log2(20) < 8 per slice
+	const double per = discrete ? 8.0 : 8.0 * (double)std::max(tick, 1e-30f);
+	const double bound = std::max(1.0, (double)std::max(1LL, n_traj) * per);
+	return std::clamp((int)std::floor(61.0 - std::log2(bound)), 0, 100);
+}
+
+double result::window_prob(int w, unsigned bin) const
+{
+	const size_t i = (size_t)w * n_bins + bin;
+	if (discrete_time)
+		return (double)win_cnt[i] / (double)n_traj;
+	return ((double)win_occ[i] / fx) / ((double)n_traj * (double)time_tick);
+}
+
+double result::window_th(int w) const
+{
+	double v = ((double)win_h[w] / fx_h) / (double)n_traj;
+	return discrete_time ? v : v / (double)time_tick;
+}
+
+// ---------------------------------------------------------------- statistics state
+
+void stats_state::init(module& m, float tick, float tmax, bool discrete, const std::vector<int>& noninternal,
+					   long long n, int fixed_capacity_log2, cudaStream_t s)
+{
+	mod = &m;
+	const int k = (int)noninternal.size();
+	if (m.noninternal_count >= 0 && m.noninternal_count != k)
+		throw engine_error(MB_ERR_INVALID, "the module was generated for " + std::to_string(m.noninternal_count) +
+											   " non-internal nodes, the statistics got " + std::to_string(k));
+	if (k > 20)
+		throw engine_error(MB_ERR_LIMIT, "more than 20 non-internal nodes (" + std::to_string(k) +
+											 ") is not supported by the dense window histogram");
+	for (int i : noninternal)
+		if (i < 0 || i >= m.state_size)
+			throw engine_error(MB_ERR_INVALID, "non-internal node index out of range");
+	if (!(tick > 0.f) || !(tmax > 0.f))
+		throw engine_error(MB_ERR_INVALID, "max_time and time_tick must be positive");
+	const float q = tmax / tick;
+	const double T = std::ceil((double)q);
+	if (T > (double)(1 << 24))
+		throw engine_error(MB_ERR_LIMIT, "too many windows (max_time / time_tick)");
+	n_windows = (int)T;
+	n_bins = 1u << k;
+	discrete_time = discrete;
+	time_tick = tick;
+	max_time = tmax;
+	noninternal_nodes = noninternal;
+	fx = std::ldexp(1.0, occupancy_exponent(n, tick, discrete));
+	fx_h = std::ldexp(1.0, entropy_exponent(n, tick, discrete));
+	h_in_smem = n_windows * sizeof(long long) <= 48 * 1024 ? 1 : 0;
+
+	const size_t cells = (size_t)n_windows * n_bins;
+	if (discrete)
+	{
+		cnt.alloc(cells * sizeof(unsigned));
+		MB_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes, s));
+	}
+	else
+	{
+		occ.alloc(cells * sizeof(long long));
+		MB_CUDA(cudaMemsetAsync(occ.p, 0, occ.bytes, s));
+	}
+	h.alloc(n_windows * sizeof(long long));
+	MB_CUDA(cudaMemsetAsync(h.p, 0, h.bytes, s));
+	fin.alloc(n_bins * sizeof(unsigned));
+	MB_CUDA(cudaMemsetAsync(fin.p, 0, fin.bytes, s));
+
+	fp_cap = fixed_capacity_log2 > 0
+				 ? (1u << std::min(fixed_capacity_log2, 28))
+				 : next_pow2((unsigned long long)std::max(1024LL, std::min(std::max(n, 0LL), 1LL << 22) * 2));
+	fp_keys.alloc((size_t)fp_cap * sizeof(mb_key128));
+	fp_counts.alloc((size_t)fp_cap * sizeof(unsigned));
+	fp_states.alloc((size_t)fp_cap * m.state_words * sizeof(unsigned));
+	MB_CUDA(cudaMemsetAsync(fp_keys.p, 0, fp_keys.bytes, s));
+	MB_CUDA(cudaMemsetAsync(fp_counts.p, 0, fp_counts.bytes, s));
+	counters.alloc(64);
+	MB_CUDA(cudaMemsetAsync(counters.p, 0, 64, s));
+
+	p = mb_stats_params{};
+	p.n_windows = n_windows;
+	p.n_bins = n_bins;
+	p.win_tick = tick;
+	p.h_in_smem = h_in_smem;
+	p.fx = fx;
+	p.fx_h = fx_h;
+	p.win_occ = occ.as<long long>();
+	p.win_cnt = cnt.as<unsigned>();
+	p.win_h = h.as<long long>();
+	p.final_cnt = fin.as<unsigned>();
+	p.fp_keys = fp_keys.as<mb_key128>();
+	p.fp_counts = fp_counts.as<unsigned>();
+	p.fp_states = fp_states.as<unsigned>();
+	p.fp_mask = fp_cap - 1;
+	p.fp_overflow = fp_overflow_ctr();
+}
+
+void stats_state::zero(cudaStream_t s)
+{
+	if (occ.p)
+		MB_CUDA(cudaMemsetAsync(occ.p, 0, occ.bytes, s));
+	if (cnt.p)
+		MB_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes, s));
+	MB_CUDA(cudaMemsetAsync(h.p, 0, h.bytes, s));
+	MB_CUDA(cudaMemsetAsync(fin.p, 0, fin.bytes, s));
+	MB_CUDA(cudaMemsetAsync(fp_keys.p, 0, fp_keys.bytes, s));
+	MB_CUDA(cudaMemsetAsync(fp_counts.p, 0, fp_counts.bytes, s));
+	MB_CUDA(cudaMemsetAsync(counters.p, 0, counters.bytes, s));
+}
+
+void stats_state::set_istate(const std::vector<float>& is, cudaStream_t s)
+{
+	if ((int)is.size() != mod->state_size)
+		throw engine_error(MB_ERR_INVALID, "initial probabilities must have one entry per node");
+	istate.alloc(is.size() * sizeof(float));
+	MB_CUDA(cudaMemcpyAsync(istate.p, is.data(), istate.bytes, cudaMemcpyHostToDevice, s));
+}
+
+void stats_state::window_batch(cudaStream_t s, int n, int stride, int traj_len, const unsigned* traj_states,
+							   const float* traj_times, const float* traj_h)
+{
+	if (n <= 0)
+		return;
+	mb_stats_params sp = p;
+	void* a[] = { &n, &stride, &traj_len, &traj_states, &traj_times, &traj_h, &sp };
+	launch(mod->window_epoch, (n + 255) / 256, 256, h_smem(), s, a);
+}
+
+void stats_state::final_batch(cudaStream_t s, int n, int stride, const unsigned* last_states,
+							  const unsigned char* statuses)
+{
+	if (n <= 0)
+		return;
+	unsigned* fc = p.final_cnt;
+	void* a[] = { &n, &stride, &last_states, &statuses, &fc };
+	launch(mod->final_epoch, (n + 255) / 256, 256, 0, s, a);
+}
+
+void stats_state::fixed_batch(cudaStream_t s, int n, int stride, const unsigned* last_states,
+							  const unsigned char* statuses)
+{
+	if (n <= 0)
+		return;
+	mb_stats_params sp = p;
+	void* a[] = { &n, &stride, &last_states, &statuses, &sp };
+	launch(mod->fixed_epoch, (n + 255) / 256, 256, 0, s, a);
+}
+
+std::unique_ptr<result> stats_state::finalize(long long n, cudaStream_t s)
+{
+	auto rp = std::make_unique<result>();
+	result& r = *rp;
+	const module& m = *mod;
+	r.state_size = m.state_size;
+	r.state_words = m.state_words;
+	r.n_windows = n_windows;
+	r.n_bins = n_bins;
+	r.n_traj = n;
+	r.discrete_time = discrete_time;
+	r.time_tick = time_tick;
+	r.max_time = max_time;
+	r.noninternal_nodes = noninternal_nodes;
+	r.fx = fx;
+	r.fx_h = fx_h;
+	const size_t cells = (size_t)n_windows * n_bins;
+	if (discrete_time)
+	{
+		r.win_cnt.resize(cells);
+		MB_CUDA(cudaMemcpyAsync(r.win_cnt.data(), cnt.p, cells * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+	}
+	else
+	{
+		r.win_occ.resize(cells);
+		MB_CUDA(cudaMemcpyAsync(r.win_occ.data(), occ.p, cells * sizeof(long long), cudaMemcpyDeviceToHost, s));
+	}
+	r.win_h.resize(n_windows);
+	MB_CUDA(cudaMemcpyAsync(r.win_h.data(), h.p, n_windows * sizeof(long long), cudaMemcpyDeviceToHost, s));
+	r.final_cnt.resize(n_bins);
+	MB_CUDA(cudaMemcpyAsync(r.final_cnt.data(), fin.p, n_bins * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+
+	// count occupied fixed-point slots, then compact them on the device and copy the records
+	unsigned ctr[8];
+	MB_CUDA(cudaMemsetAsync(extract_ctr(), 0, sizeof(unsigned), s));
+	dbuf out_counts((size_t)fp_cap * sizeof(unsigned));
+	dbuf out_states((size_t)fp_cap * m.state_words * sizeof(unsigned));
+	{
+		unsigned cap = fp_cap;
+		mb_key128* keys = p.fp_keys;
+		unsigned* counts = p.fp_counts;
+		unsigned* states = p.fp_states;
+		unsigned* out_n = extract_ctr();
+		unsigned* os = out_states.as<unsigned>();
+		unsigned* oc = out_counts.as<unsigned>();
+		void* args[] = { &cap, &keys, &counts, &states, &out_n, &os, &oc };
+		launch(m.fixed_extract, (cap + 255) / 256, 256, 0, s, args);
+	}
+	unsigned long long trans = 0;
+	MB_CUDA(cudaMemcpyAsync(ctr, counters.p, sizeof ctr, cudaMemcpyDeviceToHost, s));
+	MB_CUDA(cudaMemcpyAsync(&trans, transitions(), sizeof trans, cudaMemcpyDeviceToHost, s));
+	MB_CUDA(cudaStreamSynchronize(s));
+	r.transitions = trans;
+	r.fixed_overflow = ctr[4];
+	r.rate_errors = ctr[6];
+	const unsigned nfp = ctr[5];
+	const int W = m.state_words;
+	std::vector<unsigned> st((size_t)nfp * W), cn(nfp);
+	if (nfp)
+	{
+		MB_CUDA(cudaMemcpyAsync(st.data(), out_states.p, st.size() * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+		MB_CUDA(cudaMemcpyAsync(cn.data(), out_counts.p, cn.size() * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+		MB_CUDA(cudaStreamSynchronize(s));
+	}
+	// order like std::map<static_state_t> (state.h:43-49: compare from the highest word down)
+	std::vector<unsigned> order(nfp);
+	std::iota(order.begin(), order.end(), 0u);
+	std::sort(order.begin(), order.end(), [&](unsigned a, unsigned b) {
+		for (int w = W - 1; w >= 0; w--)
+		{
+			unsigned x = st[(size_t)a * W + w], y = st[(size_t)b * W + w];
+			if (x != y)
+				return x < y;
+		}
+		return false;
+	});
+	r.fixed_states.resize((size_t)nfp * W);
+	r.fixed_counts.resize(nfp);
+	for (unsigned i = 0; i < nfp; i++)
+	{
+		std::copy(st.begin() + (size_t)order[i] * W, st.begin() + (size_t)(order[i] + 1) * W,
+				  r.fixed_states.begin() + (size_t)i * W);
+		r.fixed_counts[i] = cn[order[i]];
+	}
+	return rp;
+}
+
+// ---------------------------------------------------------------- run drivers
+
+namespace {
+
+void launch_fused(module& m, const run_config& c, stats_state& st, long long n, cudaStream_t s)
+{
+	if (n > 0xffffffffLL)
+		throw engine_error(MB_ERR_LIMIT, "sample_count above 2^32 - 1");
+	if (n == 0)
+		return;
+	mb_fused_params P{};
+	P.st = st.p;
+	P.istate = st.istate.as<float>();
+	P.seed = c.seed;
+	P.first_traj = c.first_traj;
+	P.n_traj = (unsigned)n;
+	P.traj_len = c.mode == MB_MODE_FUSED_EXACT ? c.traj_len : 0;
+	P.next_traj = st.next_traj();
+	P.transitions = st.transitions();
+	P.errors = st.error_ctr();
+	CUfunction f = c.mode == MB_MODE_FUSED_EXACT ? m.fused_exact : m.fused_fast;
+	const size_t smem = st.h_smem();
+	const int per_sm = c.blocks_per_sm > 0 ? c.blocks_per_sm : occupancy_blocks(f, c.block, smem);
+	const long long needed = (n + c.block - 1) / c.block;
+	const unsigned grid = (unsigned)std::max(1LL, std::min<long long>(needed, (long long)per_sm * m.ctx->sm_count));
+	void* args[] = { &P };
+	launch(f, grid, c.block, smem, s, args);
+}
+
+// Buffered epochs (simulation_runner.cu:54-180): simulate -> stats -> partition -> refill.
+void run_epochs(module& m, const run_config& c, stats_state& st, long long n, cudaStream_t s, int& epochs)
+{
+	const int W = m.state_words;
+	const int L = std::max(2, c.traj_len);
+	if (n <= 0)
+		return;
+	const long long Bll = std::min<long long>(std::max(1, c.batch_limit), n);
+	const int B = (int)Bll;
+	dbuf st0((size_t)W * B * 4), st1((size_t)W * B * 4), t0((size_t)B * 4), t1((size_t)B * 4);
+	dbuf r0((size_t)B * sizeof(curandState)), r1((size_t)B * sizeof(curandState));
+	dbuf ts((size_t)L * W * B * 4), tt((size_t)L * B * 4), th((size_t)L * B * 4), stat((size_t)B);
+	const int nblocks = (B + 1023) / 1024;
+	dbuf bc((size_t)nblocks * 4), bo((size_t)(nblocks + 1) * 4);
+	unsigned long long* trans = st.transitions();
+	float* istate = st.istate.as<float>();
+
+	auto init = [&](int cnt, int offset, unsigned long long first, dbuf& sbuf, dbuf& tbuf, dbuf& rbuf) {
+		unsigned long long seed = c.seed;
+		void* rptr = rbuf.as<char>() + (size_t)offset * sizeof(curandState);
+		void* a1[] = { &cnt, &seed, &first, &rptr };
+		launch(m.init_random, (cnt + 255) / 256, 256, 0, s, a1);
+		int stride = B;
+		unsigned* sp = sbuf.as<unsigned>() + offset;
+		float* tp = tbuf.as<float>() + offset;
+		void* a2[] = { &cnt, &stride, &istate, &sp, &tp, &rptr };
+		launch(m.init_state, (cnt + 255) / 256, 256, 0, s, a2);
+	};
+
+	init(B, 0, c.first_traj, st0, t0, r0);
+	long long next_id = B;
+	int in_batch = B;
+	dbuf *cs = &st0, *ct = &t0, *cr = &r0, *ns = &st1, *nt = &t1, *nr = &r1;
+	while (in_batch > 0)
+	{
+		int stride = B;
+		int len = L;
+		unsigned* ls = cs->as<unsigned>();
+		float* lt = ct->as<float>();
+		void* rr = cr->p;
+		unsigned* tsp = ts.as<unsigned>();
+		float* ttp = tt.as<float>();
+		float* thp = th.as<float>();
+		unsigned char* stp = stat.as<unsigned char>();
+		void* as[] = { &in_batch, &stride, &len, &ls, &lt, &rr, &tsp, &ttp, &thp, &stp, &trans };
+		launch(m.sim_epoch, (in_batch + 255) / 256, 256, 0, s, as);
+		// statistics plugins in the order of main.cpp:65-74
+		st.final_batch(s, in_batch, stride, ls, stp);
+		st.fixed_batch(s, in_batch, stride, ls, stp);
+		st.window_batch(s, in_batch, stride, len, tsp, ttp, thp);
+		// partition CONTINUE trajectories to the front of the other buffer set
+		int nb = (in_batch + 1023) / 1024;
+		unsigned* bcp = bc.as<unsigned>();
+		unsigned* bop = bo.as<unsigned>();
+		void* a1[] = { &in_batch, &stp, &bcp };
+		launch(m.compact_count, nb, 1024, 0, s, a1);
+		void* a2[] = { &nb, &bcp, &bop };
+		launch(m.compact_scan, 1, 1024, 0, s, a2);
+		unsigned* nsp = ns->as<unsigned>();
+		float* ntp = nt->as<float>();
+		void* nrp = nr->p;
+		void* a3[] = { &in_batch, &stride, &stp, &bop, &ls, &lt, &rr, &nsp, &ntp, &nrp };
+		launch(m.compact_scatter, nb, 1024, 0, s, a3);
+		unsigned kept = 0;
+		MB_CUDA(cudaMemcpyAsync(&kept, bop + nb, sizeof kept, cudaMemcpyDeviceToHost, s));
+		MB_CUDA(cudaStreamSynchronize(s));
+		std::swap(cs, ns);
+		std::swap(ct, nt);
+		std::swap(cr, nr);
+		const int add = (int)std::max(0LL, std::min<long long>(B - (long long)kept, n - next_id));
+		if (add > 0)
+		{
+			init(add, (int)kept, c.first_traj + next_id, *cs, *ct, *cr);
+			next_id += add;
+		}
+		in_batch = (int)kept + add;
+		epochs++;
+	}
+}
+
+} // namespace
+
+runner::runner(module& m, const run_config& c) : mod(&m), cfg(c)
+{
+	MB_CUDA(cudaSetDevice(m.ctx->device));
+	if (c.sample_count < 0)
+		throw engine_error(MB_ERR_INVALID, "negative sample_count");
+	if (c.block <= 0 || c.block > 256 || (c.block % 32) != 0)
+		throw engine_error(MB_ERR_INVALID, "block size must be a multiple of 32 in [32, 256]");
+	if (c.mode != MB_MODE_EPOCH && c.mode != MB_MODE_FUSED_EXACT && c.mode != MB_MODE_FUSED_FAST)
+		throw engine_error(MB_ERR_INVALID, "unknown run mode");
+	cudaStream_t s = m.ctx->stream;
+	st.init(m, c.time_tick, c.max_time, c.discrete_time, c.noninternal_nodes, c.sample_count, c.fixed_capacity_log2, s);
+	st.set_istate(c.istate, s);
+	MB_CUDA(cudaEventCreate(&ev0));
+	MB_CUDA(cudaEventCreate(&ev1));
+	MB_CUDA(cudaStreamSynchronize(s));
+}
+
+runner::~runner()
+{
+	cudaSetDevice(mod->ctx->device);
+	if (ev0)
+		cudaEventDestroy(ev0);
+	if (ev1)
+		cudaEventDestroy(ev1);
+}
+
+unsigned runner::kernel_launches() const { return cfg.mode == MB_MODE_EPOCH ? 0u : (cfg.sample_count > 0 ? 1u : 0u); }
+
+void runner::launch(cudaStream_t s)
+{
+	MB_CUDA(cudaSetDevice(mod->ctx->device));
+	st.zero(s);
+	MB_CUDA(cudaEventRecord(ev0, s));
+	epochs = 0;
+	if (cfg.mode == MB_MODE_EPOCH)
+		run_epochs(*mod, cfg, st, cfg.sample_count, s, epochs);
+	else
+	{
+		launch_fused(*mod, cfg, st, cfg.sample_count, s);
+		epochs = 1;
+	}
+	MB_CUDA(cudaEventRecord(ev1, s));
+}
+
+std::unique_ptr<result> runner::collect(cudaStream_t s)
+{
+	MB_CUDA(cudaSetDevice(mod->ctx->device));
+	auto r = st.finalize(cfg.sample_count, s);
+	MB_CUDA(cudaEventSynchronize(ev1));
+	MB_CUDA(cudaEventElapsedTime(&r->kernel_ms, ev0, ev1));
+	r->epochs = epochs;
+	return r;
+}
+
+std::unique_ptr<result> run(module& m, const run_config& c)
+{
+	cudaStream_t s = m.ctx->stream;
+	cudaEvent_t t0, t1;
+	MB_CUDA(cudaSetDevice(m.ctx->device));
+	MB_CUDA(cudaEventCreate(&t0));
+	MB_CUDA(cudaEventCreate(&t1));
+	MB_CUDA(cudaEventRecord(t0, s));
+	std::unique_ptr<result> r;
+	{
+		runner rn(m, c);
+		rn.launch(s);
+		r = rn.collect(s);
+	}
+	MB_CUDA(cudaEventRecord(t1, s));
+	MB_CUDA(cudaEventSynchronize(t1));
+	MB_CUDA(cudaEventElapsedTime(&r->total_ms, t0, t1));
+	cudaEventDestroy(t0);
+	cudaEventDestroy(t1);
+	return r;
+}
+
+} // namespace mb

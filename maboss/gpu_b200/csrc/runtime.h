@@ -1,0 +1,198 @@
+// Host runtime of the B200 trajectory engine: device context, NVRTC-compiled model modules,
+// run drivers (fused persistent kernel and buffered epochs) and host-side results.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "codegen.h"
+#include "maboss_b200.h"
+#include "kernels/params.cuh"
+
+namespace mb {
+
+// Status codes (MB_OK, MB_ERR_*) and run modes (MB_MODE_*) come from the C ABI header.
+
+struct engine_error : std::runtime_error
+{
+	int code;
+	engine_error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_throw(cudaError_t e, const char* what);
+#define MB_CUDA(x) ::mb::cuda_throw((x), #x)
+
+// Device memory owned by the runtime.
+struct dbuf
+{
+	void* p = nullptr;
+	size_t bytes = 0;
+	dbuf() = default;
+	explicit dbuf(size_t n) { alloc(n); }
+	dbuf(const dbuf&) = delete;
+	dbuf& operator=(const dbuf&) = delete;
+	dbuf(dbuf&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr, o.bytes = 0; }
+	dbuf& operator=(dbuf&& o) noexcept
+	{
+		std::swap(p, o.p);
+		std::swap(bytes, o.bytes);
+		return *this;
+	}
+	~dbuf();
+	void alloc(size_t n);
+	template <typename T>
+	T* as() const
+	{
+		return static_cast<T*>(p);
+	}
+};
+
+struct context
+{
+	int device = 0;
+	int sm_count = 0;
+	int cc_major = 0, cc_minor = 0;
+	cudaStream_t stream = nullptr; // owned, non-blocking
+	explicit context(int device);
+	~context();
+};
+
+// Kernel handles resolved from an NVRTC-compiled module.
+struct module
+{
+	context* ctx = nullptr;
+	CUmodule mod = nullptr;
+	int state_size = 0, state_words = 0;
+	int noninternal_count = -1; // from the generated code (mbg_noninternal_count), -1 if absent
+	bool has_layout = false; // compiled from a model (full layout known)
+	model_layout layout;
+	std::string source; // generated model source that was compiled with the engine
+	std::string log;	// NVRTC log
+
+	CUfunction fused_exact = nullptr, fused_fast = nullptr;
+	CUfunction init_random = nullptr, init_state = nullptr, sim_epoch = nullptr;
+	CUfunction window_epoch = nullptr, final_epoch = nullptr, fixed_epoch = nullptr;
+	CUfunction compact_count = nullptr, compact_scan = nullptr, compact_scatter = nullptr, fixed_extract = nullptr;
+
+	~module();
+};
+
+// Compile generated model code together with the engine kernels (NVRTC, -arch=sm_100a).
+std::unique_ptr<module> compile_module(context& ctx, const std::string& generated_code);
+// NVRTC compilation only (no device needed): returns the cubin, throws on failure.
+std::vector<char> compile_cubin(const std::string& generated_code, std::string& log);
+
+void launch(CUfunction f, unsigned grid, unsigned block, size_t smem, cudaStream_t s, void** args);
+int occupancy_blocks(CUfunction f, int block, size_t smem);
+
+struct run_config
+{
+	int mode = MB_MODE_FUSED_EXACT;
+	long long sample_count = 0;
+	unsigned long long seed = 0;
+	unsigned long long first_traj = 0; // RNG subsequence of trajectory 0
+	float max_time = 0, time_tick = 0; // exact host floats for window statistics
+	bool discrete_time = false;
+	std::vector<float> istate;
+	std::vector<int> noninternal_nodes;
+	int traj_len = 100;				 // trajectory_len_limit (simulation_runner.cu:51)
+	int batch_limit = 1000000;		 // trajectory_batch_limit (simulation_runner.cu:50)
+	int block = 256;
+	int blocks_per_sm = 0;			 // 0 = occupancy calculator
+	int fixed_capacity_log2 = 0;	 // 0 = automatic
+};
+
+run_config config_from_layout(const model_layout& L, int mode);
+
+struct result
+{
+	int state_size = 0, state_words = 0, n_windows = 0;
+	unsigned n_bins = 0;
+	long long n_traj = 0;
+	bool discrete_time = false;
+	float time_tick = 0, max_time = 0;
+	std::vector<int> noninternal_nodes;
+	double fx = 1, fx_h = 1; // fixed-point scales of win_occ / win_h
+	std::vector<long long> win_occ;
+	std::vector<unsigned> win_cnt;
+	std::vector<long long> win_h;
+	std::vector<unsigned> final_cnt;
+	std::vector<uint32_t> fixed_states; // n_fixed * state_words, sorted like the reference's std::map
+	std::vector<unsigned> fixed_counts;
+	unsigned fixed_overflow = 0;
+	unsigned rate_errors = 0; // trajectories stopped on a non-finite total rate
+	unsigned long long transitions = 0;
+	float kernel_ms = 0; // device time of the simulation kernels
+	float total_ms = 0;	 // device time of the whole run (setup + kernels + result copies)
+	int epochs = 0;
+
+	double window_prob(int w, unsigned bin) const; // window_average_small.cpp:126-140 (fp64)
+	double window_th(int w) const;				   // TH column (window_average_small.cpp:222-223)
+};
+
+// Fixed-point exponents (shared with the oracle so that both convert slices identically).
+int occupancy_exponent(long long n_traj, float tick, bool discrete);
+int entropy_exponent(long long n_traj, float tick, bool discrete);
+
+// Device accumulators of the three built-in statistics plugins (window averages, final
+// states, fixed points) for one run.
+struct stats_state
+{
+	module* mod = nullptr;
+	dbuf occ, cnt, h, fin, fp_keys, fp_counts, fp_states, counters, istate;
+	unsigned fp_cap = 0;
+	int n_windows = 0;
+	unsigned n_bins = 0;
+	bool discrete_time = false;
+	float time_tick = 0, max_time = 0;
+	double fx = 1, fx_h = 1;
+	int h_in_smem = 0;
+	std::vector<int> noninternal_nodes;
+	mb_stats_params p{}; // device pointers + scales passed to the statistics kernels
+
+	void init(module& m, float time_tick, float max_time, bool discrete, const std::vector<int>& noninternal,
+			  long long n_traj, int fixed_capacity_log2, cudaStream_t s);
+	void zero(cudaStream_t s); // clear every accumulator (asynchronous)
+	void set_istate(const std::vector<float>& istate, cudaStream_t s);
+	size_t h_smem() const { return h_in_smem ? (size_t)n_windows * sizeof(long long) : 0; }
+	void window_batch(cudaStream_t s, int n, int stride, int traj_len, const unsigned* traj_states,
+					  const float* traj_times, const float* traj_h);
+	void final_batch(cudaStream_t s, int n, int stride, const unsigned* last_states, const unsigned char* statuses);
+	void fixed_batch(cudaStream_t s, int n, int stride, const unsigned* last_states, const unsigned char* statuses);
+	// counters (u64 view): [0] work counter, [1] transitions, [2] low: fixed-table overflow,
+	// high: extracted fixed points, [3] low: trajectories stopped on a non-finite total rate
+	unsigned long long* next_traj() const { return counters.as<unsigned long long>(); }
+	unsigned long long* transitions() const { return counters.as<unsigned long long>() + 1; }
+	unsigned* fp_overflow_ctr() const { return counters.as<unsigned>() + 4; }
+	unsigned* extract_ctr() const { return counters.as<unsigned>() + 5; }
+	unsigned* error_ctr() const { return counters.as<unsigned>() + 6; }
+	// copy everything back (synchronises the stream)
+	std::unique_ptr<result> finalize(long long n_traj, cudaStream_t s);
+};
+
+// A run whose device buffers are allocated once: launch() zeroes the accumulators and enqueues the
+// simulation on a stream without synchronising (fused modes), collect() copies the results back.
+struct runner
+{
+	module* mod = nullptr;
+	run_config cfg;
+	stats_state st;
+	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+	int epochs = 0;
+	runner(module& m, const run_config& c);
+	~runner();
+	void launch(cudaStream_t s);
+	std::unique_ptr<result> collect(cudaStream_t s);
+	unsigned kernel_launches() const; // engine kernels enqueued by one launch() (fused modes)
+};
+
+// Run a whole simulation with the built-in statistics.
+std::unique_ptr<result> run(module& m, const run_config& cfg);
+
+} // namespace mb

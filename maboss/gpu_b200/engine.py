@@ -1,0 +1,361 @@
+"""Python binding of the B200 trajectory engine (thin layer over the C ABI, no compute here)."""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._lib import check, lib, read_string
+
+MODES = {"exact": 0, "fast": 1, "epoch": 2}
+
+
+class RunConfig(C.Structure):
+    """mb_run_config (include/maboss_b200.h)."""
+
+    _fields_ = [
+        ("mode", C.c_int),
+        ("sample_count", C.c_longlong),
+        ("seed", C.c_ulonglong),
+        ("first_traj", C.c_ulonglong),
+        ("traj_len", C.c_int),
+        ("batch_limit", C.c_int),
+        ("block", C.c_int),
+        ("blocks_per_sm", C.c_int),
+        ("fixed_capacity_log2", C.c_int),
+    ]
+
+
+class Model:
+    """A parsed .bnd/.cfg model (the reference's `driver`)."""
+
+    def __init__(self, bnd_text: str, cfg_text: str):
+        h = C.c_void_p()
+        check(lib().mb_model_parse_text(bnd_text.encode(), cfg_text.encode(), C.byref(h)))
+        self._h = h
+
+    @classmethod
+    def from_files(cls, bnd_path: str, cfg_path: str) -> "Model":
+        self = cls.__new__(cls)
+        h = C.c_void_p()
+        check(lib().mb_model_parse_files(bnd_path.encode(), cfg_path.encode(), C.byref(h)))
+        self._h = h
+        return self
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().mb_model_free(h)
+            self._h = None
+
+    @property
+    def num_nodes(self) -> int:
+        n = C.c_int()
+        check(lib().mb_model_num_nodes(self._h, C.byref(n)))
+        return n.value
+
+    @property
+    def node_names(self) -> list[str]:
+        return [read_string(lib().mb_model_node_name, self._h, i) for i in range(self.num_nodes)]
+
+    def node_info(self, i: int) -> tuple[float, bool]:
+        istate, internal = C.c_float(), C.c_int()
+        check(lib().mb_model_node_info(self._h, i, C.byref(istate), C.byref(internal)))
+        return istate.value, bool(internal.value)
+
+    @property
+    def noninternal_nodes(self) -> list[int]:
+        return [i for i in range(self.num_nodes) if not self.node_info(i)[1]]
+
+    def set_istate(self, i: int, p: float) -> None:
+        check(lib().mb_model_set_istate(self._h, i, p))
+
+    def constant(self, name: str) -> float:
+        v = C.c_float()
+        check(lib().mb_model_get_constant(self._h, name.encode(), C.byref(v)))
+        return v.value
+
+    def set_constant(self, name: str, value: float) -> None:
+        check(lib().mb_model_set_constant(self._h, name.encode(), value))
+
+    def variable(self, name: str) -> float:
+        v = C.c_float()
+        check(lib().mb_model_get_variable(self._h, name.encode(), C.byref(v)))
+        return v.value
+
+    def set_variable(self, name: str, value: float) -> None:
+        check(lib().mb_model_set_variable(self._h, name.encode(), value))
+
+    @property
+    def variables(self) -> dict[str, float]:
+        n = C.c_int()
+        check(lib().mb_model_num_variables(self._h, C.byref(n)))
+        names = [read_string(lib().mb_model_variable_name, self._h, i) for i in range(n.value)]
+        return {k: self.variable(k) for k in names}
+
+    def generate_code(self) -> str:
+        return read_string(lib().mb_model_generate_code, self._h)
+
+
+class Context:
+    """A CUDA device (primary context) and the engine's stream."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib().mb_context_create(device, C.byref(h)))
+        self._h = h
+        self.device = device
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().mb_context_free(h)
+            self._h = None
+
+    @property
+    def stream(self) -> int:
+        s = C.c_void_p()
+        check(lib().mb_context_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    @property
+    def sm_count(self) -> int:
+        n = C.c_int()
+        check(lib().mb_context_sm_count(self._h, C.byref(n)))
+        return n.value
+
+    def compile(self, model: Model) -> "Module":
+        h = C.c_void_p()
+        check(lib().mb_module_compile_model(self._h, model._h, C.byref(h)))
+        return Module(h, self, model)
+
+    def compile_source(self, code: str) -> "Module":
+        h = C.c_void_p()
+        check(lib().mb_module_compile(self._h, code.encode(), C.byref(h)))
+        return Module(h, self, None)
+
+
+class Module:
+    """Kernels of one model, NVRTC-compiled for sm_100a (the reference's kernel_compiler)."""
+
+    def __init__(self, h, ctx: Context, model: Model | None):
+        self._h = h
+        self.ctx = ctx
+        self.model = model
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().mb_module_free(h)
+            self._h = None
+
+    @property
+    def state_size(self) -> tuple[int, int]:
+        n, w = C.c_int(), C.c_int()
+        check(lib().mb_module_state_size(self._h, C.byref(n), C.byref(w)))
+        return n.value, w.value
+
+    def config(self, mode: str = "exact", sample_count: int | None = None, seed: int | None = None,
+               first_traj: int = 0, traj_len: int = 100, batch_limit: int = 1_000_000, block: int = 256,
+               blocks_per_sm: int = 0, fixed_capacity_log2: int = 0) -> RunConfig:
+        cfg = RunConfig()
+        check(lib().mb_run_config_default(self.model._h, C.byref(cfg)))
+        cfg.mode = MODES[mode]
+        if sample_count is not None:
+            cfg.sample_count = sample_count
+        if seed is not None:
+            cfg.seed = seed
+        cfg.first_traj = first_traj
+        cfg.traj_len = traj_len
+        cfg.batch_limit = batch_limit
+        cfg.block = block
+        cfg.blocks_per_sm = blocks_per_sm
+        cfg.fixed_capacity_log2 = fixed_capacity_log2
+        return cfg
+
+    def run(self, mode: str = "exact", sample_count: int | None = None, **kw) -> "Result":
+        """simulation_runner::run_simulation with the built-in statistics (synchronous)."""
+        cfg = self.config(mode, sample_count, **kw)
+        h = C.c_void_p()
+        check(lib().mb_run(self._h, C.byref(cfg), C.byref(h)))
+        return Result(h)
+
+    def runner(self, mode: str = "exact", sample_count: int | None = None, **kw) -> "Runner":
+        """Buffers allocated once; launch() is asynchronous on the context's stream."""
+        cfg = self.config(mode, sample_count, **kw)
+        h = C.c_void_p()
+        check(lib().mb_runner_create(self._h, C.byref(cfg), C.byref(h)))
+        return Runner(h, self, cfg)
+
+    # -- kernel entry points on caller-owned device buffers (integer device addresses)
+    def launch_initialize_random(self, n: int, seed: int, first: int, rands: int, stream: int = 0) -> None:
+        check(lib().mb_launch_initialize_random(self._h, stream or None, n, seed, first, rands))
+
+    def launch_initialize_initial_state(self, n: int, stride: int, istate: int, last_states: int,
+                                        last_times: int, rands: int, stream: int = 0) -> None:
+        check(lib().mb_launch_initialize_initial_state(self._h, stream or None, n, stride, istate, last_states,
+                                                        last_times, rands))
+
+    def launch_simulate(self, n: int, stride: int, traj_len: int, last_states: int, last_times: int, rands: int,
+                        traj_states: int, traj_times: int, traj_h: int, statuses: int, transitions: int,
+                        stream: int = 0) -> None:
+        check(lib().mb_launch_simulate(self._h, stream or None, n, stride, traj_len, last_states, last_times, rands,
+                                       traj_states, traj_times, traj_h, statuses, transitions))
+
+    def stats(self, time_tick: float, max_time: float, discrete: bool, noninternal: list[int],
+              sample_count: int) -> "Stats":
+        arr = (C.c_int * max(1, len(noninternal)))(*noninternal)
+        h = C.c_void_p()
+        check(lib().mb_stats_create(self._h, time_tick, max_time, int(discrete), arr, len(noninternal),
+                                    sample_count, C.byref(h)))
+        return Stats(h, self)
+
+
+class Runner:
+    def __init__(self, h, mod: Module, cfg: RunConfig):
+        self._h = h
+        self.mod = mod
+        self.cfg = cfg
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().mb_runner_free(h)
+            self._h = None
+
+    def launch(self, stream: int = 0) -> None:
+        check(lib().mb_runner_launch(self._h, stream or None))
+
+    def result(self, stream: int = 0) -> "Result":
+        h = C.c_void_p()
+        check(lib().mb_runner_result(self._h, stream or None, C.byref(h)))
+        return Result(h)
+
+    @property
+    def kernel_launches(self) -> int:
+        n = C.c_uint()
+        check(lib().mb_runner_kernel_launches(self._h, C.byref(n)))
+        return n.value
+
+
+def rand_state_size() -> int:
+    return int(lib().mb_rand_state_size())
+
+
+class Stats:
+    """Device accumulators of the window / final / fixed statistics plugins."""
+
+    def __init__(self, h, mod: Module):
+        self._h = h
+        self.mod = mod
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().mb_stats_free(h)
+            self._h = None
+
+    def window(self, n, stride, traj_len, traj_states, traj_times, traj_h, stream: int = 0):
+        check(lib().mb_launch_window_average_stats(self._h, stream or None, n, stride, traj_len, traj_states,
+                                                   traj_times, traj_h))
+
+    def final(self, n, stride, last_states, statuses, stream: int = 0):
+        check(lib().mb_launch_final_states_stats(self._h, stream or None, n, stride, last_states, statuses))
+
+    def fixed(self, n, stride, last_states, statuses, stream: int = 0):
+        check(lib().mb_launch_fixed_states_stats(self._h, stream or None, n, stride, last_states, statuses))
+
+    def finalize(self, n_trajectories: int) -> "Result":
+        h = C.c_void_p()
+        check(lib().mb_stats_finalize(self._h, n_trajectories, C.byref(h)))
+        return Result(h)
+
+
+@dataclass
+class Dims:
+    windows: int
+    bins: int
+    noninternal: int
+    state_words: int
+    nodes: int
+
+
+class Result:
+    """Statistics of one run (window probabilities, entropies, final states, fixed points)."""
+
+    def __init__(self, h):
+        self._h = h
+        w, b, k, sw, n = (C.c_int() for _ in range(5))
+        check(lib().mb_result_dims(h, C.byref(w), C.byref(b), C.byref(k), C.byref(sw), C.byref(n)))
+        self.dims = Dims(w.value, b.value, k.value, sw.value, n.value)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().mb_result_free(h)
+            self._h = None
+
+    @property
+    def transitions(self) -> int:
+        t = C.c_ulonglong()
+        check(lib().mb_result_transitions(self._h, C.byref(t)))
+        return t.value
+
+    @property
+    def timing(self) -> tuple[float, float, int]:
+        k, t, e = C.c_float(), C.c_float(), C.c_int()
+        check(lib().mb_result_timing(self._h, C.byref(k), C.byref(t), C.byref(e)))
+        return k.value, t.value, e.value
+
+    @property
+    def window_probs(self) -> np.ndarray:
+        out = np.zeros((self.dims.windows, self.dims.bins), np.float64)
+        check(lib().mb_result_window_probs(self._h, out.ctypes.data))
+        return out
+
+    @property
+    def window_entropy(self) -> np.ndarray:
+        out = np.zeros(self.dims.windows, np.float64)
+        check(lib().mb_result_window_entropy(self._h, out.ctypes.data))
+        return out
+
+    def raw(self) -> dict:
+        T, S = self.dims.windows, self.dims.bins
+        occ = np.zeros(T * S, np.int64)
+        cnt = np.zeros(T * S, np.uint32)
+        h = np.zeros(T, np.int64)
+        eo, eh = C.c_int(), C.c_int()
+        check(lib().mb_result_window_raw(self._h, occ.ctypes.data, cnt.ctypes.data, h.ctypes.data,
+                                         C.byref(eo), C.byref(eh)))
+        return dict(occ=occ.reshape(T, S), cnt=cnt.reshape(T, S), h=h, occ_exp=eo.value, ent_exp=eh.value)
+
+    @property
+    def final_counts(self) -> np.ndarray:
+        out = np.zeros(self.dims.bins, np.uint32)
+        check(lib().mb_result_final_counts(self._h, out.ctypes.data))
+        return out
+
+    @property
+    def fixed_overflow(self) -> int:
+        n, o = C.c_int(), C.c_uint()
+        check(lib().mb_result_num_fixed(self._h, C.byref(n), C.byref(o)))
+        return o.value
+
+    @property
+    def fixed(self) -> list[tuple[np.ndarray, int]]:
+        n, o = C.c_int(), C.c_uint()
+        check(lib().mb_result_num_fixed(self._h, C.byref(n), C.byref(o)))
+        out = []
+        for i in range(n.value):
+            st = np.zeros(self.dims.state_words, np.uint32)
+            c = C.c_uint()
+            check(lib().mb_result_fixed(self._h, i, st.ctypes.data, C.byref(c)))
+            out.append((st, c.value))
+        return out
+
+    def write_csv(self, model: Model, prefix: str) -> None:
+        check(lib().mb_result_write_csv(self._h, model._h, prefix.encode()))
+
+    def visualize(self, model: Model) -> str:
+        return read_string(lib().mb_result_visualize, self._h, model._h)

@@ -1,0 +1,1245 @@
+// CPU ORACLE -- test infrastructure only. Not part of the product, never called by it.
+//
+// A plain C++/OpenMP restatement of the reference MaBoSS.GPU trajectory path, used to check the
+// CUDA engine (tests/, __graft_entry__.smoke) and as the CPU baseline of bench.py. It has its own
+// model parser and its own evaluator of the generated-code semantics, written independently of
+// the engine's front-end. Every function cites the reference file:line it restates (paths
+// relative to the reference project).
+//
+// Parity pins: the oracle's window probabilities, final states and fixed points are checked
+// against the reference's golden outputs test/{cellcycle,sizek,metastasis,Montagud2022_Prostate_Cancer}.res
+// (statistically, 4 sigma; tests/test_oracle_golden.py).
+//
+// Random numbers: curand's XORWOW generator through its header-only device API compiled for
+// the host (curand_init(seed, trajectory, 0), curand_uniform), so the streams are the ones the
+// GPU draws. Waiting times use the host logf; the device logf may differ in the last ulp, so
+// continuous-time times can differ by a few ulps from the GPU while flips, steps and states agree.
+//
+// Modes: 0 = exact (reference semantics incl. the 100-slot epoch boundary), 1 = fast (Philox
+// streams, no epoch boundary, entropy via sum r*log2 r), mirroring the engine's two fused modes.
+#include <curand_kernel.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cctype>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// ------------------------------------------------------------------ expressions
+
+enum class K
+{
+	num,
+	node,
+	var,
+	alias,
+	un,
+	bin,
+	tern,
+	paren
+};
+
+struct E
+{
+	K k = K::num;
+	float v = 0;
+	std::string s;
+	char op = 0; // '+','-','*','/','&','|','^','!','=' (==),'n' (!=),'<','l' (<=),'>','g' (>=)
+	std::shared_ptr<E> a, b, c;
+};
+using P = std::shared_ptr<E>;
+
+struct node_def
+{
+	std::string name;
+	std::vector<std::pair<std::string, P>> attrs;
+	float istate = 0.5f;
+	P attr(const std::string& n) const
+	{
+		for (auto& a : attrs)
+			if (a.first == n)
+				return a.second; // first attribute wins (parse_types.cpp:6-13)
+		return nullptr;
+	}
+};
+
+struct model
+{
+	std::map<std::string, float> vars, consts;
+	std::vector<node_def> nodes;
+	int index(const std::string& n) const
+	{
+		for (size_t i = 0; i < nodes.size(); i++)
+			if (nodes[i].name == n)
+				return (int)i;
+		return -1;
+	}
+};
+
+// float evaluation (expressions.cpp evaluate methods)
+float feval(const model& m, const E& e)
+{
+	switch (e.k)
+	{
+		case K::num: return e.v;
+		case K::var:
+		{
+			auto it = m.vars.find(e.s);
+			if (it == m.vars.end())
+				throw std::runtime_error("unknown variable " + e.s);
+			return it->second;
+		}
+		case K::paren: return feval(m, *e.a);
+		case K::tern: return feval(m, *e.a) ? feval(m, *e.b) : feval(m, *e.c);
+		case K::un:
+			if (e.op == '-')
+				return -feval(m, *e.a);
+			if (e.op == '!')
+				return !feval(m, *e.a);
+			return feval(m, *e.a);
+		case K::bin:
+		{
+			float x = feval(m, *e.a);
+			switch (e.op)
+			{
+				case '&': return x && feval(m, *e.b);
+				case '|': return x || feval(m, *e.b);
+				default: break;
+			}
+			float y = feval(m, *e.b);
+			switch (e.op)
+			{
+				case '+': return x + y;
+				case '-': return x - y;
+				case '*': return x * y;
+				case '/': return x / y;
+				case '^': return (x != 0) != (y != 0);
+				case '=': return x == y;
+				case 'n': return x != y;
+				case '<': return x < y;
+				case 'l': return x <= y;
+				case '>': return x > y;
+				case 'g': return x >= y;
+			}
+			throw std::runtime_error("bad operator");
+		}
+		default: throw std::runtime_error("node or alias in a constant expression");
+	}
+}
+
+bool is_const(const model& m, const E& e)
+{
+	if (e.k == K::node || e.k == K::alias)
+		return false;
+	if (e.k == K::var)
+		return m.vars.count(e.s) != 0;
+	return (!e.a || is_const(m, *e.a)) && (!e.b || is_const(m, *e.b)) && (!e.c || is_const(m, *e.c));
+}
+
+// ---- C semantics of the generated CUDA code (generator.cpp + expressions.cpp generate_code):
+// a literal or $variable is printed with 6 significant digits; the text is an int literal unless
+// it has '.', 'e', "inf" or "nan"; identifiers become bool, & | ^ ! comparisons give int.
+struct tv
+{
+	bool dbl = false;
+	double d = 0;
+	long long i = 0;
+	double get() const { return dbl ? d : (double)i; }
+	bool truth() const { return dbl ? d != 0 : i != 0; }
+};
+
+tv printed(float v)
+{
+	char buf[64];
+	std::snprintf(buf, sizeof buf, "%g", (double)v);
+	tv r;
+	if (std::strpbrk(buf, ".eEnNiI"))
+	{
+		r.dbl = true;
+		r.d = std::strtod(buf, nullptr);
+	}
+	else
+		r.i = std::strtoll(buf, nullptr, 10);
+	return r;
+}
+
+// ------------------------------------------------------------------ parser (scanner.ll, parser.yy)
+
+struct tok
+{
+	char t = 0; // 'i' ident, 'v' $var, 'a' @alias, 'f' float, 'd' int, 'E' end, else punctuation code
+	std::string s;
+	double num = 0;
+	int line = 1;
+};
+
+struct lex
+{
+	std::string src;
+	size_t p = 0;
+	int line = 1;
+	tok next()
+	{
+		for (;;)
+		{
+			while (p < src.size() && std::strchr(" \t\r\n", src[p]))
+				line += src[p++] == '\n';
+			if (p + 1 < src.size() && src[p] == '/' && src[p + 1] == '/')
+			{
+				while (p < src.size() && src[p] != '\n')
+					p++;
+				continue;
+			}
+			break;
+		}
+		tok k;
+		k.line = line;
+		if (p >= src.size())
+		{
+			k.t = 'E';
+			return k;
+		}
+		char c = src[p];
+		auto alpha = [](char x) { return std::isalpha((unsigned char)x) != 0; };
+		auto digit = [](char x) { return std::isdigit((unsigned char)x) != 0; };
+		if (digit(c) || (c == '.' && p + 1 < src.size() && digit(src[p + 1])))
+		{
+			size_t q = p;
+			bool f = false;
+			while (q < src.size() && digit(src[q]))
+				q++;
+			if (q < src.size() && src[q] == '.')
+			{
+				f = true;
+				q++;
+				while (q < src.size() && digit(src[q]))
+					q++;
+			}
+			if (q < src.size() && (src[q] == 'e' || src[q] == 'E'))
+			{
+				size_t r = q + 1;
+				if (r < src.size() && (src[r] == '+' || src[r] == '-'))
+					r++;
+				if (r < src.size() && digit(src[r]))
+				{
+					while (r < src.size() && digit(src[r]))
+						r++;
+					q = r;
+					f = true;
+				}
+			}
+			k.s = src.substr(p, q - p);
+			k.t = f ? 'f' : 'd';
+			k.num = f ? (double)(float)std::strtod(k.s.c_str(), nullptr) : (double)std::strtol(k.s.c_str(), nullptr, 10);
+			p = q;
+			return k;
+		}
+		if (alpha(c) || ((c == '$' || c == '@') && p + 1 < src.size() && alpha(src[p + 1])))
+		{
+			size_t q = p + 1;
+			while (q < src.size() && (alpha(src[q]) || digit(src[q]) || src[q] == '_'))
+				q++;
+			k.s = src.substr(p, q - p);
+			p = q;
+			std::string low = k.s;
+			for (auto& ch : low)
+				ch = (char)std::tolower((unsigned char)ch);
+			k.t = c == '$' ? 'v' : c == '@' ? 'a' : 'i';
+			if (k.t == 'i')
+			{
+				if (low == "and")
+					k.t = '&';
+				else if (low == "or")
+					k.t = '|';
+				else if (low == "xor")
+					k.t = '^';
+				else if (low == "not")
+					k.t = '!';
+				else if (low == "true" || low == "false")
+				{
+					k.t = 'd';
+					k.num = low == "true";
+				}
+			}
+			return k;
+		}
+		auto two = [&](const char* o) { return p + 1 < src.size() && src[p] == o[0] && src[p + 1] == o[1]; };
+		if (two("&&") || two("||"))
+		{
+			k.t = src[p];
+			p += 2;
+			return k;
+		}
+		if (two("=="))
+			k.t = '=';
+		else if (two("!="))
+			k.t = 'n';
+		else if (two("<="))
+			k.t = 'l';
+		else if (two(">="))
+			k.t = 'g';
+		if (k.t)
+		{
+			p += 2;
+			return k;
+		}
+		if (std::strchr("-+*/()=?:&|^!<>{}.;[],", c))
+		{
+			k.t = c == '=' ? 'A' : c; // single '=' is assignment
+			p++;
+			return k;
+		}
+		throw std::runtime_error("line " + std::to_string(line) + ": invalid character " + std::string(1, c));
+	}
+};
+
+struct parser
+{
+	lex L;
+	tok cur;
+	model& m;
+	parser(const std::string& s, model& mm) : m(mm)
+	{
+		L.src = s;
+		cur = L.next();
+	}
+	[[noreturn]] void err(const std::string& what)
+	{
+		throw std::runtime_error("line " + std::to_string(cur.line) + ": " + what);
+	}
+	tok take(char t)
+	{
+		if (cur.t != t)
+			err(std::string("expected '") + t + "'");
+		tok k = cur;
+		cur = L.next();
+		return k;
+	}
+	static int prec(char t)
+	{
+		switch (t)
+		{
+			case '^': return 1;
+			case '|': return 2;
+			case '&': return 3;
+			case '=':
+			case 'n': return 4;
+			case '<':
+			case 'l':
+			case '>':
+			case 'g': return 5;
+			case '+':
+			case '-': return 6;
+			case '*':
+			case '/': return 7;
+		}
+		return 0;
+	}
+	P mk(K k)
+	{
+		auto e = std::make_shared<E>();
+		e->k = k;
+		return e;
+	}
+	P atom()
+	{
+		tok t = cur;
+		if (t.t == '-' || t.t == '+' || t.t == '!')
+		{
+			cur = L.next();
+			P e = mk(K::un);
+			e->op = t.t;
+			e->a = atom();
+			return e;
+		}
+		cur = L.next();
+		P e;
+		switch (t.t)
+		{
+			case 'f':
+			case 'd':
+				e = mk(K::num);
+				e->v = (float)t.num;
+				return e;
+			case 'i': e = mk(K::node); break;
+			case 'v': e = mk(K::var); break;
+			case 'a': e = mk(K::alias); break;
+			case '(':
+				e = mk(K::paren);
+				e->a = expr();
+				take(')');
+				return e;
+			default: err("unexpected token in expression");
+		}
+		e->s = t.s;
+		return e;
+	}
+	P binary(int minp)
+	{
+		P l = atom();
+		for (;;)
+		{
+			int p = prec(cur.t);
+			if (!p || p < minp)
+				return l;
+			char op = cur.t;
+			cur = L.next();
+			P r = binary(p + 1);
+			P e = mk(K::bin);
+			e->op = op;
+			e->a = l;
+			e->b = r;
+			l = e;
+		}
+	}
+	P expr()
+	{
+		P c = binary(1);
+		if (cur.t != '?')
+			return c;
+		cur = L.next();
+		P e = mk(K::tern);
+		e->a = c;
+		e->b = expr();
+		take(':');
+		e->c = expr();
+		return e;
+	}
+	void bnd()
+	{
+		while (cur.t != 'E')
+		{
+			tok kw = take('i');
+			std::string low = kw.s;
+			for (auto& ch : low)
+				ch = (char)std::tolower((unsigned char)ch);
+			if (low != "node")
+				err("expected 'node'");
+			node_def n;
+			n.name = take('i').s;
+			take('{');
+			do
+			{
+				std::string an = take('i').s;
+				take('A');
+				P e = expr();
+				take(';');
+				n.attrs.emplace_back(an, e);
+			} while (cur.t == 'i');
+			take('}');
+			if (m.index(n.name) >= 0)
+				err("duplicate node " + n.name);
+			if (!n.attr("rate_up") || !n.attr("rate_down"))
+				err("node " + n.name + " lacks rate_up/rate_down");
+			m.nodes.push_back(n);
+		}
+	}
+	void cfg()
+	{
+		while (cur.t != 'E')
+		{
+			if (cur.t == 'v')
+			{
+				std::string n = take('v').s;
+				take('A');
+				P e = expr();
+				take(';');
+				m.vars[n] = feval(m, *e);
+			}
+			else if (cur.t == 'i')
+			{
+				std::string n = take('i').s;
+				if (cur.t == '.')
+				{
+					take('.');
+					std::string a = take('i').s;
+					take('A');
+					P e = expr();
+					take(';');
+					int i = m.index(n);
+					if (i < 0)
+						err("unknown node " + n);
+					if (a == "istate")
+						m.nodes[i].istate = feval(m, *e);
+					else
+						m.nodes[i].attrs.emplace_back(a, e);
+				}
+				else
+				{
+					take('A');
+					P e = expr();
+					take(';');
+					m.consts[n] = feval(m, *e);
+				}
+			}
+			else if (cur.t == '[')
+			{
+				take('[');
+				std::string n = take('i').s;
+				take(']');
+				take('.');
+				if (take('i').s != "istate")
+					err("expected istate");
+				take('A');
+				P l = expr();
+				take('[');
+				int il = (int)take('d').num;
+				take(']');
+				take(',');
+				P r = expr();
+				take('[');
+				int ir = (int)take('d').num;
+				take(']');
+				take(';');
+				if (!((il == 0 && ir == 1) || (il == 1 && ir == 0)))
+					err("numbers in [] must be 0 and 1");
+				int i = m.index(n);
+				if (i < 0)
+					err("unknown node " + n);
+				float a = feval(m, *l), b = feval(m, *r);
+				m.nodes[i].istate = il == 1 ? a / (a + b) : b / (a + b);
+			}
+			else
+				err("unexpected token");
+		}
+	}
+};
+
+// ------------------------------------------------------------------ compiled model
+
+// Flattened expression with identifiers resolved to node indices, $variables and literals
+// resolved to their printed C literal (int or double), and @aliases inlined.
+struct flat
+{
+	struct op_t
+	{
+		K k;
+		char op;
+		int node;
+		tv lit;
+		int a, b, c;
+	};
+	std::vector<op_t> ops;
+	int root = -1;
+
+	int add(const model& m, const E& e, int self, int depth = 0)
+	{
+		if (depth > 64)
+			throw std::runtime_error("alias recursion");
+		op_t o{ e.k, e.op, -1, tv{}, -1, -1, -1 };
+		switch (e.k)
+		{
+			case K::num: o.lit = printed(e.v); break;
+			case K::var:
+				o.k = K::num;
+				o.lit = printed(m.vars.at(e.s));
+				break;
+			case K::node:
+				o.node = m.index(e.s);
+				if (o.node < 0)
+					throw std::runtime_error("unknown node " + e.s);
+				break;
+			case K::alias:
+			{
+				P a = m.nodes[self].attr(e.s.substr(1));
+				if (!a)
+					throw std::runtime_error("missing attribute " + e.s);
+				return add(m, *a, self, depth + 1);
+			}
+			case K::paren: return add(m, *e.a, self, depth);
+			default:
+				o.a = e.a ? add(m, *e.a, self, depth) : -1;
+				o.b = e.b ? add(m, *e.b, self, depth) : -1;
+				o.c = e.c ? add(m, *e.c, self, depth) : -1;
+		}
+		ops.push_back(o);
+		return (int)ops.size() - 1;
+	}
+
+	tv eval(int i, const uint32_t* s) const
+	{
+		const op_t& o = ops[i];
+		switch (o.k)
+		{
+			case K::num: return o.lit;
+			case K::node:
+			{
+				tv r;
+				r.i = (s[o.node / 32] >> (o.node % 32)) & 1u;
+				return r;
+			}
+			case K::tern:
+			{
+				tv c = eval(o.a, s), x = eval(o.b, s), y = eval(o.c, s);
+				tv r = c.truth() ? x : y;
+				if (x.dbl || y.dbl)
+				{
+					r.d = r.get();
+					r.dbl = true;
+				}
+				return r;
+			}
+			case K::un:
+			{
+				tv x = eval(o.a, s);
+				if (o.op == '-')
+				{
+					x.d = -x.d;
+					x.i = -x.i;
+				}
+				else if (o.op == '!')
+				{
+					tv r;
+					r.i = x.truth() ? 0 : 1;
+					return r;
+				}
+				return x;
+			}
+			case K::bin:
+			{
+				tv x = eval(o.a, s), y = eval(o.b, s), r;
+				const bool dbl = x.dbl || y.dbl;
+				switch (o.op)
+				{
+					case '+':
+					case '-':
+					case '*':
+					case '/':
+						if (dbl)
+						{
+							r.dbl = true;
+							double p = x.get(), q = y.get();
+							r.d = o.op == '+' ? p + q : o.op == '-' ? p - q : o.op == '*' ? p * q : p / q;
+						}
+						else
+						{
+							if (o.op == '/' && y.i == 0)
+								throw std::runtime_error("integer division by zero in a rate");
+							r.i = o.op == '+' ? x.i + y.i : o.op == '-' ? x.i - y.i : o.op == '*' ? x.i * y.i : x.i / y.i;
+						}
+						return r;
+					case '&':
+					case '|':
+					case '^':
+						if (dbl)
+							throw std::runtime_error("bitwise operator on a floating-point operand");
+						r.i = o.op == '&' ? (x.i & y.i) : o.op == '|' ? (x.i | y.i) : (x.i ^ y.i);
+						return r;
+					default:
+					{
+						bool v;
+						if (dbl)
+						{
+							double p = x.get(), q = y.get();
+							v = o.op == '=' ? p == q : o.op == 'n' ? p != q : o.op == '<' ? p < q : o.op == 'l' ? p <= q
+								: o.op == '>' ? p > q : p >= q;
+						}
+						else
+						{
+							long long p = x.i, q = y.i;
+							v = o.op == '=' ? p == q : o.op == 'n' ? p != q : o.op == '<' ? p < q : o.op == 'l' ? p <= q
+								: o.op == '>' ? p > q : p >= q;
+						}
+						r.i = v;
+						return r;
+					}
+				}
+			}
+			default: throw std::runtime_error("bad flat expression");
+		}
+	}
+	tv eval(const uint32_t* s) const { return eval(root, s); }
+};
+
+struct compiled
+{
+	model m;
+	int N = 0, W = 0;
+	std::vector<int> ni;			// non-internal nodes in order
+	std::vector<char> fast;			// fast-path form (generator.cpp:57-82)
+	std::vector<float> up, down;	// fast-path rate values as compiled
+	std::vector<float> ul, dl;		// r * log2(r) constants of the fast-mode entropy
+	std::vector<flat> logic, rup, rdown;
+	// truth tables of fast-path logic (exactly the flat evaluation, tabulated over the inputs)
+	std::vector<std::vector<int>> tt_in;
+	std::vector<std::vector<uint64_t>> tt;
+	bool nonneg = true;
+	bool discrete = false;
+	float max_time_f = 0, tick_f = 0;	  // exact floats (window statistics)
+	float max_time_sim = 0, tick_sim = 0; // 6-significant-digit constexprs used by simulate
+	long long sample_count = 0;
+	unsigned long long seed = 0;
+	int T = 0;
+
+	float constant(const char* n) const
+	{
+		auto it = m.consts.find(n);
+		return it == m.consts.end() ? 0.f : it->second;
+	}
+
+	bool logic_ternary(const P& e, bool is_up, float& val) const
+	{
+		if (!e || e->k != K::tern || e->a->k != K::alias || e->a->s != "@logic")
+			return false;
+		if (!is_const(m, *e->b) || !is_const(m, *e->c))
+			return false;
+		float l = feval(m, *e->b), r = feval(m, *e->c);
+		val = is_up ? l : r;
+		return (is_up ? r : l) == 0.f;
+	}
+
+	// <node>_rate of the generated code (generator.cpp:84-122)
+	float rate(int i, const uint32_t* s) const
+	{
+		const bool is_up = (s[i / 32] >> (i % 32)) & 1u;
+		if (fast[i])
+		{
+			bool lg;
+			if (!tt[i].empty())
+			{
+				unsigned p = 0;
+				const std::vector<int>& in = tt_in[i];
+				for (size_t k = 0; k < in.size(); k++)
+					p |= ((s[in[k] / 32] >> (in[k] % 32)) & 1u) << k;
+				lg = (tt[i][p >> 6] >> (p & 63)) & 1u;
+			}
+			else
+				lg = logic[i].eval(s).truth();
+			return is_up == lg ? 0.f : (is_up ? down[i] : up[i]);
+		}
+		tv r = is_up ? rdown[i].eval(s) : rup[i].eval(s);
+		return (float)r.get();
+	}
+
+	uint32_t ni_index(const uint32_t* s) const
+	{
+		uint32_t idx = 0;
+		for (size_t k = 0; k < ni.size(); k++)
+			idx |= ((s[ni[k] / 32] >> (ni[k] % 32)) & 1u) << k;
+		return idx;
+	}
+};
+
+float print6(float v)
+{
+	char buf[64];
+	std::snprintf(buf, sizeof buf, "%g", (double)v);
+	return (float)std::strtod(buf, nullptr);
+}
+
+std::unique_ptr<compiled> compile(const std::string& bnd, const std::string& cfg)
+{
+	auto c = std::make_unique<compiled>();
+	model& m = c->m;
+	m.consts["discrete_time"] = 0; // driver.cpp:7-14
+	m.consts["sample_count"] = 1000000;
+	m.consts["max_time"] = 10;
+	m.consts["time_tick"] = 0.1f;
+	m.consts["seed_pseudorandom"] = 0;
+	parser(bnd, m).bnd();
+	parser(cfg, m).cfg();
+	c->N = (int)m.nodes.size();
+	c->W = (c->N + 31) / 32;
+	c->fast.assign(c->N, 0);
+	c->up.assign(c->N, 0);
+	c->down.assign(c->N, 0);
+	c->ul.assign(c->N, 0);
+	c->dl.assign(c->N, 0);
+	for (int i = 0; i < c->N; i++)
+	{
+		const node_def& n = m.nodes[i];
+		P internal = n.attr("is_internal");
+		if (!(internal && feval(m, *internal) != 0.f))
+			c->ni.push_back(i);
+		float u = 0, d = 0;
+		const bool f =
+			n.attr("logic") && c->logic_ternary(n.attr("rate_up"), true, u) && c->logic_ternary(n.attr("rate_down"), false, d);
+		c->fast[i] = f;
+		if (f)
+		{
+			c->up[i] = (float)printed(u).get();
+			c->down[i] = (float)printed(d).get();
+			c->ul[i] = c->up[i] > 0 ? (float)((double)c->up[i] * std::log2((double)c->up[i])) : 0.f;
+			c->dl[i] = c->down[i] > 0 ? (float)((double)c->down[i] * std::log2((double)c->down[i])) : 0.f;
+			if (!(c->up[i] >= 0) || !(c->down[i] >= 0))
+				c->nonneg = false;
+		}
+		else
+			c->nonneg = false;
+	}
+	c->logic.resize(c->N);
+	c->rup.resize(c->N);
+	c->rdown.resize(c->N);
+	for (int i = 0; i < c->N; i++)
+	{
+		const node_def& n = m.nodes[i];
+		if (c->fast[i])
+			c->logic[i].root = c->logic[i].add(m, *n.attr("logic"), i);
+		else
+		{
+			c->rup[i].root = c->rup[i].add(m, *n.attr("rate_up"), i);
+			c->rdown[i].root = c->rdown[i].add(m, *n.attr("rate_down"), i);
+		}
+	}
+	c->tt_in.resize(c->N);
+	c->tt.resize(c->N);
+	for (int i = 0; i < c->N; i++)
+	{
+		if (!c->fast[i])
+			continue;
+		std::vector<int> in;
+		for (auto& o : c->logic[i].ops)
+			if (o.k == K::node && std::find(in.begin(), in.end(), o.node) == in.end())
+				in.push_back(o.node);
+		if (in.size() > 16)
+			continue;
+		std::vector<uint64_t> t(((1u << in.size()) + 63) / 64, 0);
+		std::vector<uint32_t> st(c->W, 0u);
+		for (unsigned p = 0; p < (1u << in.size()); p++)
+		{
+			for (size_t k = 0; k < in.size(); k++)
+			{
+				const uint32_t bit = 1u << (in[k] % 32);
+				st[in[k] / 32] = (p >> k) & 1u ? (st[in[k] / 32] | bit) : (st[in[k] / 32] & ~bit);
+			}
+			if (c->logic[i].eval(st.data()).truth())
+				t[p >> 6] |= 1ull << (p & 63);
+		}
+		c->tt_in[i] = in;
+		c->tt[i] = t;
+	}
+	c->discrete = c->constant("discrete_time") != 0;
+	c->max_time_f = c->constant("max_time");
+	c->tick_f = c->constant("time_tick");
+	c->max_time_sim = print6(c->max_time_f);
+	c->tick_sim = print6(c->tick_f);
+	c->sample_count = (long long)c->constant("sample_count");
+	c->seed = (unsigned long long)c->constant("seed_pseudorandom");
+	c->T = (int)std::ceil(c->max_time_f / c->tick_f);
+	return c;
+}
+
+// ------------------------------------------------------------------ simulation
+
+struct sinks
+{
+	int T = 0;
+	uint32_t S = 0;
+	double fx = 1, fxh = 1;
+	std::vector<long long> occ, h;
+	std::vector<unsigned> cnt, fin;
+	std::map<std::vector<uint32_t>, unsigned> fixed;
+	unsigned long long transitions = 0;
+};
+
+template <typename T>
+void atomic_add(T* p, T v)
+{
+	__atomic_fetch_add(p, v, __ATOMIC_RELAXED);
+}
+
+struct run_acc
+{
+	int ow = -1;
+	uint32_t oi = 0;
+	long long oq = 0;
+	int hw = -1;
+	long long hq = 0;
+	void flush(sinks& s)
+	{
+		if (ow >= 0 && oq)
+			atomic_add(&s.occ[(size_t)ow * s.S + oi], oq);
+		if (hw >= 0 && hq)
+			atomic_add(&s.h[hw], hq);
+		ow = hw = -1;
+		oq = hq = 0;
+	}
+};
+
+// window_average_small.cu:66-92 (continuous) and :117-130 (discrete)
+void record(const compiled& c, sinks& s, run_acc& a, uint32_t idx, float t0, float t1, float h)
+{
+	if (t1 == 0.f)
+		return;
+	if (c.discrete)
+	{
+		const int w = (int)lroundf(t0 / c.tick_f);
+		if (w >= 0 && w < s.T)
+		{
+			atomic_add(&s.cnt[(size_t)w * s.S + idx], 1u);
+			long long q = llrint((double)h * s.fxh);
+			if (q)
+				atomic_add(&s.h[w], q);
+		}
+		return;
+	}
+	float sb = t0;
+	int w = (int)floorf(sb / c.tick_f);
+	for (int guard = 0; t1 > sb && guard <= s.T + 2; guard++)
+	{
+		const float we = (float)(w + 1) * c.tick_f;
+		const float se = std::fmin(t1, we);
+		const float sl = se - sb;
+		if (w >= 0 && w < s.T)
+		{
+			const long long q = llrint((double)sl * s.fx);
+			if (w == a.ow && idx == a.oi)
+				a.oq += q;
+			else
+			{
+				if (a.ow >= 0 && a.oq)
+					atomic_add(&s.occ[(size_t)a.ow * s.S + a.oi], a.oq);
+				a.ow = w;
+				a.oi = idx;
+				a.oq = q;
+			}
+			const float hs = h * sl;
+			const long long hq = llrint((double)hs * s.fxh);
+			if (w == a.hw)
+				a.hq += hq;
+			else
+			{
+				if (a.hw >= 0 && a.hq)
+					atomic_add(&s.h[a.hw], a.hq);
+				a.hw = w;
+				a.hq = hq;
+			}
+		}
+		w++;
+		sb = se;
+	}
+}
+
+// compute_transition_entropy over the rates of one step (generator.cpp:146-175)
+float entropy_exact(const compiled& c, const float* rates)
+{
+	float tot = 0.f;
+	for (int i : c.ni)
+		tot += rates[i];
+	if (tot == 0.f)
+		return 0.f;
+	float e = 0.f;
+	for (int i : c.ni)
+	{
+		const float p = rates[i] / tot;
+		e -= (p == 0.f) ? 0.f : log2f(p) * p;
+	}
+	return e;
+}
+
+// fast-mode entropy: log2(S) - (sum r log2 r) / S with r log2 r from per-node constants
+float entropy_fast(const compiled& c, const float* rates, const uint32_t* s)
+{
+	float t = 0.f, tl = 0.f;
+	for (int i : c.ni)
+	{
+		const float r = rates[i];
+		if (c.fast[i])
+		{
+			if (r != 0.f)
+			{
+				const bool up = (s[i / 32] >> (i % 32)) & 1u;
+				t += up ? c.down[i] : c.up[i];
+				tl += up ? c.dl[i] : c.ul[i];
+			}
+		}
+		else
+		{
+			t += r;
+			tl += (r > 0.f) ? r * log2f(r) : 0.f;
+		}
+	}
+	if (!(t > 0.f))
+		return 0.f;
+	const float h = log2f(t) - tl / t;
+	return h > 0.f ? h : 0.f;
+}
+
+// One trajectory (simulation.cu:34-71 initial state, :77-164 loop; simulation_runner.cu:104-162
+// epochs). `trace` (optional) receives (flip, time) per step.
+template <typename RNG>
+void trajectory(const compiled& c, sinks& s, RNG& rng, bool exact, int traj_len, run_acc& acc,
+				unsigned long long& trans, std::vector<std::pair<int, float>>* trace)
+{
+	std::vector<uint32_t> st(c.W, 0u);
+	std::vector<float> rates(c.N);
+	for (int i = 0; i < c.N; i++)
+		if (curand_uniform(&rng) <= c.m.nodes[i].istate)
+			st[i / 32] |= 1u << (i % 32);
+	float time = 0.f;
+	int slot = 1;
+	bool fixed = false;
+	for (;;)
+	{
+		// compute_transition_rates: rates in node order, sequential fp32 sum (generator.cpp:124-144)
+		float total = 0.f;
+		for (int i = 0; i < c.N; i++)
+		{
+			rates[i] = c.rate(i, st.data());
+			total += rates[i];
+		}
+		float h = 0.f, tn;
+		if (total == 0.f)
+		{
+			fixed = true;
+			tn = c.max_time_sim;
+		}
+		else
+		{
+			if (c.discrete)
+			{
+				tn = time + c.tick_sim;
+				tn = c.max_time_sim - c.tick_sim < tn ? c.max_time_sim : tn;
+			}
+			else
+			{
+				const float u = curand_uniform(&rng);
+				tn = time + -logf(u) / total;
+			}
+			tn = std::fmin(tn, c.max_time_sim);
+			h = exact ? entropy_exact(c, rates.data()) : entropy_fast(c, rates.data(), st.data());
+		}
+		trans += tn != 0.f;
+		record(c, s, acc, c.ni_index(st.data()), time, tn, h);
+		time = tn;
+		if (time >= c.max_time_sim)
+		{
+			if (trace)
+				trace->emplace_back(-1, time);
+			break;
+		}
+		if (exact && traj_len > 1 && ++slot >= traj_len)
+		{
+			slot = 1;
+			if (trace)
+				trace->emplace_back(-2, time);
+			continue;
+		}
+		// select_flip_bit, simulation.cu:9-21
+		const float r = curand_uniform(&rng) * total;
+		float sum = 0.f;
+		int idx = 0;
+		for (int i = 0; i < c.N; i++)
+		{
+			sum += rates[i];
+			idx += (sum < r) ? 1 : 0;
+		}
+		if (idx >= c.N)
+			idx = c.N - 1;
+		if (trace)
+			trace->emplace_back(idx, time);
+		st[idx / 32] ^= 1u << (idx % 32);
+	}
+	atomic_add(&s.fin[c.ni_index(st.data())], 1u);
+	if (fixed)
+	{
+#pragma omp critical(oracle_fixed)
+		s.fixed[st]++;
+	}
+}
+
+} // namespace
+
+// ------------------------------------------------------------------ C interface (ctypes)
+
+struct oracle_model
+{
+	std::unique_ptr<compiled> c;
+	std::string err;
+};
+
+struct oracle_result
+{
+	sinks s;
+	std::vector<uint32_t> fixed_states;
+	std::vector<unsigned> fixed_counts;
+	double seconds = 0;
+};
+
+extern "C" {
+
+oracle_model* oracle_model_load(const char* bnd_text, const char* cfg_text, char* err, size_t errcap)
+{
+	try
+	{
+		auto m = new oracle_model;
+		m->c = compile(bnd_text, cfg_text);
+		return m;
+	}
+	catch (const std::exception& e)
+	{
+		if (err && errcap)
+			std::snprintf(err, errcap, "%s", e.what());
+		return nullptr;
+	}
+}
+
+void oracle_model_free(oracle_model* m) { delete m; }
+
+// dims: nodes, words, non-internal count, windows, discrete, sample_count, seed, tick, max_time
+int oracle_model_dims(const oracle_model* m, int* nodes, int* words, int* noninternal, int* windows, int* discrete,
+					  long long* sample_count, unsigned long long* seed, float* tick, float* max_time)
+{
+	const compiled& c = *m->c;
+	*nodes = c.N;
+	*words = c.W;
+	*noninternal = (int)c.ni.size();
+	*windows = c.T;
+	*discrete = c.discrete;
+	*sample_count = c.sample_count;
+	*seed = c.seed;
+	*tick = c.tick_f;
+	*max_time = c.max_time_f;
+	return 0;
+}
+
+int oracle_model_noninternal(const oracle_model* m, int* out)
+{
+	for (size_t k = 0; k < m->c->ni.size(); k++)
+		out[k] = m->c->ni[k];
+	return (int)m->c->ni.size();
+}
+
+// Rate of node i and the total in state `s` (for unit tests of the model semantics).
+float oracle_model_rate(const oracle_model* m, int i, const uint32_t* s) { return m->c->rate(i, s); }
+
+// Run n trajectories [first, first + n). Fixed-point exponents must be those of the GPU run.
+oracle_result* oracle_run(const oracle_model* m, int mode, long long n, unsigned long long seed,
+						  unsigned long long first, int traj_len, int occ_exp, int ent_exp, int threads)
+{
+	const compiled& c = *m->c;
+	if (c.ni.size() > 20)
+		return nullptr;
+	auto r = new oracle_result;
+	sinks& s = r->s;
+	s.T = c.T;
+	s.S = 1u << c.ni.size();
+	s.fx = std::ldexp(1.0, occ_exp);
+	s.fxh = std::ldexp(1.0, ent_exp);
+	if (c.discrete)
+		s.cnt.assign((size_t)s.T * s.S, 0u);
+	else
+		s.occ.assign((size_t)s.T * s.S, 0);
+	s.h.assign(s.T, 0);
+	s.fin.assign(s.S, 0u);
+#ifdef _OPENMP
+	const double t0 = omp_get_wtime();
+	if (threads > 0)
+		omp_set_num_threads(threads);
+#endif
+	unsigned long long trans = 0;
+#pragma omp parallel reduction(+ : trans)
+	{
+		run_acc acc;
+#pragma omp for schedule(dynamic, 16)
+		for (long long t = 0; t < n; t++)
+		{
+			if (mode == 0)
+			{
+				curandState rng;
+				curand_init(seed, first + (unsigned long long)t, 0ull, &rng);
+				trajectory(c, s, rng, true, traj_len, acc, trans, nullptr);
+			}
+			else
+			{
+				curandStatePhilox4_32_10_t rng;
+				curand_init(seed, first + (unsigned long long)t, 0ull, &rng);
+				trajectory(c, s, rng, false, 0, acc, trans, nullptr);
+			}
+		}
+		acc.flush(s);
+	}
+	s.transitions = trans;
+#ifdef _OPENMP
+	r->seconds = omp_get_wtime() - t0;
+#endif
+	for (auto& kv : s.fixed)
+	{
+		r->fixed_states.insert(r->fixed_states.end(), kv.first.begin(), kv.first.end());
+		r->fixed_counts.push_back(kv.second);
+	}
+	return r;
+}
+
+void oracle_result_free(oracle_result* r) { delete r; }
+
+int oracle_result_get(const oracle_result* r, long long* occ, unsigned* cnt, long long* h, unsigned* fin,
+					  unsigned long long* transitions, double* seconds)
+{
+	const sinks& s = r->s;
+	if (occ && !s.occ.empty())
+		std::memcpy(occ, s.occ.data(), s.occ.size() * sizeof(long long));
+	if (cnt && !s.cnt.empty())
+		std::memcpy(cnt, s.cnt.data(), s.cnt.size() * sizeof(unsigned));
+	if (h)
+		std::memcpy(h, s.h.data(), s.h.size() * sizeof(long long));
+	if (fin)
+		std::memcpy(fin, s.fin.data(), s.fin.size() * sizeof(unsigned));
+	if (transitions)
+		*transitions = s.transitions;
+	if (seconds)
+		*seconds = r->seconds;
+	return 0;
+}
+
+int oracle_result_num_fixed(const oracle_result* r) { return (int)r->fixed_counts.size(); }
+
+int oracle_result_fixed(const oracle_result* r, uint32_t* states, unsigned* counts)
+{
+	if (states && !r->fixed_states.empty())
+		std::memcpy(states, r->fixed_states.data(), r->fixed_states.size() * sizeof(uint32_t));
+	if (counts && !r->fixed_counts.empty())
+		std::memcpy(counts, r->fixed_counts.data(), r->fixed_counts.size() * sizeof(unsigned));
+	return 0;
+}
+
+// Trace of one trajectory: flip indices (-1 = end, -2 = epoch boundary) and the time before
+// each event. Returns the number of events (may exceed cap; only cap are written).
+int oracle_trace(const oracle_model* m, int mode, unsigned long long seed, unsigned long long traj, int traj_len,
+				 int* flips, float* times, int cap)
+{
+	const compiled& c = *m->c;
+	sinks s;
+	s.T = c.T;
+	s.S = 1u << std::min<size_t>(c.ni.size(), 20);
+	s.occ.assign((size_t)s.T * s.S, 0);
+	s.cnt.assign((size_t)s.T * s.S, 0);
+	s.h.assign(s.T, 0);
+	s.fin.assign(s.S, 0);
+	std::vector<std::pair<int, float>> tr;
+	run_acc acc;
+	unsigned long long trans = 0;
+	if (mode == 0)
+	{
+		curandState rng;
+		curand_init(seed, traj, 0ull, &rng);
+		trajectory(c, s, rng, true, traj_len, acc, trans, &tr);
+	}
+	else
+	{
+		curandStatePhilox4_32_10_t rng;
+		curand_init(seed, traj, 0ull, &rng);
+		trajectory(c, s, rng, false, 0, acc, trans, &tr);
+	}
+	for (int i = 0; i < (int)tr.size() && i < cap; i++)
+	{
+		flips[i] = tr[i].first;
+		times[i] = tr[i].second;
+	}
+	return (int)tr.size();
+}
+
+} // extern "C"

@@ -1,0 +1,50 @@
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+MODELS = os.path.join(GOLDEN, "models")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a B200 (sm_100) GPU")
+
+
+def model_files(name: str) -> tuple[str, str]:
+    return os.path.join(MODELS, f"{name}.bnd"), os.path.join(MODELS, f"{name}.cfg")
+
+
+def model_text(name: str) -> tuple[str, str]:
+    b, c = model_files(name)
+    with open(b) as f, open(c) as g:
+        return f.read(), g.read()
+
+
+@pytest.fixture(scope="session", autouse=True)
+def _built():
+    """Build the engine library and the oracle in place once per session."""
+    subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "maboss", "gpu_b200", "csrc")], check=True)
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+
+
+@pytest.fixture(scope="session")
+def gpu():
+    import maboss.gpu_b200 as mb
+    return mb.Context(0)
+
+
+def pooled_z(p: np.ndarray, n1: int, q: np.ndarray, n2: int) -> np.ndarray:
+    """|p - q| in units of the pooled binomial standard error of two independent estimates."""
+    pooled = (p * n1 + q * n2) / (n1 + n2)
+    var = pooled * (1.0 - pooled) * (1.0 / n1 + 1.0 / n2)
+    z = np.zeros_like(p)
+    nz = var > 0
+    z[nz] = np.abs(p[nz] - q[nz]) / np.sqrt(var[nz])
+    return z

@@ -1,0 +1,190 @@
+"""GPU parity tests: the CUDA engine against the CPU oracle, through the C ABI.
+
+Exact mode draws the same XORWOW streams as the reference (curand_init(seed, trajectory, 0)) and
+performs the reference's fp32 operations in the same order, so integer results (final-state and
+discrete window counts, fixed points, number of transitions) must be identical to the oracle's.
+Continuous-time waiting times use logf, whose device and host implementations may differ in the
+last ulp; window occupancies are therefore compared with a tolerance of
+    |p_gpu - p_oracle| <= 1e-5 + 1e-4 * p_oracle     (probabilities per window and bin)
+and the per-window transition entropy (log2f on both sides) with a relative tolerance of 1e-4.
+"""
+import numpy as np
+import pytest
+
+import maboss.gpu_b200 as mb
+from conftest import model_text, pooled_z
+from maboss.gpu_b200 import synth
+from oracle.oracle import OracleModel
+
+pytestmark = pytest.mark.gpu
+
+P_ABS, P_REL, H_REL = 1e-5, 1e-4, 1e-4
+
+
+def _run_both(gpu, bnd, cfg, n, mode="exact", **kw):
+    model = mb.Model(bnd, cfg)
+    mod = gpu.compile(model)
+    res = mod.run(mode=mode, sample_count=n, **kw)
+    raw = res.raw()
+    o = OracleModel(bnd, cfg)
+    ref = o.run(n=n, mode=0 if mode in ("exact", "epoch") else 1, occ_exp=raw["occ_exp"], ent_exp=raw["ent_exp"],
+                seed=kw.get("seed"))
+    return model, res, raw, o, ref
+
+
+def _assert_same(res, raw, ref, discrete):
+    assert res.transitions == ref["transitions"]
+    assert np.array_equal(res.final_counts, ref["final"])
+    fx = res.fixed
+    assert len(fx) == len(ref["fixed_counts"])
+    for (st, c), st2, c2 in zip(fx, ref["fixed_states"], ref["fixed_counts"]):
+        assert np.array_equal(st, st2) and c == c2
+    assert res.fixed_overflow == 0
+    if discrete:
+        assert np.array_equal(raw["cnt"], ref["cnt"])
+    else:
+        p, q = res.window_probs, ref["probs"]
+        assert np.all(np.abs(p - q) <= P_ABS + P_REL * q), np.abs(p - q).max()
+    th, th2 = res.window_entropy, ref["th"]
+    assert np.all(np.abs(th - th2) <= 1e-6 + H_REL * np.abs(th2)), np.abs(th - th2).max()
+
+
+@pytest.mark.parametrize("name,n", [("cellcycle", 20_000), ("sizek", 2_000), ("metastasis", 1_000),
+                                    ("Montagud2022_Prostate_Cancer", 3_000)])
+def test_exact_mode_matches_oracle_on_reference_models(gpu, name, n):
+    bnd, cfg = model_text(name)
+    model, res, raw, o, ref = _run_both(gpu, bnd, cfg, n)
+    _assert_same(res, raw, ref, o.discrete)
+
+
+@pytest.mark.parametrize("gen,kw,n", [(synth.c1, {}, 20_000), (synth.c2, dict(noninternal=20), 300),
+                                      (synth.c2, dict(noninternal=12, discrete=True), 2_000),
+                                      (synth.c4, {}, 2_000), (synth.c3, {}, 40)])
+def test_exact_mode_matches_oracle_on_synthetic_networks(gpu, gen, kw, n):
+    bnd, cfg = gen(**kw)
+    model, res, raw, o, ref = _run_both(gpu, bnd, cfg, n)
+    _assert_same(res, raw, ref, o.discrete)
+
+
+@pytest.mark.parametrize("name,n", [("cellcycle", 5_000), ("sizek", 1_000)])
+def test_fast_mode_matches_oracle_fast_mode(gpu, name, n):
+    bnd, cfg = model_text(name)
+    model, res, raw, o, ref = _run_both(gpu, bnd, cfg, n, mode="fast")
+    _assert_same(res, raw, ref, o.discrete)
+
+
+@pytest.mark.parametrize("name,n", [("cellcycle", 3_000), ("metastasis", 1_000), ("sizek", 1_500)])
+def test_epoch_mode_is_identical_to_fused_exact(gpu, name, n):
+    """Buffered epochs (SoA trajectory buffers + stats kernels) and the fused kernel agree bit for bit."""
+    model = mb.Model(*model_text(name))
+    mod = gpu.compile(model)
+    a, b = mod.run(mode="exact", sample_count=n), mod.run(mode="epoch", sample_count=n)
+    ra, rb = a.raw(), b.raw()
+    for k in ("occ", "cnt", "h"):
+        assert np.array_equal(ra[k], rb[k]), k
+    assert np.array_equal(a.final_counts, b.final_counts)
+    assert a.transitions == b.transitions
+    assert [(s.tolist(), c) for s, c in a.fixed] == [(s.tolist(), c) for s, c in b.fixed]
+
+
+def test_epoch_refill_beyond_batch_limit(gpu):
+    """More trajectories than the batch: refilled slots start fresh streams; totals stay consistent."""
+    model = mb.Model(*model_text("metastasis"))
+    mod = gpu.compile(model)
+    r = mod.run(mode="epoch", sample_count=2_500, batch_limit=1_000)
+    assert r.final_counts.sum() == 2_500
+    assert r.timing[2] >= 3
+    p = r.window_probs
+    assert np.allclose(p.sum(axis=1), 1.0, atol=1e-5)
+
+
+def test_fast_mode_statistically_equivalent_to_exact(gpu):
+    bnd, cfg = synth.c1()
+    model = mb.Model(bnd, cfg)
+    mod = gpu.compile(model)
+    n = 100_000
+    a, b = mod.run(mode="exact", sample_count=n), mod.run(mode="fast", sample_count=n)
+    z = pooled_z(a.window_probs.ravel(), n, b.window_probs.ravel(), n)
+    assert z.max() < 4.5
+    zf = pooled_z(a.final_counts / n, n, b.final_counts / n, n)
+    assert zf.max() < 4.5
+
+
+def test_results_are_reproducible(gpu):
+    model = mb.Model(*model_text("sizek"))
+    mod = gpu.compile(model)
+    a, b = mod.run(mode="fast", sample_count=4_000), mod.run(mode="fast", sample_count=4_000)
+    assert np.array_equal(a.raw()["occ"], b.raw()["occ"])
+    assert np.array_equal(a.final_counts, b.final_counts)
+
+
+def test_low_level_kernel_entry_points(gpu):
+    """init_random -> init_state -> simulate -> window/final/fixed stats through the C ABI on
+    caller-owned device buffers reproduces the whole-run result (one epoch suffices here)."""
+    import torch
+
+    bnd, cfg = model_text("cellcycle")  # 25 discrete steps < one epoch of 100 slots
+    model = mb.Model(bnd, cfg)
+    mod = gpu.compile(model)
+    n, L = 4_096, 100
+    N, W = mod.state_size
+    dev = torch.device("cuda", 0)
+    rands = torch.empty(n * mb.rand_state_size(), dtype=torch.uint8, device=dev)
+    last = torch.empty(W * n, dtype=torch.int32, device=dev)
+    times = torch.empty(n, dtype=torch.float32, device=dev)
+    istate = torch.tensor([model.node_info(i)[0] for i in range(N)], dtype=torch.float32, device=dev)
+    ts = torch.empty(L * W * n, dtype=torch.int32, device=dev)
+    tt = torch.empty(L * n, dtype=torch.float32, device=dev)
+    th = torch.empty(L * n, dtype=torch.float32, device=dev)
+    stat = torch.empty(n, dtype=torch.uint8, device=dev)
+    trans = torch.zeros(1, dtype=torch.int64, device=dev)
+    torch.cuda.synchronize()
+    seed = int(model.constant("seed_pseudorandom"))
+    mod.launch_initialize_random(n, seed, 0, rands.data_ptr())
+    mod.launch_initialize_initial_state(n, n, istate.data_ptr(), last.data_ptr(), times.data_ptr(), rands.data_ptr())
+    mod.launch_simulate(n, n, L, last.data_ptr(), times.data_ptr(), rands.data_ptr(), ts.data_ptr(), tt.data_ptr(),
+                        th.data_ptr(), stat.data_ptr(), trans.data_ptr())
+    st = mod.stats(model.constant("time_tick"), model.constant("max_time"), bool(model.constant("discrete_time")),
+                   model.noninternal_nodes, n)
+    st.final(n, n, last.data_ptr(), stat.data_ptr())
+    st.fixed(n, n, last.data_ptr(), stat.data_ptr())
+    st.window(n, n, L, ts.data_ptr(), tt.data_ptr(), th.data_ptr())
+    r = st.finalize(n)
+    assert int((stat == 0).sum()) == 0  # every trajectory finished in one epoch
+    ref = mod.run(mode="exact", sample_count=n)
+    assert np.array_equal(r.raw()["cnt"], ref.raw()["cnt"])
+    assert np.array_equal(r.final_counts, ref.final_counts)
+    assert int(trans.item()) == ref.transitions
+    # slot 0 holds the start time, recorded times are tick multiples
+    assert float(tt[:n].abs().max()) == 0.0
+    assert float(tt[n:2 * n].min()) == pytest.approx(model.constant("time_tick"))
+
+
+def test_edge_cases(gpu):
+    bnd, cfg = model_text("metastasis")
+    model = mb.Model(bnd, cfg)
+    mod = gpu.compile(model)
+    r0 = mod.run(sample_count=0)
+    assert r0.final_counts.sum() == 0 and r0.transitions == 0
+    r1 = mod.run(sample_count=1)
+    assert r1.final_counts.sum() == 1
+    # every node internal: a single bin
+    allint = "\n".join(f"{n}.is_internal = 1;" for n in model.node_names)
+    m2 = mb.Model(bnd, cfg + allint)
+    r2 = gpu.compile(m2).run(sample_count=500)
+    assert r2.dims.bins == 1 and r2.final_counts[0] == 500
+    assert np.allclose(r2.window_probs[:, 0], 1.0, atol=1e-5)
+
+
+def test_window_edge_ticks(gpu):
+    """tick not dividing max_time, single window, and word-boundary network sizes (32/33 nodes)."""
+    for n_nodes in (32, 33):
+        names = [f"Y{i}" for i in range(n_nodes)]
+        bnd = "".join(f"node {names[i]} {{ logic = !{names[(i + 1) % n_nodes]}; rate_up = @logic ? 1 : 0; "
+                      f"rate_down = @logic ? 0 : 2; }}\n" for i in range(n_nodes))
+        outs = {0, 31, n_nodes - 1}
+        internal = "".join(f"{names[i]}.is_internal = 1;\n" for i in range(n_nodes) if i not in outs)
+        for tail in ("max_time = 3; time_tick = 0.7;", "max_time = 0.5; time_tick = 1;"):
+            cfg = internal + tail + " sample_count = 500;"
+            model, res, raw, o, ref = _run_both(gpu, bnd, cfg, 500)
+            _assert_same(res, raw, ref, False)
