@@ -105,8 +105,8 @@ mb_status mb_module_compile(mb_context c, const char* generated_code, mb_module*
 /* Generate + compile in one call; the module keeps the model's layout. */
 mb_status mb_module_compile_model(mb_context c, mb_model m, mb_module* out);
 mb_status mb_module_free(mb_module mod);
-/* NVRTC compilation of generated code + engine for sm_100a without a device (build checks);
- * writes the cubin size and the compiler log. */
+/* NVRTC compilation of generated code + every engine kernel family for sm_100a without a
+ * device (build checks); writes the total cubin size and the compiler log. */
 mb_status mb_jit_check(const char* generated_code, size_t* cubin_size, char* log, size_t cap);
 mb_status mb_module_state_size(mb_module mod, int* state_size, int* state_words);
 /* NVRTC log of the compilation (may be empty). */

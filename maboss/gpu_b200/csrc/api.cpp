@@ -300,11 +300,17 @@ mb_status mb_jit_check(const char* generated_code, size_t* cubin_size, char* log
 {
 	return guard([&] {
 		need(generated_code, "null code");
-		std::string lg;
-		auto cubin = mb::compile_cubin(generated_code, lg);
+		std::string all;
+		size_t total = 0;
+		for (int f = 0; f < mb::FAMILY_COUNT; f++)
+		{
+			std::string lg;
+			total += mb::compile_cubin(generated_code, lg, f).size();
+			all += lg;
+		}
 		if (cubin_size)
-			*cubin_size = cubin.size();
-		copy_out(lg, log, cap, nullptr);
+			*cubin_size = total;
+		copy_out(all, log, cap, nullptr);
 	});
 }
 
@@ -346,6 +352,8 @@ mb_status mb_launch_initialize_random(mb_module mod, void* stream, int n, unsign
 			return;
 		mb::module& m = *mod->mod;
 		MB_CUDA(cudaSetDevice(m.ctx->device));
+		if (!m.init_random)
+			m.ensure(mb::FAMILY_EPOCH);
 		void* a[] = { &n, &seed, &first, &rands };
 		mb::launch(m.init_random, (n + 255) / 256, 256, 0, stream_of(m.ctx, stream), a);
 	});
@@ -362,6 +370,7 @@ mb_status mb_launch_initialize_initial_state(mb_module mod, void* stream, int n,
 		need(initial_probs && last_states && last_times && rands, "null buffer");
 		mb::module& m = *mod->mod;
 		MB_CUDA(cudaSetDevice(m.ctx->device));
+		m.ensure_any();
 		void* a[] = { &n, &stride, &initial_probs, &last_states, &last_times, &rands };
 		mb::launch(m.init_state, (n + 255) / 256, 256, 0, stream_of(m.ctx, stream), a);
 	});
@@ -380,6 +389,7 @@ mb_status mb_launch_simulate(mb_module mod, void* stream, int n, int stride, int
 			 "null buffer");
 		mb::module& m = *mod->mod;
 		MB_CUDA(cudaSetDevice(m.ctx->device));
+		m.ensure(mb::FAMILY_EPOCH);
 		void* a[] = { &n,		   &stride,		 &traj_len,		  &last_states, &last_times,  &rands,
 					  &traj_states, &traj_times, &traj_entropies, &statuses,	&transitions };
 		mb::launch(m.sim_epoch, (n + 255) / 256, 256, 0, stream_of(m.ctx, stream), a);

@@ -218,6 +218,65 @@ std::string ident(const std::string& node_name) { return node_name; }
 
 void emit_bit(std::ostream& os, int i) { os << "((state[" << i / 32 << "] & " << (1u << (i % 32)) << "u) != 0)"; }
 
+template <typename T>
+void emit_array(std::ostream& os, const char* type, const char* name, const std::vector<T>& v)
+{
+	os << "__device__ const " << type << " " << name << "[" << std::max<size_t>(1, v.size()) << "] = {";
+	if (v.empty())
+		os << "0";
+	for (size_t i = 0; i < v.size(); i++)
+		os << (i ? (i % 16 ? ", " : ",\n    ") : "") << v[i];
+	os << "};" << std::endl;
+}
+
+// Tables of the incremental fast-mode kernel (see kernels/engine.cuh: mb_fused_incr).
+void emit_incremental_tables(std::ostream& ss, const model_layout& L)
+{
+	ss << std::endl << "// ---- incremental engine tables" << std::endl;
+	if (!L.incremental_ok)
+	{
+		ss << "constexpr int mbg_inc_rate_shift = 0;" << std::endl;
+		return;
+	}
+	const int N = L.state_size;
+	ss << "#define MBG_INCREMENTAL 1" << std::endl;
+	ss << "constexpr int mbg_inc_rate_shift = " << L.rate_shift << ";" << std::endl;
+	emit_array(ss, "unsigned", "mbg_inc_q_up", L.q_up);
+	emit_array(ss, "unsigned", "mbg_inc_q_down", L.q_down);
+	emit_array(ss, "int", "mbg_inc_dep_ptr", L.dep_ptr);
+	emit_array(ss, "int", "mbg_inc_dep_idx", L.dep_idx);
+	emit_array(ss, "int", "mbg_inc_in_ptr", L.in_ptr);
+	emit_array(ss, "int", "mbg_inc_in_idx", L.in_idx);
+	emit_array(ss, "int", "mbg_inc_tt_ptr", L.tt_ptr);
+	emit_array(ss, "unsigned", "mbg_inc_tt", L.tt_words);
+	std::vector<int> ni_pos(N, -1);
+	for (size_t k = 0; k < L.noninternal_nodes.size(); k++)
+		ni_pos[L.noninternal_nodes[k]] = (int)k;
+	emit_array(ss, "int", "mbg_inc_ni_pos", ni_pos);
+	std::vector<float> ni_up, ni_down, ni_ul, ni_dl;
+	for (int i : L.noninternal_nodes)
+	{
+		const double u = L.up[i], d = L.down[i];
+		ni_up.push_back(L.up[i]);
+		ni_down.push_back(L.down[i]);
+		ni_ul.push_back(u > 0 ? (float)(u * std::log2(u)) : 0.f);
+		ni_dl.push_back(d > 0 ? (float)(d * std::log2(d)) : 0.f);
+	}
+	std::vector<std::string> f_up, f_down, f_ul, f_dl;
+	for (size_t k = 0; k < ni_up.size(); k++)
+	{
+		f_up.push_back(flit(ni_up[k]));
+		f_down.push_back(flit(ni_down[k]));
+		f_ul.push_back(flit(ni_ul[k]));
+		f_dl.push_back(flit(ni_dl[k]));
+	}
+	emit_array(ss, "float", "mbg_inc_ni_up", f_up);
+	emit_array(ss, "float", "mbg_inc_ni_down", f_down);
+	emit_array(ss, "float", "mbg_inc_ni_ul", f_ul);
+	emit_array(ss, "float", "mbg_inc_ni_dl", f_dl);
+	emit_array(ss, "int", "mbg_inc_ni_node", L.noninternal_nodes);
+}
+
 } // namespace
 
 int model_layout::windows() const
@@ -339,8 +398,40 @@ model_layout analyze_model(const model_t& m)
 				L.dep_ptr.push_back((int)L.dep_idx.size());
 			}
 		}
+		if (L.incremental_ok)
+		{
+			// fixed-point scale: every word's largest possible rate sum stays below 2^31
+			double worst = 0;
+			for (int w = 0; w < L.state_words; w++)
+			{
+				double sw = 0;
+				for (int i = 32 * w; i < std::min(N, 32 * w + 32); i++)
+					sw += std::max((double)L.up[i], (double)L.down[i]);
+				worst = std::max(worst, sw);
+			}
+			int shift = 30;
+			while (shift > 0 && worst * std::ldexp(1.0, shift) >= 2147483648.0)
+				shift--;
+			L.rate_shift = shift;
+			L.q_up.resize(N);
+			L.q_down.resize(N);
+			for (int i = 0; i < N && L.incremental_ok; i++)
+			{
+				for (int which = 0; which < 2; which++)
+				{
+					const double r = which ? L.down[i] : L.up[i];
+					const double q = std::nearbyint(r * std::ldexp(1.0, shift));
+					// positive rates need enough resolution (relative error below 2^-10)
+					if (r > 0 && q < 1024.0)
+						L.incremental_ok = false;
+					(which ? L.q_down[i] : L.q_up[i]) = (unsigned)q;
+				}
+			}
+		}
 		if (!L.incremental_ok)
 		{
+			L.q_up.clear();
+			L.q_down.clear();
 			L.in_ptr.clear();
 			L.in_idx.clear();
 			L.tt_ptr.clear();
@@ -368,7 +459,9 @@ std::string generate_code(const model_t& m)
 	ss << "constexpr float time_tick = " << print_float(m.constant("time_tick")) << ";" << std::endl;
 	ss << "using state_word_t = uint32_t;" << std::endl << std::endl;
 
-	// ---- per-node rate functions (generator.cpp:84-122)
+	// ---- per-node rate functions (generator.cpp:84-122); internal linkage so that kernels which
+	// do not use them do not pay for their compilation
+	ss << "namespace {" << std::endl << std::endl;
 	for (int i = 0; i < N; i++)
 	{
 		const node_t& node = m.nodes[i];
@@ -434,6 +527,7 @@ std::string generate_code(const model_t& m)
 		ss << "    entropy -= (tmp_prob == 0.f) ? 0.f : log2f(tmp_prob) * tmp_prob;" << std::endl;
 	}
 	ss << "    return entropy;" << std::endl << "}" << std::endl << std::endl;
+	ss << "} // namespace" << std::endl << std::endl;
 
 	// ---- get_non_internal_index (generator.cpp:207-235)
 	ss << "__device__ uint32_t get_non_internal_index(const state_word_t* __restrict__ state)" << std::endl;
@@ -543,6 +637,7 @@ std::string generate_code(const model_t& m)
 	ss << "    const float h = log2f(t) - tl / t;" << std::endl;
 	ss << "    return h > 0.f ? h : 0.f;" << std::endl << "}" << std::endl;
 
+	emit_incremental_tables(ss, L);
 	return ss.str();
 }
 

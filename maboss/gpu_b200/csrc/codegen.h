@@ -44,6 +44,8 @@ struct model_layout
 	std::vector<int> tt_ptr;				// offset (in 32-bit words) of each node's truth table
 	std::vector<unsigned> tt_words;			// truth tables, bit b = logic value for input pattern b
 	std::vector<int> dep_ptr, dep_idx;		// nodes whose rate must be re-evaluated after a flip
+	int rate_shift = 0;						// fast-mode rates in fixed point: q = round(rate * 2^shift)
+	std::vector<unsigned> q_up, q_down;
 
 	int windows() const; // ceil(max_time / time_tick) in float, window_average_small.cpp:305
 };

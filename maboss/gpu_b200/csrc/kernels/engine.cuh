@@ -331,14 +331,301 @@ __device__ __forceinline__ void mb_fused_body(const mb_fused_params& P)
 	}
 }
 
+#ifdef MB_FAMILY_EXACT
 extern "C" __global__ void __launch_bounds__(256) mb_fused_exact(mb_fused_params P) { mb_fused_body<true>(P); }
+#endif
+
+#ifdef MB_FAMILY_FAST
+#ifndef MBG_INCREMENTAL
 extern "C" __global__ void __launch_bounds__(256) mb_fused_fast(mb_fused_params P) { mb_fused_body<false>(P); }
+#else
+// ---------------------------------------------------------------- incremental fast kernel
+// Fast mode for models whose rates all have the form `@logic ? U : 0` / `@logic ? 0 : D`.
+// A node is unstable when its bit differs from its logic; only unstable nodes have a rate
+// (U when off, D when on). Per trajectory, in shared memory: the state words, the unstable
+// masks and the integer rate sum of every state word (rates in fixed point 2^-shift); in
+// registers: group sums over MB_WPG words and the total. After a flip only the flipped node
+// and the nodes whose logic reads it are re-evaluated (truth tables over their inputs), so a
+// step costs O(dependents + W/MB_WPG + MB_WPG + 32) instead of O(N) rate evaluations. The flip
+// is drawn exactly in proportion to the integer rates with a 64-bit uniform; waiting times and
+// window slices are computed as in the other kernels. Statistically equivalent to the
+// reference; not bit-exact (different random streams and rate rounding below 2^-shift).
+constexpr int MB_WPG = state_words <= 2 ? 1 : (state_words <= 8 ? 2 : 4);
+constexpr int MB_GROUPS = (state_words + MB_WPG - 1) / MB_WPG;
+
+struct mb_incr_view
+{
+	uint32_t* st; // [w * blockDim + t]
+	uint32_t* un;
+	uint32_t* ws;
+	int stride;
+	__device__ __forceinline__ uint32_t& S(int w) const { return st[w * stride]; }
+	__device__ __forceinline__ uint32_t& U(int w) const { return un[w * stride]; }
+	__device__ __forceinline__ uint32_t& Q(int w) const { return ws[w * stride]; }
+};
+
+__device__ __forceinline__ bool mb_incr_logic(const mb_incr_view& v, int k)
+{
+	const int a = __ldg(mbg_inc_in_ptr + k), b = __ldg(mbg_inc_in_ptr + k + 1);
+	unsigned p = 0;
+	for (int t = a; t < b; t++)
+	{
+		const int in = __ldg(mbg_inc_in_idx + t);
+		p |= ((v.S(in >> 5) >> (in & 31)) & 1u) << (t - a);
+	}
+	return (__ldg(mbg_inc_tt + __ldg(mbg_inc_tt_ptr + k) + (p >> 5)) >> (p & 31)) & 1u;
+}
+
+__device__ __forceinline__ void mb_group_add(unsigned long long (&gs)[MB_GROUPS], int g, long long d)
+{
+#pragma unroll
+	for (int i = 0; i < MB_GROUPS; i++)
+		gs[i] += (i == g) ? (unsigned long long)d : 0ull;
+}
+
+// entropy of the non-internal rates, h = log2(S) - sum(r log2 r) / S
+__device__ __forceinline__ float mb_incr_entropy(const mb_incr_view& v)
+{
+	float t = 0.f, tl = 0.f;
+	for (int k = 0; k < mbg_noninternal_count; k++)
+	{
+		const int i = __ldg(mbg_inc_ni_node + k);
+		const uint32_t bit = 1u << (i & 31);
+		if (v.U(i >> 5) & bit)
+		{
+			const bool up = (v.S(i >> 5) & bit) != 0;
+			t += up ? __ldg(mbg_inc_ni_down + k) : __ldg(mbg_inc_ni_up + k);
+			tl += up ? __ldg(mbg_inc_ni_dl + k) : __ldg(mbg_inc_ni_ul + k);
+		}
+	}
+	if (!(t > 0.f))
+		return 0.f;
+	const float h = log2f(t) - tl / t;
+	return h > 0.f ? h : 0.f;
+}
+
+extern "C" __global__ void __launch_bounds__(128) mb_fused_fast(mb_fused_params P)
+{
+	extern __shared__ uint32_t mb_smem_u32[];
+	const int B = blockDim.x;
+	mb_incr_view v;
+	v.stride = B;
+	v.st = mb_smem_u32 + threadIdx.x;
+	v.un = mb_smem_u32 + (size_t)state_words * B + threadIdx.x;
+	v.ws = mb_smem_u32 + (size_t)2 * state_words * B + threadIdx.x;
+	long long* hsink = P.st.win_h;
+	long long* smem_h = reinterpret_cast<long long*>(mb_smem_u32 + (size_t)3 * state_words * B);
+	if (P.st.h_in_smem)
+	{
+		for (int i = threadIdx.x; i < P.st.n_windows; i += B)
+			smem_h[i] = 0;
+		__syncthreads();
+		hsink = smem_h;
+	}
+	const float inv_scale = 1.0f / (float)(1u << mbg_inc_rate_shift);
+
+	unsigned long long trans = 0;
+	mb_win_acc acc;
+	mb_acc_init(acc);
+	for (;;)
+	{
+		const unsigned long long t = atomicAdd(P.next_traj, 1ull);
+		if (t >= P.n_traj)
+			break;
+		curandStatePhilox4_32_10_t rng;
+		curand_init(P.seed, P.first_traj + t, 0ull, &rng);
+
+		// initial state, unstable masks, word / group / total rate sums
+		for (int w = 0; w < state_words; w++)
+		{
+			uint32_t s = 0;
+			const int nb = (w == state_words - 1) ? state_size - 32 * w : 32;
+			for (int b = 0; b < nb; b++)
+				if (curand_uniform(&rng) <= __ldg(P.istate + 32 * w + b))
+					s |= 1u << b;
+			v.S(w) = s;
+		}
+		unsigned long long gs[MB_GROUPS];
+#pragma unroll
+		for (int g = 0; g < MB_GROUPS; g++)
+			gs[g] = 0;
+		unsigned long long total = 0;
+		uint32_t idx = 0;
+		for (int w = 0; w < state_words; w++)
+		{
+			const uint32_t sw = v.S(w);
+			uint32_t uw = 0, qw = 0;
+			const int nb = (w == state_words - 1) ? state_size - 32 * w : 32;
+			for (int b = 0; b < nb; b++)
+			{
+				const int i = 32 * w + b;
+				const bool on = (sw >> b) & 1u;
+				if (on != mb_incr_logic(v, i))
+				{
+					uw |= 1u << b;
+					qw += on ? __ldg(mbg_inc_q_down + i) : __ldg(mbg_inc_q_up + i);
+				}
+				const int pos = __ldg(mbg_inc_ni_pos + i);
+				if (pos >= 0 && on)
+					idx |= 1u << pos;
+			}
+			v.U(w) = uw;
+			v.Q(w) = qw;
+			mb_group_add(gs, w / MB_WPG, qw);
+			total += qw;
+		}
+		float h = mb_incr_entropy(v);
+
+		float time = 0.f;
+		bool fixed = false;
+		for (;;)
+		{
+			float tn;
+			const float total_f = (float)total * inv_scale;
+			if (total == 0)
+			{
+				fixed = true;
+				tn = max_time;
+			}
+			else
+			{
+				if (discrete_time)
+				{
+					tn = time + time_tick;
+					tn = max_time - time_tick < tn ? max_time : tn;
+				}
+				else
+					tn = time + -logf(curand_uniform(&rng)) / total_f;
+				tn = fminf(tn, max_time);
+			}
+			trans += (tn != 0.f) ? 1ull : 0ull;
+			if (tn != 0.f)
+			{
+				if (discrete_time)
+					mb_record_disc(P.st, hsink, idx, time, total == 0 ? 0.f : h);
+				else
+					mb_record_cont(acc, P.st, hsink, idx, time, tn, total == 0 ? 0.f : h);
+			}
+			time = tn;
+			if (time >= max_time)
+				break;
+
+			// draw the flip: r uniform in [0, total), then group -> word -> node
+			const unsigned hi = curand(&rng);
+			const unsigned lo = curand(&rng);
+			const unsigned long long r64 = ((unsigned long long)hi << 32) | lo;
+			const unsigned long long r = __umul64hi(r64, total);
+			unsigned long long cum = 0;
+			int g = -1;
+#pragma unroll
+			for (int i = 0; i < MB_GROUPS; i++)
+			{
+				const bool hit = g < 0 && r < cum + gs[i];
+				g = hit ? i : g;
+				cum += (g < 0) ? gs[i] : 0ull;
+			}
+			if (g < 0)
+				g = MB_GROUPS - 1; // unreachable: sum of gs is total
+			int word = g * MB_WPG;
+			for (int i = 0; i < MB_WPG; i++)
+			{
+				const int w = g * MB_WPG + i;
+				if (w >= state_words)
+					break;
+				word = w;
+				const uint32_t q = v.Q(w);
+				if (r < cum + q)
+					break;
+				cum += q;
+			}
+			const uint32_t sw = v.S(word);
+			uint32_t um = v.U(word);
+			int j = 32 * word + 31 - __clz(um | 1u);
+			while (um)
+			{
+				const int b = __ffs(um) - 1;
+				const int i = 32 * word + b;
+				const uint32_t q = ((sw >> b) & 1u) ? __ldg(mbg_inc_q_down + i) : __ldg(mbg_inc_q_up + i);
+				if (r < cum + q)
+				{
+					j = i;
+					break;
+				}
+				cum += q;
+				um &= um - 1u;
+			}
+
+			// flip j and re-evaluate it and its dependents
+			v.S(j >> 5) ^= 1u << (j & 31);
+			const int pj = __ldg(mbg_inc_ni_pos + j);
+			if (pj >= 0)
+				idx ^= 1u << pj;
+			bool ni_changed = pj >= 0;
+			const int d0 = __ldg(mbg_inc_dep_ptr + j), d1 = __ldg(mbg_inc_dep_ptr + j + 1);
+			for (int d = d0; d < d1; d++)
+			{
+				const int k = __ldg(mbg_inc_dep_idx + d);
+				const int wk = k >> 5;
+				const uint32_t bk = 1u << (k & 31);
+				const bool on = (v.S(wk) & bk) != 0;
+				const bool was_on = (k == j) ? !on : on;
+				const uint32_t uw = v.U(wk);
+				const bool was_unstable = (uw & bk) != 0;
+				const bool unstable = on != mb_incr_logic(v, k);
+				const uint32_t qo = was_unstable ? (was_on ? __ldg(mbg_inc_q_down + k) : __ldg(mbg_inc_q_up + k)) : 0u;
+				const uint32_t qn = unstable ? (on ? __ldg(mbg_inc_q_down + k) : __ldg(mbg_inc_q_up + k)) : 0u;
+				if (unstable != was_unstable)
+					v.U(wk) = uw ^ bk;
+				if (qn != qo)
+				{
+					const long long dq = (long long)qn - (long long)qo;
+					v.Q(wk) += (uint32_t)dq;
+					mb_group_add(gs, wk / MB_WPG, dq);
+					total += (unsigned long long)dq;
+					ni_changed |= __ldg(mbg_inc_ni_pos + k) >= 0;
+				}
+				else if (unstable != was_unstable)
+					ni_changed |= __ldg(mbg_inc_ni_pos + k) >= 0;
+			}
+			if (ni_changed)
+				h = mb_incr_entropy(v);
+		}
+		atomicAdd(P.st.final_cnt + idx, 1u);
+		if (fixed)
+		{
+			state_word_t st[state_words];
+#pragma unroll
+			for (int w = 0; w < state_words; w++)
+				st[w] = v.S(w);
+			mb_fixed_insert(P.st, st);
+		}
+	}
+	mb_acc_flush(acc, P.st, hsink);
+
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+		trans += __shfl_down_sync(0xffffffffu, trans, o);
+	if ((threadIdx.x & 31) == 0 && trans)
+		atomicAdd(P.transitions, trans);
+
+	if (P.st.h_in_smem)
+	{
+		__syncthreads();
+		for (int i = threadIdx.x; i < P.st.n_windows; i += B)
+			if (smem_h[i] != 0)
+				atomicAdd(reinterpret_cast<unsigned long long*>(P.st.win_h + i), (unsigned long long)smem_h[i]);
+	}
+}
+#endif // MBG_INCREMENTAL
+#endif // MB_FAMILY_FAST
 
 // ---------------------------------------------------------------- buffered epoch kernels (SoA)
 // Layouts (stride = batch capacity B):
 //   last_states[w * B + i], last_times[i], rands[i] (curandState), statuses[i]
 //   traj_states[(s * W + w) * B + i], traj_times[s * B + i], traj_h[s * B + i]
 
+#if defined(MB_FAMILY_EXACT) || defined(MB_FAMILY_EPOCH)
+// (kept out of the fast family: curand_init's XORWOW skip-ahead tables are megabytes of code)
 extern "C" __global__ void mb_initialize_random(int n, unsigned long long seed, unsigned long long first,
 												 curandState* __restrict__ rands)
 {
@@ -347,6 +634,7 @@ extern "C" __global__ void mb_initialize_random(int n, unsigned long long seed, 
 		return;
 	curand_init(seed, first + id, 0ull, rands + id); // simulation.cu:23-32
 }
+#endif
 
 extern "C" __global__ void mb_initialize_initial_state(int n, int stride, const float* __restrict__ istate,
 														uint32_t* __restrict__ states, float* __restrict__ times,
@@ -365,6 +653,7 @@ extern "C" __global__ void mb_initialize_initial_state(int n, int stride, const 
 	rands[id] = r;
 }
 
+#ifdef MB_FAMILY_EPOCH
 // One epoch of at most L-1 recorded steps per trajectory (simulation.cu:77-164).
 extern "C" __global__ void __launch_bounds__(256)
 	mb_simulate_epoch(int n, int stride, int L, uint32_t* __restrict__ last_states, float* __restrict__ last_times,
@@ -442,6 +731,8 @@ extern "C" __global__ void __launch_bounds__(256)
 	if ((threadIdx.x & 31) == 0 && trans)
 		atomicAdd(transitions, trans);
 }
+
+#endif // MB_FAMILY_EPOCH
 
 // Window statistics over one epoch's buffer, one thread per trajectory walking its slots
 // (coalesced across threads for every slot).

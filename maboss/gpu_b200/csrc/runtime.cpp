@@ -7,6 +7,7 @@
 #include <nvrtc.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -186,17 +187,20 @@ context::~context()
 
 module::~module()
 {
-	if (mod)
-	{
-		cudaSetDevice(ctx->device);
-		drv().ModuleUnload(mod);
-	}
+	cudaSetDevice(ctx->device);
+	for (CUmodule& m : mods)
+		if (m)
+			drv().ModuleUnload(m);
 }
 
-std::vector<char> compile_cubin(const std::string& generated_code, std::string& log)
+std::vector<char> compile_cubin(const std::string& generated_code, std::string& log, int family)
 {
+	static const char* defines[FAMILY_COUNT] = { "#define MB_FAMILY_EXACT 1\n", "#define MB_FAMILY_FAST 1\n",
+												 "#define MB_FAMILY_EPOCH 1\n" };
+	if (family < 0 || family >= FAMILY_COUNT)
+		throw engine_error(MB_ERR_INVALID, "bad kernel family");
 	const std::string source = generated_code + "\n// ---- engine: kernel parameter blocks\n" + mb_params_source +
-							   "\n// ---- engine: kernels\n" + mb_engine_source;
+							   "\n// ---- engine: kernels\n" + defines[family] + mb_engine_source;
 	const int N = parse_constexpr(generated_code, "state_size", -1);
 	const int W = parse_constexpr(generated_code, "state_words", -1);
 	if (N <= 0 || W != (N + 31) / 32)
@@ -242,23 +246,58 @@ std::unique_ptr<module> compile_module(context& ctx, const std::string& generate
 	m->state_size = parse_constexpr(generated_code, "state_size", -1);
 	m->state_words = parse_constexpr(generated_code, "state_words", -1);
 	m->noninternal_count = parse_constexpr(generated_code, "mbg_noninternal_count", -1);
-	std::vector<char> cubin = compile_cubin(generated_code, m->log);
+	m->incremental = generated_code.find("#define MBG_INCREMENTAL 1") != std::string::npos;
 	m->source = generated_code;
-	cu_throw(drv().ModuleLoadData(&m->mod, cubin.data()), "cuModuleLoadData");
-	auto get = [&](CUfunction& f, const char* name) { cu_throw(drv().ModuleGetFunction(&f, m->mod, name), name); };
-	get(m->fused_exact, "mb_fused_exact");
-	get(m->fused_fast, "mb_fused_fast");
-	get(m->init_random, "mb_initialize_random");
-	get(m->init_state, "mb_initialize_initial_state");
-	get(m->sim_epoch, "mb_simulate_epoch");
-	get(m->window_epoch, "mb_window_epoch");
-	get(m->final_epoch, "mb_final_epoch");
-	get(m->fixed_epoch, "mb_fixed_epoch");
-	get(m->compact_count, "mb_compact_count");
-	get(m->compact_scan, "mb_compact_scan");
-	get(m->compact_scatter, "mb_compact_scatter");
-	get(m->fixed_extract, "mb_fixed_extract");
+	// the fast family is compiled now so that errors in the generated code surface here
+	m->ensure(FAMILY_FAST);
 	return m;
+}
+
+namespace {
+std::mutex family_mu;
+}
+
+void module::ensure(int family)
+{
+	std::lock_guard<std::mutex> lk(family_mu);
+	if (mods[family])
+		return;
+	MB_CUDA(cudaSetDevice(ctx->device));
+	auto t0 = std::chrono::steady_clock::now();
+	std::string lg;
+	std::vector<char> cubin = compile_cubin(source, lg, family);
+	compile_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+	if (!lg.empty())
+		log += lg;
+	CUmodule cm = nullptr;
+	cu_throw(drv().ModuleLoadData(&cm, cubin.data()), "cuModuleLoadData");
+	mods[family] = cm;
+	auto get = [&](CUfunction& f, const char* name) { cu_throw(drv().ModuleGetFunction(&f, cm, name), name); };
+	if (family == FAMILY_EXACT)
+		get(fused_exact, "mb_fused_exact");
+	if (family == FAMILY_FAST)
+		get(fused_fast, "mb_fused_fast");
+	if (family == FAMILY_EPOCH)
+		get(sim_epoch, "mb_simulate_epoch");
+	if (family != FAMILY_FAST && !init_random)
+		get(init_random, "mb_initialize_random");
+	if (!init_state)
+	{
+		get(init_state, "mb_initialize_initial_state");
+		get(window_epoch, "mb_window_epoch");
+		get(final_epoch, "mb_final_epoch");
+		get(fixed_epoch, "mb_fixed_epoch");
+		get(compact_count, "mb_compact_count");
+		get(compact_scan, "mb_compact_scan");
+		get(compact_scatter, "mb_compact_scatter");
+		get(fixed_extract, "mb_fixed_extract");
+	}
+}
+
+void module::ensure_any()
+{
+	if (!init_state)
+		ensure(FAMILY_FAST);
 }
 
 void launch(CUfunction f, unsigned grid, unsigned block, size_t smem, cudaStream_t s, void** args)
@@ -330,6 +369,7 @@ void stats_state::init(module& m, float tick, float tmax, bool discrete, const s
 					   long long n, int fixed_capacity_log2, cudaStream_t s)
 {
 	mod = &m;
+	m.ensure_any();
 	const int k = (int)noninternal.size();
 	if (m.noninternal_count >= 0 && m.noninternal_count != k)
 		throw engine_error(MB_ERR_INVALID, "the module was generated for " + std::to_string(m.noninternal_count) +
@@ -559,13 +599,26 @@ void launch_fused(module& m, const run_config& c, stats_state& st, long long n, 
 	P.next_traj = st.next_traj();
 	P.transitions = st.transitions();
 	P.errors = st.error_ctr();
+	m.ensure(c.mode == MB_MODE_FUSED_EXACT ? FAMILY_EXACT : FAMILY_FAST);
 	CUfunction f = c.mode == MB_MODE_FUSED_EXACT ? m.fused_exact : m.fused_fast;
-	const size_t smem = st.h_smem();
-	const int per_sm = c.blocks_per_sm > 0 ? c.blocks_per_sm : occupancy_blocks(f, c.block, smem);
-	const long long needed = (n + c.block - 1) / c.block;
+	int block = c.block;
+	size_t smem = st.h_smem();
+	if (c.mode == MB_MODE_FUSED_FAST && m.incremental)
+	{
+		// per thread: state words, unstable masks and word rate sums in shared memory
+		constexpr size_t max_smem = 227 * 1024;
+		block = std::min(block, 128);
+		while (block > 32 && (size_t)12 * m.state_words * block + smem > max_smem)
+			block -= 32;
+		if ((size_t)12 * m.state_words * block + smem > max_smem)
+			throw engine_error(MB_ERR_LIMIT, "model too large for the incremental kernel's shared memory");
+		smem += (size_t)12 * m.state_words * block;
+	}
+	const int per_sm = c.blocks_per_sm > 0 ? c.blocks_per_sm : occupancy_blocks(f, block, smem);
+	const long long needed = (n + block - 1) / block;
 	const unsigned grid = (unsigned)std::max(1LL, std::min<long long>(needed, (long long)per_sm * m.ctx->sm_count));
 	void* args[] = { &P };
-	launch(f, grid, c.block, smem, s, args);
+	launch(f, grid, block, smem, s, args);
 }
 
 // Buffered epochs (simulation_runner.cu:54-180): simulate -> stats -> partition -> refill.
@@ -575,6 +628,7 @@ void run_epochs(module& m, const run_config& c, stats_state& st, long long n, cu
 	const int L = std::max(2, c.traj_len);
 	if (n <= 0)
 		return;
+	m.ensure(FAMILY_EPOCH);
 	const long long Bll = std::min<long long>(std::max(1, c.batch_limit), n);
 	const int B = (int)Bll;
 	dbuf st0((size_t)W * B * 4), st1((size_t)W * B * 4), t0((size_t)B * 4), t1((size_t)B * 4);

@@ -63,13 +63,24 @@ struct context
 	~context();
 };
 
-// Kernel handles resolved from an NVRTC-compiled module.
+// Kernel families, compiled (NVRTC) and loaded on first use: the generated per-node code is
+// inlined only into the kernels of the family that needs it.
+enum kernel_family : int
+{
+	FAMILY_EXACT = 0, // mb_fused_exact
+	FAMILY_FAST = 1,  // mb_fused_fast (incremental or dense)
+	FAMILY_EPOCH = 2, // mb_simulate_epoch
+	FAMILY_COUNT = 3
+};
+
+// Kernel handles resolved from NVRTC-compiled modules.
 struct module
 {
 	context* ctx = nullptr;
-	CUmodule mod = nullptr;
+	CUmodule mods[FAMILY_COUNT] = { nullptr, nullptr, nullptr };
 	int state_size = 0, state_words = 0;
 	int noninternal_count = -1; // from the generated code (mbg_noninternal_count), -1 if absent
+	bool incremental = false;	// fast mode uses the incremental kernel (generated MBG_INCREMENTAL)
 	bool has_layout = false; // compiled from a model (full layout known)
 	model_layout layout;
 	std::string source; // generated model source that was compiled with the engine
@@ -80,13 +91,16 @@ struct module
 	CUfunction window_epoch = nullptr, final_epoch = nullptr, fixed_epoch = nullptr;
 	CUfunction compact_count = nullptr, compact_scan = nullptr, compact_scatter = nullptr, fixed_extract = nullptr;
 
+	void ensure(int family);		// compile + load a family if needed (thread-safe)
+	void ensure_any();				// at least one family (the shared statistics kernels)
+	double compile_seconds = 0;		// NVRTC time spent so far
 	~module();
 };
 
 // Compile generated model code together with the engine kernels (NVRTC, -arch=sm_100a).
 std::unique_ptr<module> compile_module(context& ctx, const std::string& generated_code);
 // NVRTC compilation only (no device needed): returns the cubin, throws on failure.
-std::vector<char> compile_cubin(const std::string& generated_code, std::string& log);
+std::vector<char> compile_cubin(const std::string& generated_code, std::string& log, int family = FAMILY_FAST);
 
 void launch(CUfunction f, unsigned grid, unsigned block, size_t smem, cudaStream_t s, void** args);
 int occupancy_blocks(CUfunction f, int block, size_t smem);

@@ -677,6 +677,10 @@ struct compiled
 	std::vector<std::vector<int>> tt_in;
 	std::vector<std::vector<uint64_t>> tt;
 	bool nonneg = true;
+	// integer-rate fast mode (all rates of the @logic form, logic fan-in <= 12, enough resolution)
+	bool integer_rates = false;
+	int shift = 0;
+	std::vector<unsigned> q_up, q_down;
 	bool discrete = false;
 	float max_time_f = 0, tick_f = 0;	  // exact floats (window statistics)
 	float max_time_sim = 0, tick_sim = 0; // 6-significant-digit constexprs used by simulate
@@ -821,6 +825,38 @@ std::unique_ptr<compiled> compile(const std::string& bnd, const std::string& cfg
 		c->tt_in[i] = in;
 		c->tt[i] = t;
 	}
+	// integer-rate eligibility and fixed-point scale: largest per-32-node-word sum of
+	// max(up, down) below 2^31
+	c->integer_rates = c->N > 0;
+	for (int i = 0; i < c->N; i++)
+		if (!c->fast[i] || c->tt_in[i].size() > 12 || c->tt[i].empty())
+			c->integer_rates = false;
+	if (c->integer_rates)
+	{
+		double worst = 0;
+		for (int w = 0; w < c->W; w++)
+		{
+			double sw = 0;
+			for (int i = 32 * w; i < std::min(c->N, 32 * w + 32); i++)
+				sw += std::max((double)c->up[i], (double)c->down[i]);
+			worst = std::max(worst, sw);
+		}
+		int sh = 30;
+		while (sh > 0 && worst * std::ldexp(1.0, sh) >= 2147483648.0)
+			sh--;
+		c->shift = sh;
+		c->q_up.resize(c->N);
+		c->q_down.resize(c->N);
+		for (int i = 0; i < c->N; i++)
+		{
+			const double qu = std::nearbyint((double)c->up[i] * std::ldexp(1.0, sh));
+			const double qd = std::nearbyint((double)c->down[i] * std::ldexp(1.0, sh));
+			if ((c->up[i] > 0 && qu < 1024.0) || (c->down[i] > 0 && qd < 1024.0))
+				c->integer_rates = false;
+			c->q_up[i] = (unsigned)qu;
+			c->q_down[i] = (unsigned)qd;
+		}
+	}
 	c->discrete = c->constant("discrete_time") != 0;
 	c->max_time_f = c->constant("max_time");
 	c->tick_f = c->constant("time_tick");
@@ -834,6 +870,18 @@ std::unique_ptr<compiled> compile(const std::string& bnd, const std::string& cfg
 
 // ------------------------------------------------------------------ simulation
 
+// static_state_t::operator< (state.h:43-49): compare from the highest word down
+struct state_less
+{
+	bool operator()(const std::vector<uint32_t>& a, const std::vector<uint32_t>& b) const
+	{
+		for (size_t w = a.size(); w-- > 0;)
+			if (a[w] != b[w])
+				return a[w] < b[w];
+		return false;
+	}
+};
+
 struct sinks
 {
 	int T = 0;
@@ -841,7 +889,7 @@ struct sinks
 	double fx = 1, fxh = 1;
 	std::vector<long long> occ, h;
 	std::vector<unsigned> cnt, fin;
-	std::map<std::vector<uint32_t>, unsigned> fixed;
+	std::map<std::vector<uint32_t>, unsigned, state_less> fixed;
 	unsigned long long transitions = 0;
 };
 
@@ -970,6 +1018,99 @@ float entropy_fast(const compiled& c, const float* rates, const uint32_t* s)
 
 // One trajectory (simulation.cu:34-71 initial state, :77-164 loop; simulation_runner.cu:104-162
 // epochs). `trace` (optional) receives (flip, time) per step.
+// Fast mode with integer rates (the engine's incremental kernel): rates in fixed point
+// q = round(rate * 2^shift), the flip drawn as the first node (in node order) whose cumulative
+// integer rate exceeds r = floor(u64 * total / 2^64), u64 from two raw 32-bit draws.
+void trajectory_integer(const compiled& c, sinks& s, curandStatePhilox4_32_10_t& rng, run_acc& acc,
+						unsigned long long& trans, std::vector<std::pair<int, float>>* trace)
+{
+	std::vector<uint32_t> st(c.W, 0u);
+	std::vector<float> rates(c.N);
+	std::vector<unsigned> q(c.N);
+	for (int i = 0; i < c.N; i++)
+		if (curand_uniform(&rng) <= c.m.nodes[i].istate)
+			st[i / 32] |= 1u << (i % 32);
+	const float inv_scale = 1.0f / (float)(1u << c.shift);
+	float time = 0.f;
+	bool fixed = false;
+	for (;;)
+	{
+		unsigned long long total = 0;
+		for (int i = 0; i < c.N; i++)
+		{
+			rates[i] = c.rate(i, st.data());
+			q[i] = 0;
+		}
+		for (int i = 0; i < c.N; i++)
+		{
+			const bool on = (st[i / 32] >> (i % 32)) & 1u;
+			// unstable <=> bit differs from logic <=> the generated rate takes the U/D branch
+			unsigned p = 0;
+			const std::vector<int>& in = c.tt_in[i];
+			for (size_t k = 0; k < in.size(); k++)
+				p |= ((st[in[k] / 32] >> (in[k] % 32)) & 1u) << k;
+			const bool lg = (c.tt[i][p >> 6] >> (p & 63)) & 1u;
+			if (on != lg)
+				q[i] = on ? c.q_down[i] : c.q_up[i];
+			total += q[i];
+		}
+		float h = 0.f, tn;
+		if (total == 0)
+		{
+			fixed = true;
+			tn = c.max_time_sim;
+		}
+		else
+		{
+			if (c.discrete)
+			{
+				tn = time + c.tick_sim;
+				tn = c.max_time_sim - c.tick_sim < tn ? c.max_time_sim : tn;
+			}
+			else
+			{
+				const float total_f = (float)total * inv_scale;
+				tn = time + -logf(curand_uniform(&rng)) / total_f;
+			}
+			tn = std::fmin(tn, c.max_time_sim);
+			h = entropy_fast(c, rates.data(), st.data());
+		}
+		trans += tn != 0.f;
+		record(c, s, acc, c.ni_index(st.data()), time, tn, h);
+		time = tn;
+		if (time >= c.max_time_sim)
+		{
+			if (trace)
+				trace->emplace_back(-1, time);
+			break;
+		}
+		const unsigned hi = curand(&rng);
+		const unsigned lo = curand(&rng);
+		const unsigned long long r64 = ((unsigned long long)hi << 32) | lo;
+		const unsigned long long r = (unsigned long long)(((unsigned __int128)r64 * total) >> 64);
+		unsigned long long cum = 0;
+		int j = -1;
+		for (int i = 0; i < c.N; i++)
+		{
+			cum += q[i];
+			if (r < cum)
+			{
+				j = i;
+				break;
+			}
+		}
+		if (trace)
+			trace->emplace_back(j, time);
+		st[j / 32] ^= 1u << (j % 32);
+	}
+	atomic_add(&s.fin[c.ni_index(st.data())], 1u);
+	if (fixed)
+	{
+#pragma omp critical(oracle_fixed)
+		s.fixed[st]++;
+	}
+}
+
 template <typename RNG>
 void trajectory(const compiled& c, sinks& s, RNG& rng, bool exact, int traj_len, run_acc& acc,
 				unsigned long long& trans, std::vector<std::pair<int, float>>* trace)
@@ -1106,6 +1247,14 @@ int oracle_model_dims(const oracle_model* m, int* nodes, int* words, int* nonint
 	return 0;
 }
 
+// 1 when fast mode uses integer rates (the engine's incremental kernel); writes the scale
+int oracle_model_integer_rates(const oracle_model* m, int* shift)
+{
+	if (shift)
+		*shift = m->c->shift;
+	return m->c->integer_rates ? 1 : 0;
+}
+
 int oracle_model_noninternal(const oracle_model* m, int* out)
 {
 	for (size_t k = 0; k < m->c->ni.size(); k++)
@@ -1157,7 +1306,10 @@ oracle_result* oracle_run(const oracle_model* m, int mode, long long n, unsigned
 			{
 				curandStatePhilox4_32_10_t rng;
 				curand_init(seed, first + (unsigned long long)t, 0ull, &rng);
-				trajectory(c, s, rng, false, 0, acc, trans, nullptr);
+				if (c.integer_rates)
+					trajectory_integer(c, s, rng, acc, trans, nullptr);
+				else
+					trajectory(c, s, rng, false, 0, acc, trans, nullptr);
 			}
 		}
 		acc.flush(s);
@@ -1232,7 +1384,10 @@ int oracle_trace(const oracle_model* m, int mode, unsigned long long seed, unsig
 	{
 		curandStatePhilox4_32_10_t rng;
 		curand_init(seed, traj, 0ull, &rng);
-		trajectory(c, s, rng, false, 0, acc, trans, &tr);
+		if (c.integer_rates)
+			trajectory_integer(c, s, rng, acc, trans, &tr);
+		else
+			trajectory(c, s, rng, false, 0, acc, trans, &tr);
 	}
 	for (int i = 0; i < (int)tr.size() && i < cap; i++)
 	{

@@ -66,11 +66,32 @@ def test_exact_mode_matches_oracle_on_synthetic_networks(gpu, gen, kw, n):
     _assert_same(res, raw, ref, o.discrete)
 
 
-@pytest.mark.parametrize("name,n", [("cellcycle", 5_000), ("sizek", 1_000)])
+@pytest.mark.parametrize("name,n", [("cellcycle", 5_000), ("sizek", 1_000), ("metastasis", 1_000),
+                                    ("Montagud2022_Prostate_Cancer", 2_000)])
 def test_fast_mode_matches_oracle_fast_mode(gpu, name, n):
+    """Fast mode (incremental kernel: Philox streams, integer rates) against the oracle's
+    restatement of the same algorithm."""
     bnd, cfg = model_text(name)
     model, res, raw, o, ref = _run_both(gpu, bnd, cfg, n, mode="fast")
     _assert_same(res, raw, ref, o.discrete)
+
+
+@pytest.mark.parametrize("gen,kw,n", [(synth.c1, {}, 20_000), (synth.c2, dict(noninternal=20), 500),
+                                      (synth.c2, dict(noninternal=12, discrete=True), 2_000),
+                                      (synth.c4, {}, 3_000), (synth.c3, {}, 300)])
+def test_fast_mode_matches_oracle_on_synthetic_networks(gpu, gen, kw, n):
+    bnd, cfg = gen(**kw)
+    model, res, raw, o, ref = _run_both(gpu, bnd, cfg, n, mode="fast")
+    _assert_same(res, raw, ref, o.discrete)
+
+
+def test_fast_mode_dense_kernel_for_general_rates(gpu):
+    """Rates that are not of the @logic form use the dense fast kernel (float rates)."""
+    bnd = "".join(f"node Z{i} {{ logic = !Z{(i + 1) % 6}; rate_up = Z{(i + 2) % 6} ? 2 : 0.5; "
+                  f"rate_down = @logic ? 0 : 1.5; }}\n" for i in range(6))
+    cfg = "max_time = 4; time_tick = 0.25; sample_count = 3000;"
+    model, res, raw, o, ref = _run_both(gpu, bnd, cfg, 3000, mode="fast")
+    _assert_same(res, raw, ref, False)
 
 
 @pytest.mark.parametrize("name,n", [("cellcycle", 3_000), ("metastasis", 1_000), ("sizek", 1_500)])
