@@ -404,10 +404,74 @@ __device__ __forceinline__ float mb_incr_entropy(const mb_incr_view& v)
 	return h > 0.f ? h : 0.f;
 }
 
+// Warp-cooperative start of trajectory `t` for the lane whose shared-memory column is `col`:
+// lane l draws the initial bit of node 32w + l (Philox is counter based, so the uniform of node
+// i is output i of the trajectory's stream, as in a sequential draw), evaluates its logic and
+// rate, and the words, unstable masks and word sums are assembled with warp votes/reductions.
+// Returns (through the references, valid in every lane) the group sums, total and the index of
+// the non-internal state.
+__device__ __forceinline__ void mb_incr_start(const mb_fused_params& P, const mb_incr_view& v0, int col,
+											  unsigned long long t, unsigned long long (&gs)[MB_GROUPS],
+											  unsigned long long& total, uint32_t& idx)
+{
+	const int lane = threadIdx.x & 31;
+	mb_incr_view v = v0;
+	v.st = v0.st - (threadIdx.x - col);
+	v.un = v0.un - (threadIdx.x - col);
+	v.ws = v0.ws - (threadIdx.x - col);
+	for (int w = 0; w < state_words; w++)
+	{
+		const int i = 32 * w + lane;
+		bool on = false;
+		if (i < state_size)
+		{
+			curandStatePhilox4_32_10_t r;
+			curand_init(P.seed, P.first_traj + t, (unsigned long long)i, &r);
+			on = curand_uniform(&r) <= __ldg(P.istate + i);
+		}
+		const uint32_t word = __ballot_sync(0xffffffffu, on);
+		if (lane == 0)
+			v.S(w) = word;
+	}
+	__syncwarp();
+#pragma unroll
+	for (int g = 0; g < MB_GROUPS; g++)
+		gs[g] = 0;
+	total = 0;
+	idx = 0;
+	for (int w = 0; w < state_words; w++)
+	{
+		const int i = 32 * w + lane;
+		const uint32_t sw = v.S(w);
+		const bool on = (sw >> lane) & 1u;
+		bool unstable = false;
+		uint32_t q = 0, nibit = 0;
+		if (i < state_size)
+		{
+			unstable = on != mb_incr_logic(v, i);
+			q = unstable ? (on ? __ldg(mbg_inc_q_down + i) : __ldg(mbg_inc_q_up + i)) : 0u;
+			const int pos = __ldg(mbg_inc_ni_pos + i);
+			nibit = (pos >= 0 && on) ? (1u << pos) : 0u;
+		}
+		const uint32_t um = __ballot_sync(0xffffffffu, unstable);
+		const uint32_t qw = __reduce_add_sync(0xffffffffu, q);
+		idx |= __reduce_or_sync(0xffffffffu, nibit);
+		if (lane == 0)
+		{
+			v.U(w) = um;
+			v.Q(w) = qw;
+		}
+		mb_group_add(gs, w / MB_WPG, qw);
+		total += qw;
+	}
+	__syncwarp();
+}
+
 extern "C" __global__ void __launch_bounds__(128) mb_fused_fast(mb_fused_params P)
 {
 	extern __shared__ uint32_t mb_smem_u32[];
 	const int B = blockDim.x;
+	const int lane = threadIdx.x & 31;
 	mb_incr_view v;
 	v.stride = B;
 	v.st = mb_smem_u32 + threadIdx.x;
@@ -427,66 +491,63 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_fast(mb_fused_params 
 	unsigned long long trans = 0;
 	mb_win_acc acc;
 	mb_acc_init(acc);
-	for (;;)
+
+	// per-lane trajectory registers
+	bool working = true;  // the work counter is not exhausted for this lane
+	bool running = false; // the lane holds a trajectory
+	unsigned long long gs[MB_GROUPS];
+	unsigned long long total = 0;
+	uint32_t idx = 0;
+	float time = 0.f, h = 0.f;
+	curandStatePhilox4_32_10_t rng;
+
+	// The warp stays converged at the top of every iteration: lanes that need a trajectory take
+	// one from the work counter and the whole warp initialises them together; then every lane
+	// with a trajectory performs one Gillespie step.
+	while (__any_sync(0xffffffffu, working || running))
 	{
-		const unsigned long long t = atomicAdd(P.next_traj, 1ull);
-		if (t >= P.n_traj)
-			break;
-		curandStatePhilox4_32_10_t rng;
-		curand_init(P.seed, P.first_traj + t, 0ull, &rng);
-
-		// initial state, unstable masks, word / group / total rate sums
-		for (int w = 0; w < state_words; w++)
+		unsigned long long t = 0;
+		bool starting = false;
+		if (working && !running)
 		{
-			uint32_t s = 0;
-			const int nb = (w == state_words - 1) ? state_size - 32 * w : 32;
-			for (int b = 0; b < nb; b++)
-				if (curand_uniform(&rng) <= __ldg(P.istate + 32 * w + b))
-					s |= 1u << b;
-			v.S(w) = s;
+			t = atomicAdd(P.next_traj, 1ull);
+			if (t < P.n_traj)
+				starting = true;
+			else
+				working = false;
 		}
-		unsigned long long gs[MB_GROUPS];
-#pragma unroll
-		for (int g = 0; g < MB_GROUPS; g++)
-			gs[g] = 0;
-		unsigned long long total = 0;
-		uint32_t idx = 0;
-		for (int w = 0; w < state_words; w++)
+		unsigned pending = __ballot_sync(0xffffffffu, starting);
+		while (pending)
 		{
-			const uint32_t sw = v.S(w);
-			uint32_t uw = 0, qw = 0;
-			const int nb = (w == state_words - 1) ? state_size - 32 * w : 32;
-			for (int b = 0; b < nb; b++)
+			const int src = __ffs(pending) - 1;
+			pending &= pending - 1u;
+			const unsigned long long ts = __shfl_sync(0xffffffffu, t, src);
+			unsigned long long gsx[MB_GROUPS];
+			unsigned long long tot;
+			uint32_t ix;
+			mb_incr_start(P, v, (threadIdx.x & ~31) + src, ts, gsx, tot, ix);
+			if (lane == src)
 			{
-				const int i = 32 * w + b;
-				const bool on = (sw >> b) & 1u;
-				if (on != mb_incr_logic(v, i))
-				{
-					uw |= 1u << b;
-					qw += on ? __ldg(mbg_inc_q_down + i) : __ldg(mbg_inc_q_up + i);
-				}
-				const int pos = __ldg(mbg_inc_ni_pos + i);
-				if (pos >= 0 && on)
-					idx |= 1u << pos;
+#pragma unroll
+				for (int g = 0; g < MB_GROUPS; g++)
+					gs[g] = gsx[g];
+				total = tot;
+				idx = ix;
 			}
-			v.U(w) = uw;
-			v.Q(w) = qw;
-			mb_group_add(gs, w / MB_WPG, qw);
-			total += qw;
 		}
-		float h = mb_incr_entropy(v);
+		if (starting)
+		{
+			curand_init(P.seed, P.first_traj + t, (unsigned long long)state_size, &rng);
+			h = mb_incr_entropy(v);
+			time = 0.f;
+			running = true;
+		}
 
-		float time = 0.f;
-		bool fixed = false;
-		for (;;)
+		if (running)
 		{
 			float tn;
-			const float total_f = (float)total * inv_scale;
 			if (total == 0)
-			{
-				fixed = true;
 				tn = max_time;
-			}
 			else
 			{
 				if (discrete_time)
@@ -495,7 +556,7 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_fast(mb_fused_params 
 					tn = max_time - time_tick < tn ? max_time : tn;
 				}
 				else
-					tn = time + -logf(curand_uniform(&rng)) / total_f;
+					tn = time + -logf(curand_uniform(&rng)) / ((float)total * inv_scale);
 				tn = fminf(tn, max_time);
 			}
 			trans += (tn != 0.f) ? 1ull : 0ull;
@@ -508,104 +569,109 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_fast(mb_fused_params 
 			}
 			time = tn;
 			if (time >= max_time)
-				break;
-
-			// draw the flip: r uniform in [0, total), then group -> word -> node
-			const unsigned hi = curand(&rng);
-			const unsigned lo = curand(&rng);
-			const unsigned long long r64 = ((unsigned long long)hi << 32) | lo;
-			const unsigned long long r = __umul64hi(r64, total);
-			unsigned long long cum = 0;
-			int g = -1;
-#pragma unroll
-			for (int i = 0; i < MB_GROUPS; i++)
 			{
-				const bool hit = g < 0 && r < cum + gs[i];
-				g = hit ? i : g;
-				cum += (g < 0) ? gs[i] : 0ull;
-			}
-			if (g < 0)
-				g = MB_GROUPS - 1; // unreachable: sum of gs is total
-			int word = g * MB_WPG;
-			for (int i = 0; i < MB_WPG; i++)
-			{
-				const int w = g * MB_WPG + i;
-				if (w >= state_words)
-					break;
-				word = w;
-				const uint32_t q = v.Q(w);
-				if (r < cum + q)
-					break;
-				cum += q;
-			}
-			const uint32_t sw = v.S(word);
-			uint32_t um = v.U(word);
-			int j = 32 * word + 31 - __clz(um | 1u);
-			while (um)
-			{
-				const int b = __ffs(um) - 1;
-				const int i = 32 * word + b;
-				const uint32_t q = ((sw >> b) & 1u) ? __ldg(mbg_inc_q_down + i) : __ldg(mbg_inc_q_up + i);
-				if (r < cum + q)
+				// end of the trajectory: final state, fixed point
+				running = false;
+				atomicAdd(P.st.final_cnt + idx, 1u);
+				if (total == 0)
 				{
-					j = i;
-					break;
-				}
-				cum += q;
-				um &= um - 1u;
-			}
-
-			// flip j and re-evaluate it and its dependents
-			v.S(j >> 5) ^= 1u << (j & 31);
-			const int pj = __ldg(mbg_inc_ni_pos + j);
-			if (pj >= 0)
-				idx ^= 1u << pj;
-			bool ni_changed = pj >= 0;
-			const int d0 = __ldg(mbg_inc_dep_ptr + j), d1 = __ldg(mbg_inc_dep_ptr + j + 1);
-			for (int d = d0; d < d1; d++)
-			{
-				const int k = __ldg(mbg_inc_dep_idx + d);
-				const int wk = k >> 5;
-				const uint32_t bk = 1u << (k & 31);
-				const bool on = (v.S(wk) & bk) != 0;
-				const bool was_on = (k == j) ? !on : on;
-				const uint32_t uw = v.U(wk);
-				const bool was_unstable = (uw & bk) != 0;
-				const bool unstable = on != mb_incr_logic(v, k);
-				const uint32_t qo = was_unstable ? (was_on ? __ldg(mbg_inc_q_down + k) : __ldg(mbg_inc_q_up + k)) : 0u;
-				const uint32_t qn = unstable ? (on ? __ldg(mbg_inc_q_down + k) : __ldg(mbg_inc_q_up + k)) : 0u;
-				if (unstable != was_unstable)
-					v.U(wk) = uw ^ bk;
-				if (qn != qo)
-				{
-					const long long dq = (long long)qn - (long long)qo;
-					v.Q(wk) += (uint32_t)dq;
-					mb_group_add(gs, wk / MB_WPG, dq);
-					total += (unsigned long long)dq;
-					ni_changed |= __ldg(mbg_inc_ni_pos + k) >= 0;
-				}
-				else if (unstable != was_unstable)
-					ni_changed |= __ldg(mbg_inc_ni_pos + k) >= 0;
-			}
-			if (ni_changed)
-				h = mb_incr_entropy(v);
-		}
-		atomicAdd(P.st.final_cnt + idx, 1u);
-		if (fixed)
-		{
-			state_word_t st[state_words];
+					state_word_t st[state_words];
 #pragma unroll
-			for (int w = 0; w < state_words; w++)
-				st[w] = v.S(w);
-			mb_fixed_insert(P.st, st);
+					for (int w = 0; w < state_words; w++)
+						st[w] = v.S(w);
+					mb_fixed_insert(P.st, st);
+				}
+			}
+			else
+			{
+				// draw the flip: r uniform in [0, total), then group -> word -> node
+				const unsigned hi = curand(&rng);
+				const unsigned lo = curand(&rng);
+				const unsigned long long r = __umul64hi(((unsigned long long)hi << 32) | lo, total);
+				unsigned long long cum = 0;
+				int g = -1;
+#pragma unroll
+				for (int i = 0; i < MB_GROUPS; i++)
+				{
+					const bool hit = g < 0 && r < cum + gs[i];
+					g = hit ? i : g;
+					cum += (g < 0) ? gs[i] : 0ull;
+				}
+				if (g < 0)
+					g = MB_GROUPS - 1; // unreachable: the group sums add up to total
+				int word = g * MB_WPG;
+				for (int i = 0; i < MB_WPG; i++)
+				{
+					const int w = g * MB_WPG + i;
+					if (w >= state_words)
+						break;
+					word = w;
+					const uint32_t q = v.Q(w);
+					if (r < cum + q)
+						break;
+					cum += q;
+				}
+				const uint32_t sw = v.S(word);
+				uint32_t um = v.U(word);
+				int j = 32 * word + 31 - __clz(um | 1u);
+				while (um)
+				{
+					const int b = __ffs(um) - 1;
+					const int i = 32 * word + b;
+					const uint32_t q = ((sw >> b) & 1u) ? __ldg(mbg_inc_q_down + i) : __ldg(mbg_inc_q_up + i);
+					if (r < cum + q)
+					{
+						j = i;
+						break;
+					}
+					cum += q;
+					um &= um - 1u;
+				}
+
+				// flip j and re-evaluate it and the nodes whose logic reads it
+				v.S(j >> 5) ^= 1u << (j & 31);
+				const int pj = __ldg(mbg_inc_ni_pos + j);
+				if (pj >= 0)
+					idx ^= 1u << pj;
+				bool ni_changed = pj >= 0;
+				const int d0 = __ldg(mbg_inc_dep_ptr + j), d1 = __ldg(mbg_inc_dep_ptr + j + 1);
+				for (int d = d0; d < d1; d++)
+				{
+					const int k = __ldg(mbg_inc_dep_idx + d);
+					const int wk = k >> 5;
+					const uint32_t bk = 1u << (k & 31);
+					const bool on = (v.S(wk) & bk) != 0;
+					const bool was_on = (k == j) ? !on : on;
+					const uint32_t uw = v.U(wk);
+					const bool was_unstable = (uw & bk) != 0;
+					const bool unstable = on != mb_incr_logic(v, k);
+					const uint32_t qo =
+						was_unstable ? (was_on ? __ldg(mbg_inc_q_down + k) : __ldg(mbg_inc_q_up + k)) : 0u;
+					const uint32_t qn = unstable ? (on ? __ldg(mbg_inc_q_down + k) : __ldg(mbg_inc_q_up + k)) : 0u;
+					if (unstable != was_unstable)
+						v.U(wk) = uw ^ bk;
+					if (qn != qo)
+					{
+						const long long dq = (long long)qn - (long long)qo;
+						v.Q(wk) += (uint32_t)dq;
+						mb_group_add(gs, wk / MB_WPG, dq);
+						total += (unsigned long long)dq;
+					}
+					if (qn != qo || unstable != was_unstable)
+						ni_changed |= __ldg(mbg_inc_ni_pos + k) >= 0;
+				}
+				if (ni_changed)
+					h = mb_incr_entropy(v);
+			}
 		}
+		__syncwarp();
 	}
 	mb_acc_flush(acc, P.st, hsink);
 
 #pragma unroll
 	for (int o = 16; o > 0; o >>= 1)
 		trans += __shfl_down_sync(0xffffffffu, trans, o);
-	if ((threadIdx.x & 31) == 0 && trans)
+	if (lane == 0 && trans)
 		atomicAdd(P.transitions, trans);
 
 	if (P.st.h_in_smem)

@@ -314,6 +314,10 @@ void launch(CUfunction f, unsigned grid, unsigned block, size_t smem, cudaStream
 int occupancy_blocks(CUfunction f, int block, size_t smem)
 {
 	int n = 0;
+	// the occupancy calculator counts dynamic shared memory above 48 KB only after the opt-in
+	if (smem > 48 * 1024)
+		cu_throw(drv().FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem),
+				 "cuFuncSetAttribute");
 	cu_throw(drv().OccupancyMaxActiveBlocksPerMultiprocessor(&n, f, block, smem), "cuOccupancyMaxActiveBlocks");
 	return std::max(n, 1);
 }

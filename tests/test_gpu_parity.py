@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import maboss.gpu_b200 as mb
-from conftest import model_text, pooled_z
+from conftest import assert_statistically_equal, model_text
 from maboss.gpu_b200 import synth
 from oracle.oracle import OracleModel
 
@@ -125,10 +125,8 @@ def test_fast_mode_statistically_equivalent_to_exact(gpu):
     mod = gpu.compile(model)
     n = 100_000
     a, b = mod.run(mode="exact", sample_count=n), mod.run(mode="fast", sample_count=n)
-    z = pooled_z(a.window_probs.ravel(), n, b.window_probs.ravel(), n)
-    assert z.max() < 4.5
-    zf = pooled_z(a.final_counts / n, n, b.final_counts / n, n)
-    assert zf.max() < 4.5
+    assert_statistically_equal(a.window_probs, n, b.window_probs, n)
+    assert_statistically_equal(a.final_counts / n, n, b.final_counts / n, n)
 
 
 def test_results_are_reproducible(gpu):
@@ -189,9 +187,12 @@ def test_edge_cases(gpu):
     assert r0.final_counts.sum() == 0 and r0.transitions == 0
     r1 = mod.run(sample_count=1)
     assert r1.final_counts.sum() == 1
-    # every node internal: a single bin
+    # every node internal: a single bin (the first is_internal attribute of a node wins, so the
+    # model's own declarations are removed first)
+    import re
+    stripped = re.sub(r"(?m)^\s*\w+\.is_internal\s*=.*$", "", cfg)
     allint = "\n".join(f"{n}.is_internal = 1;" for n in model.node_names)
-    m2 = mb.Model(bnd, cfg + allint)
+    m2 = mb.Model(bnd, stripped + allint)
     r2 = gpu.compile(m2).run(sample_count=500)
     assert r2.dims.bins == 1 and r2.final_counts[0] == 500
     assert np.allclose(r2.window_probs[:, 0], 1.0, atol=1e-5)
