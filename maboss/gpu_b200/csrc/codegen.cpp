@@ -229,7 +229,13 @@ void emit_array(std::ostream& os, const char* type, const char* name, const std:
 	os << "};" << std::endl;
 }
 
-// Tables of the incremental fast-mode kernel (see kernels/engine.cuh: mb_fused_incr).
+// Tables of the incremental fast-mode kernel (kernels/engine.cuh, MBG_INCREMENTAL):
+//   mbg_inc_node[i]   = {q_up, q_down, first dependent record, dependents | (ni_pos + 1) << 16}
+//   dependent records (node i's own logic record first is not assumed; mbg_inc_self[i] points to it):
+//   mbg_inc_rec_hdr[r] = {k | m << 16 | (ni_pos(k) + 1) << 21, q_up(k), q_down(k), truth table or offset}
+//   mbg_inc_rec_in[r]  = inputs 0..7 of k's logic as 16-bit node indices, mbg_inc_rec_in2[r] = inputs 8..15
+// The truth table of k is inline when it has at most 5 inputs (32 patterns), else an offset into
+// mbg_inc_tt. Records keep everything one dependent re-evaluation needs in two 16-byte loads.
 void emit_incremental_tables(std::ostream& ss, const model_layout& L)
 {
 	ss << std::endl << "// ---- incremental engine tables" << std::endl;
@@ -239,36 +245,61 @@ void emit_incremental_tables(std::ostream& ss, const model_layout& L)
 		return;
 	}
 	const int N = L.state_size;
-	ss << "#define MBG_INCREMENTAL 1" << std::endl;
-	ss << "constexpr int mbg_inc_rate_shift = " << L.rate_shift << ";" << std::endl;
-	emit_array(ss, "unsigned", "mbg_inc_q_up", L.q_up);
-	emit_array(ss, "unsigned", "mbg_inc_q_down", L.q_down);
-	emit_array(ss, "int", "mbg_inc_dep_ptr", L.dep_ptr);
-	emit_array(ss, "int", "mbg_inc_dep_idx", L.dep_idx);
-	emit_array(ss, "int", "mbg_inc_in_ptr", L.in_ptr);
-	emit_array(ss, "int", "mbg_inc_in_idx", L.in_idx);
-	emit_array(ss, "int", "mbg_inc_tt_ptr", L.tt_ptr);
-	emit_array(ss, "unsigned", "mbg_inc_tt", L.tt_words);
 	std::vector<int> ni_pos(N, -1);
 	for (size_t k = 0; k < L.noninternal_nodes.size(); k++)
 		ni_pos[L.noninternal_nodes[k]] = (int)k;
-	emit_array(ss, "int", "mbg_inc_ni_pos", ni_pos);
-	std::vector<float> ni_up, ni_down, ni_ul, ni_dl;
+
+	std::vector<std::string> node, hdr, in1, in2;
+	std::vector<unsigned> tt_big;
+	std::vector<int> self(N, -1);
+	auto u4 = [](unsigned a, unsigned b, unsigned c, unsigned d) {
+		return "{" + std::to_string(a) + "u, " + std::to_string(b) + "u, " + std::to_string(c) + "u, " +
+			   std::to_string(d) + "u}";
+	};
+	for (int j = 0; j < N; j++)
+	{
+		const int d0 = L.dep_ptr[j], d1 = L.dep_ptr[j + 1];
+		node.push_back(u4(L.q_up[j], L.q_down[j], (unsigned)d0, (unsigned)(d1 - d0) | ((unsigned)(ni_pos[j] + 1) << 16)));
+		for (int d = d0; d < d1; d++)
+		{
+			const int k = L.dep_idx[d];
+			if (k == j)
+				self[j] = d;
+			const int a0 = L.in_ptr[k], m = L.in_ptr[k + 1] - a0;
+			unsigned tt;
+			const int t0 = L.tt_ptr[k], nt = L.tt_ptr[k + 1] - t0;
+			if (m <= 5)
+				tt = L.tt_words[t0];
+			else
+			{
+				tt = (unsigned)tt_big.size();
+				tt_big.insert(tt_big.end(), L.tt_words.begin() + t0, L.tt_words.begin() + t0 + nt);
+			}
+			hdr.push_back(u4((unsigned)k | ((unsigned)m << 16) | ((unsigned)(ni_pos[k] + 1) << 21), L.q_up[k],
+							 L.q_down[k], tt));
+			unsigned in[16] = { 0 };
+			for (int t = 0; t < m; t++)
+				in[t] = (unsigned)L.in_idx[a0 + t];
+			in1.push_back(u4(in[0] | in[1] << 16, in[2] | in[3] << 16, in[4] | in[5] << 16, in[6] | in[7] << 16));
+			in2.push_back(u4(in[8] | in[9] << 16, in[10] | in[11] << 16, in[12] | in[13] << 16, in[14] | in[15] << 16));
+		}
+	}
+	ss << "#define MBG_INCREMENTAL 1" << std::endl;
+	ss << "constexpr int mbg_inc_rate_shift = " << L.rate_shift << ";" << std::endl;
+	emit_array(ss, "uint4", "mbg_inc_node", node);
+	emit_array(ss, "uint4", "mbg_inc_rec_hdr", hdr);
+	emit_array(ss, "uint4", "mbg_inc_rec_in", in1);
+	emit_array(ss, "uint4", "mbg_inc_rec_in2", in2);
+	emit_array(ss, "unsigned", "mbg_inc_tt", tt_big);
+	emit_array(ss, "int", "mbg_inc_self", self);
+	std::vector<std::string> f_up, f_down, f_ul, f_dl;
 	for (int i : L.noninternal_nodes)
 	{
 		const double u = L.up[i], d = L.down[i];
-		ni_up.push_back(L.up[i]);
-		ni_down.push_back(L.down[i]);
-		ni_ul.push_back(u > 0 ? (float)(u * std::log2(u)) : 0.f);
-		ni_dl.push_back(d > 0 ? (float)(d * std::log2(d)) : 0.f);
-	}
-	std::vector<std::string> f_up, f_down, f_ul, f_dl;
-	for (size_t k = 0; k < ni_up.size(); k++)
-	{
-		f_up.push_back(flit(ni_up[k]));
-		f_down.push_back(flit(ni_down[k]));
-		f_ul.push_back(flit(ni_ul[k]));
-		f_dl.push_back(flit(ni_dl[k]));
+		f_up.push_back(flit(L.up[i]));
+		f_down.push_back(flit(L.down[i]));
+		f_ul.push_back(flit(u > 0 ? (float)(u * std::log2(u)) : 0.f));
+		f_dl.push_back(flit(d > 0 ? (float)(d * std::log2(d)) : 0.f));
 	}
 	emit_array(ss, "float", "mbg_inc_ni_up", f_up);
 	emit_array(ss, "float", "mbg_inc_ni_down", f_down);
@@ -337,7 +368,7 @@ model_layout analyze_model(const model_t& m)
 	}
 
 	// incremental tables (fast-path models with small logic fan-in only)
-	L.incremental_ok = L.all_fast_path;
+	L.incremental_ok = L.all_fast_path && N <= 65535;
 	constexpr int max_inputs = 12;
 	if (L.incremental_ok)
 	{

@@ -350,7 +350,7 @@ extern "C" __global__ void __launch_bounds__(256) mb_fused_fast(mb_fused_params 
 // is drawn exactly in proportion to the integer rates with a 64-bit uniform; waiting times and
 // window slices are computed as in the other kernels. Statistically equivalent to the
 // reference; not bit-exact (different random streams and rate rounding below 2^-shift).
-constexpr int MB_WPG = state_words <= 2 ? 1 : (state_words <= 8 ? 2 : 4);
+constexpr int MB_WPG = state_words <= 2 ? 1 : (state_words <= 8 ? 2 : 8);
 constexpr int MB_GROUPS = (state_words + MB_WPG - 1) / MB_WPG;
 
 struct mb_incr_view
@@ -364,16 +364,37 @@ struct mb_incr_view
 	__device__ __forceinline__ uint32_t& Q(int w) const { return ws[w * stride]; }
 };
 
-__device__ __forceinline__ bool mb_incr_logic(const mb_incr_view& v, int k)
+// Logic value of the node of dependent record `hdr`/`in` in the state held by view `v`.
+__device__ __forceinline__ bool mb_incr_logic(const mb_incr_view& v, int r, const uint4& hdr, const uint4& in)
 {
-	const int a = __ldg(mbg_inc_in_ptr + k), b = __ldg(mbg_inc_in_ptr + k + 1);
+	const int m = (hdr.x >> 16) & 31;
+	const unsigned ins[4] = { in.x, in.y, in.z, in.w };
 	unsigned p = 0;
-	for (int t = a; t < b; t++)
+#pragma unroll
+	for (int t = 0; t < 8; t++)
 	{
-		const int in = __ldg(mbg_inc_in_idx + t);
-		p |= ((v.S(in >> 5) >> (in & 31)) & 1u) << (t - a);
+		if (t < m)
+		{
+			const unsigned node = (ins[t >> 1] >> ((t & 1) * 16)) & 0xffffu;
+			p |= ((v.S(node >> 5) >> (node & 31)) & 1u) << t;
+		}
 	}
-	return (__ldg(mbg_inc_tt + __ldg(mbg_inc_tt_ptr + k) + (p >> 5)) >> (p & 31)) & 1u;
+	if (m > 8)
+	{
+		const uint4 in2 = __ldg(mbg_inc_rec_in2 + r);
+		const unsigned ins2[4] = { in2.x, in2.y, in2.z, in2.w };
+#pragma unroll
+		for (int t = 8; t < 16; t++)
+		{
+			if (t < m)
+			{
+				const unsigned node = (ins2[(t - 8) >> 1] >> ((t & 1) * 16)) & 0xffffu;
+				p |= ((v.S(node >> 5) >> (node & 31)) & 1u) << t;
+			}
+		}
+	}
+	const unsigned ttw = m <= 5 ? hdr.w : __ldg(mbg_inc_tt + hdr.w + (p >> 5));
+	return (ttw >> (p & 31)) & 1u;
 }
 
 __device__ __forceinline__ void mb_group_add(unsigned long long (&gs)[MB_GROUPS], int g, long long d)
@@ -448,9 +469,11 @@ __device__ __forceinline__ void mb_incr_start(const mb_fused_params& P, const mb
 		uint32_t q = 0, nibit = 0;
 		if (i < state_size)
 		{
-			unstable = on != mb_incr_logic(v, i);
-			q = unstable ? (on ? __ldg(mbg_inc_q_down + i) : __ldg(mbg_inc_q_up + i)) : 0u;
-			const int pos = __ldg(mbg_inc_ni_pos + i);
+			const int r = __ldg(mbg_inc_self + i);
+			const uint4 hdr = __ldg(mbg_inc_rec_hdr + r);
+			unstable = on != mb_incr_logic(v, r, hdr, __ldg(mbg_inc_rec_in + r));
+			q = unstable ? (on ? hdr.z : hdr.y) : 0u;
+			const int pos = (int)((hdr.x >> 21) & 31u) - 1;
 			nibit = (pos >= 0 && on) ? (1u << pos) : 0u;
 		}
 		const uint32_t um = __ballot_sync(0xffffffffu, unstable);
@@ -467,7 +490,7 @@ __device__ __forceinline__ void mb_incr_start(const mb_fused_params& P, const mb
 	__syncwarp();
 }
 
-extern "C" __global__ void __launch_bounds__(128) mb_fused_fast(mb_fused_params P)
+extern "C" __global__ void __launch_bounds__(128, 4) mb_fused_fast(mb_fused_params P)
 {
 	extern __shared__ uint32_t mb_smem_u32[];
 	const int B = blockDim.x;
@@ -537,7 +560,8 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_fast(mb_fused_params 
 		}
 		if (starting)
 		{
-			curand_init(P.seed, P.first_traj + t, (unsigned long long)state_size, &rng);
+			// after the N initial-state uniforms, every step uses one whole Philox block (4 x 32 bits)
+			curand_init(P.seed, P.first_traj + t, (unsigned long long)((state_size + 3) & ~3), &rng);
 			h = mb_incr_entropy(v);
 			time = 0.f;
 			running = true;
@@ -545,6 +569,7 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_fast(mb_fused_params 
 
 		if (running)
 		{
+			const uint4 rb = curand4(&rng); // x: waiting time, (y, z): flip
 			float tn;
 			if (total == 0)
 				tn = max_time;
@@ -556,7 +581,11 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_fast(mb_fused_params 
 					tn = max_time - time_tick < tn ? max_time : tn;
 				}
 				else
-					tn = time + -logf(curand_uniform(&rng)) / ((float)total * inv_scale);
+				{
+					// uniform in (0, 1]: the top 24 bits plus one, times 2^-24
+					const float u = (float)((rb.x >> 8) + 1u) * 5.9604644775390625e-8f;
+					tn = time + -logf(u) / ((float)total * inv_scale);
+				}
 				tn = fminf(tn, max_time);
 			}
 			trans += (tn != 0.f) ? 1ull : 0ull;
@@ -585,9 +614,7 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_fast(mb_fused_params 
 			else
 			{
 				// draw the flip: r uniform in [0, total), then group -> word -> node
-				const unsigned hi = curand(&rng);
-				const unsigned lo = curand(&rng);
-				const unsigned long long r = __umul64hi(((unsigned long long)hi << 32) | lo, total);
+				const unsigned long long r = __umul64hi(((unsigned long long)rb.y << 32) | rb.z, total);
 				unsigned long long cum = 0;
 				int g = -1;
 #pragma unroll
@@ -614,40 +641,42 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_fast(mb_fused_params 
 				const uint32_t sw = v.S(word);
 				uint32_t um = v.U(word);
 				int j = 32 * word + 31 - __clz(um | 1u);
+				uint4 nj = make_uint4(0u, 0u, 0u, 0u);
 				while (um)
 				{
 					const int b = __ffs(um) - 1;
 					const int i = 32 * word + b;
-					const uint32_t q = ((sw >> b) & 1u) ? __ldg(mbg_inc_q_down + i) : __ldg(mbg_inc_q_up + i);
+					const uint4 nr = __ldg(mbg_inc_node + i);
+					const uint32_t q = ((sw >> b) & 1u) ? nr.y : nr.x;
+					j = i;
+					nj = nr;
 					if (r < cum + q)
-					{
-						j = i;
 						break;
-					}
 					cum += q;
 					um &= um - 1u;
 				}
 
 				// flip j and re-evaluate it and the nodes whose logic reads it
 				v.S(j >> 5) ^= 1u << (j & 31);
-				const int pj = __ldg(mbg_inc_ni_pos + j);
+				const int pj = (int)(nj.w >> 16) - 1;
 				if (pj >= 0)
 					idx ^= 1u << pj;
 				bool ni_changed = pj >= 0;
-				const int d0 = __ldg(mbg_inc_dep_ptr + j), d1 = __ldg(mbg_inc_dep_ptr + j + 1);
+				const int d0 = (int)nj.z, d1 = d0 + (int)(nj.w & 0xffffu);
 				for (int d = d0; d < d1; d++)
 				{
-					const int k = __ldg(mbg_inc_dep_idx + d);
+					const uint4 hdr = __ldg(mbg_inc_rec_hdr + d);
+					const uint4 in = __ldg(mbg_inc_rec_in + d);
+					const int k = (int)(hdr.x & 0xffffu);
 					const int wk = k >> 5;
 					const uint32_t bk = 1u << (k & 31);
 					const bool on = (v.S(wk) & bk) != 0;
 					const bool was_on = (k == j) ? !on : on;
 					const uint32_t uw = v.U(wk);
 					const bool was_unstable = (uw & bk) != 0;
-					const bool unstable = on != mb_incr_logic(v, k);
-					const uint32_t qo =
-						was_unstable ? (was_on ? __ldg(mbg_inc_q_down + k) : __ldg(mbg_inc_q_up + k)) : 0u;
-					const uint32_t qn = unstable ? (on ? __ldg(mbg_inc_q_down + k) : __ldg(mbg_inc_q_up + k)) : 0u;
+					const bool unstable = on != mb_incr_logic(v, d, hdr, in);
+					const uint32_t qo = was_unstable ? (was_on ? hdr.z : hdr.y) : 0u;
+					const uint32_t qn = unstable ? (on ? hdr.z : hdr.y) : 0u;
 					if (unstable != was_unstable)
 						v.U(wk) = uw ^ bk;
 					if (qn != qo)
@@ -658,7 +687,7 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_fast(mb_fused_params 
 						total += (unsigned long long)dq;
 					}
 					if (qn != qo || unstable != was_unstable)
-						ni_changed |= __ldg(mbg_inc_ni_pos + k) >= 0;
+						ni_changed |= ((hdr.x >> 21) & 31u) != 0u;
 				}
 				if (ni_changed)
 					h = mb_incr_entropy(v);

@@ -1021,9 +1021,11 @@ float entropy_fast(const compiled& c, const float* rates, const uint32_t* s)
 // Fast mode with integer rates (the engine's incremental kernel): rates in fixed point
 // q = round(rate * 2^shift), the flip drawn as the first node (in node order) whose cumulative
 // integer rate exceeds r = floor(u64 * total / 2^64), u64 from two raw 32-bit draws.
-void trajectory_integer(const compiled& c, sinks& s, curandStatePhilox4_32_10_t& rng, run_acc& acc,
+void trajectory_integer(const compiled& c, sinks& s, unsigned long long seed, unsigned long long traj, run_acc& acc,
 						unsigned long long& trans, std::vector<std::pair<int, float>>* trace)
 {
+	curandStatePhilox4_32_10_t rng;
+	curand_init(seed, traj, 0ull, &rng);
 	std::vector<uint32_t> st(c.W, 0u);
 	std::vector<float> rates(c.N);
 	std::vector<unsigned> q(c.N);
@@ -1031,10 +1033,14 @@ void trajectory_integer(const compiled& c, sinks& s, curandStatePhilox4_32_10_t&
 		if (curand_uniform(&rng) <= c.m.nodes[i].istate)
 			st[i / 32] |= 1u << (i % 32);
 	const float inv_scale = 1.0f / (float)(1u << c.shift);
+	// the stream continues at the next whole Philox block; each step consumes one block of four
+	// 32-bit outputs: x for the waiting time, (y, z) for the flip
+	curand_init(seed, traj, (unsigned long long)((c.N + 3) & ~3), &rng);
 	float time = 0.f;
 	bool fixed = false;
 	for (;;)
 	{
+		const uint4 rb = curand4(&rng);
 		unsigned long long total = 0;
 		for (int i = 0; i < c.N; i++)
 		{
@@ -1070,7 +1076,8 @@ void trajectory_integer(const compiled& c, sinks& s, curandStatePhilox4_32_10_t&
 			else
 			{
 				const float total_f = (float)total * inv_scale;
-				tn = time + -logf(curand_uniform(&rng)) / total_f;
+				const float u = (float)((rb.x >> 8) + 1u) * 5.9604644775390625e-8f; // (top 24 bits + 1) / 2^24
+				tn = time + -logf(u) / total_f;
 			}
 			tn = std::fmin(tn, c.max_time_sim);
 			h = entropy_fast(c, rates.data(), st.data());
@@ -1084,9 +1091,7 @@ void trajectory_integer(const compiled& c, sinks& s, curandStatePhilox4_32_10_t&
 				trace->emplace_back(-1, time);
 			break;
 		}
-		const unsigned hi = curand(&rng);
-		const unsigned lo = curand(&rng);
-		const unsigned long long r64 = ((unsigned long long)hi << 32) | lo;
+		const unsigned long long r64 = ((unsigned long long)rb.y << 32) | rb.z;
 		const unsigned long long r = (unsigned long long)(((unsigned __int128)r64 * total) >> 64);
 		unsigned long long cum = 0;
 		int j = -1;
@@ -1302,14 +1307,13 @@ oracle_result* oracle_run(const oracle_model* m, int mode, long long n, unsigned
 				curand_init(seed, first + (unsigned long long)t, 0ull, &rng);
 				trajectory(c, s, rng, true, traj_len, acc, trans, nullptr);
 			}
+			else if (c.integer_rates)
+				trajectory_integer(c, s, seed, first + (unsigned long long)t, acc, trans, nullptr);
 			else
 			{
 				curandStatePhilox4_32_10_t rng;
 				curand_init(seed, first + (unsigned long long)t, 0ull, &rng);
-				if (c.integer_rates)
-					trajectory_integer(c, s, rng, acc, trans, nullptr);
-				else
-					trajectory(c, s, rng, false, 0, acc, trans, nullptr);
+				trajectory(c, s, rng, false, 0, acc, trans, nullptr);
 			}
 		}
 		acc.flush(s);
@@ -1380,14 +1384,13 @@ int oracle_trace(const oracle_model* m, int mode, unsigned long long seed, unsig
 		curand_init(seed, traj, 0ull, &rng);
 		trajectory(c, s, rng, true, traj_len, acc, trans, &tr);
 	}
+	else if (c.integer_rates)
+		trajectory_integer(c, s, seed, traj, acc, trans, &tr);
 	else
 	{
 		curandStatePhilox4_32_10_t rng;
 		curand_init(seed, traj, 0ull, &rng);
-		if (c.integer_rates)
-			trajectory_integer(c, s, rng, acc, trans, &tr);
-		else
-			trajectory(c, s, rng, false, 0, acc, trans, &tr);
+		trajectory(c, s, rng, false, 0, acc, trans, &tr);
 	}
 	for (int i = 0; i < (int)tr.size() && i < cap; i++)
 	{
