@@ -152,6 +152,27 @@ mb_status mb_launch_fixed_states_stats(mb_stats st, void* stream, int n, int str
 /* stats::finalize (device -> host); the result is independent of the stats object. */
 mb_status mb_stats_finalize(mb_stats st, long long n_trajectories, mb_result* out);
 
+/* Fixed-point statistics for callers that cannot allocate device memory. No counterpart in the
+ * reference. Same result as mb_launch_fixed_states_stats followed by mb_stats_finalize (the
+ * distinct FIXED_POINT states among the n trajectories and how many trajectories ended in each),
+ * but the work table is a static 8 MiB device array inside this library instead of memory allocated
+ * per call, so the call itself allocates nothing: use it from code whose device memory belongs to
+ * someone else (a framework's caching allocator that owns the whole device, a process with a fixed
+ * memory budget) or where a cudaMalloc would stall the device.
+ *   inputs  (device): last_states[word * stride + i] and statuses[i] for i < n (SoA, as the kernels write them)
+ *   outputs (device): out_states[j * state_words + w] and out_counts[j] for j < *out_n, in no particular
+ *                     order; *out_n (host) is the number of distinct fixed points
+ * Limits: state_words <= 64 (2048 nodes); at most P/2 distinct fixed points, P the largest power of
+ * two with P * (20 + 4 * state_words) + 256 <= 8 MiB (131072 for 1 word, 16384 for 32 words); larger
+ * inputs return MB_ERR_LIMIT with a message. Runs on `stream` and synchronises it.
+ * The first call on a device looks up the array's device address with that device current; make that
+ * first call before any stream capture. Every call reuses the same array and clears it first, so
+ * calls that overlap on the GPU (other streams, other host threads) race: serialise them. Every GPU
+ * that loads the library holds the 8 MiB until the process exits. */
+mb_status mb_fixed_states_noalloc(void* stream, int n, int stride, int state_words, const uint32_t* last_states,
+                                  const uint8_t* statuses, uint32_t* out_states, unsigned* out_counts,
+                                  int out_cap, int* out_n);
+
 /* ------------------------------------------------------------------ whole runs (simulation_runner) */
 
 typedef struct mb_run_config_s

@@ -109,6 +109,11 @@ std::vector<std::string> names_of(const mb::model_t& m)
 
 } // namespace
 
+namespace mb {
+// lets entry points outside this file report through mb_last_error()
+void set_last_error(const std::string& message) { g_last_error = message; }
+} // namespace mb
+
 extern "C" {
 
 const char* mb_version(void) { return "maboss_b200 0.1 (sm_100a)"; }
