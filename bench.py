@@ -34,6 +34,12 @@ def bytes_per_transition(words: int, ni_words: int) -> int:
     return 4 * words + 8 + 4 * ni_words + 8
 
 
+EXTRA_WORKLOADS = {
+    "c5": "batched sweep: 256 rate-perturbed variants (lognormal sigma 0.3) of 8 networks of 20-144 nodes, "
+          "1e3-1e5 trajectories each, max_time 20-200, one persistent launch",
+    "c4grad": "score-function gradient of the 50-node network w.r.t. 40 rate parameters, 1e6 trajectories",
+}
+
 WORKLOADS = {
     # name: (generator, kwargs, description)
     "c1": ("c1", {}, "10-node random network, 1e5 trajectories, max_time 5, tick 0.2"),
@@ -155,6 +161,107 @@ def run_reference(args) -> None:
                                    f"{cores} OpenMP threads); the reference ships no CPU implementation"},
         "e2e": {"value": value, "unit": "transitions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    print(json.dumps(line), flush=True)
+
+
+def _timed_line(args, value, ms_per_step, config, extra) -> dict:
+    line = {"metric": "Gillespie transitions/s", "value": value, "unit": "transitions/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config}
+    line.update(extra)
+    return line
+
+
+def run_batched(args) -> None:
+    """C5: one persistent launch over 256 variants, against running the variants one by one."""
+    import maboss.gpu_b200 as mb
+    from maboss.gpu_b200 import synth
+
+    mb.build()
+    ctx = mb.Context(0)
+    bases, variants = synth.c5_sweep()
+    models = [mb.Model(*b) for b in bases]
+    batch = mb.Batch(ctx)
+    nets = [batch.add_model(m) for m in models]
+    for net, params, n in variants:
+        batch.add_variant(nets[net], n, params)
+    for _ in range(args.warmup):
+        batch.run(0)
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms, trans = [], 0
+    for step in range(args.steps):
+        ms.append(batch.run(step))
+        trans += sum(batch.result(v).transitions for v in range(len(variants)))
+    clk = clocks.stop()
+    value = trans / (sum(ms) / 1e3)
+    # the same variants one launch each (first 32 variants), and with one compilation per variant
+    # as the reference needs ($variables are baked into its generated code)
+    single_ms, single_trans = 0.0, 0
+    for net, params, n in variants[:32]:
+        b = mb.Batch(ctx)
+        k = b.add_model(models[net])
+        v = b.add_variant(k, n, params)
+        b.run(0)
+        single_ms += b.run(0)
+        single_trans += b.result(v).transitions
+    t0 = time.perf_counter()
+    comp_trans = 0
+    for net, params, n in variants[:4]:
+        m = mb.Model(*bases[net])
+        for k2, val in params.items():
+            m.set_variable(k2, val)
+        comp_trans += ctx.compile(m).run(mode="fast", sample_count=n).transitions
+    comp_s = time.perf_counter() - t0
+    line = _timed_line(args, value, sum(ms) / args.steps,
+                       {"workload": f"c5: {EXTRA_WORKLOADS['c5']}", "mode": "fast (batched kernel)",
+                        "variants": len(variants), "trajectories": sum(v[2] for v in variants),
+                        "transitions_per_step": trans // args.steps,
+                        "l2": "not flushed (each step re-uploads tables and clears accumulators before the launch)"},
+                       {"per_variant_launch": {"value": single_trans / (single_ms / 1e3), "variants": 32,
+                                               "note": "the first 32 variants, one batched launch each"},
+                        "per_variant_compile_and_run": {"value": comp_trans / comp_s, "variants": 4,
+                                                        "note": "NVRTC compile + fused fast run per variant, wall time"},
+                        "gpu_launches": args.steps, "clocks": clk})
+    print(json.dumps(line), flush=True)
+
+
+def run_gradient(args) -> None:
+    """C4: cost of the score-function gradient against the forward simulation."""
+    import maboss.gpu_b200 as mb
+    from maboss.gpu_b200 import synth
+
+    mb.build()
+    ctx = mb.Context(0)
+    model = mb.Model(*synth.c4())
+    names = sorted(model.variables)
+    theta = {k: model.variable(k) for k in names}
+    n = args.samples or 1_000_000
+    b = mb.Batch(ctx)
+    v = b.add_variant(b.add_model(model), n, theta)
+    dims = None
+    for _ in range(args.warmup):
+        b.run(0)
+    dims = b.result(v).dims
+    cot = np.zeros((dims.windows, dims.bins))
+    cot[:, [s for s in range(dims.bins) if s & 1]] = 1.0
+    for _ in range(args.warmup):
+        mb.gradient(ctx, model, theta, cot, n, 0)
+    fwd_ms, grad_ms, trans = [], [], 0
+    clocks = ClockSampler(0)
+    clocks.start()
+    for step in range(args.steps):
+        fwd_ms.append(b.run(step))
+        g, res = mb.gradient(ctx, model, theta, cot, n, step)
+        grad_ms.append(res.timing[0])
+        trans += res.transitions
+    clk = clocks.stop()
+    line = _timed_line(args, trans / (sum(grad_ms) / 1e3), sum(grad_ms) / args.steps,
+                       {"workload": f"c4grad: {EXTRA_WORKLOADS['c4grad']}", "parameters": len(names),
+                        "trajectories": n},
+                       {"forward_ms": float(np.mean(fwd_ms)), "gradient_ms": float(np.mean(grad_ms)),
+                        "gradient_over_forward": float(np.mean(grad_ms) / np.mean(fwd_ms)),
+                        "gpu_launches": args.steps, "clocks": clk})
     print(json.dumps(line), flush=True)
 
 
@@ -298,7 +405,7 @@ def main() -> None:
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=sorted(WORKLOADS), default="c3")
+    p.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(EXTRA_WORKLOADS), default="c3")
     p.add_argument("--mode", choices=["fast", "exact"], default="fast")
     p.add_argument("--samples", type=int, default=None, help="trajectories per GPU (default: the workload's)")
     p.add_argument("--cpu-sample", type=int, default=2000, help="trajectories of the CPU baseline sample")
@@ -306,6 +413,10 @@ def main() -> None:
     args = p.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "c5":
+        run_batched(args)
+    elif args.workload == "c4grad":
+        run_gradient(args)
     else:
         run_ours(args)
 

@@ -207,6 +207,35 @@ mb_status mb_runner_result(mb_runner r, void* stream, mb_result* out);
 mb_status mb_runner_kernel_launches(mb_runner r, unsigned* n);
 mb_status mb_runner_free(mb_runner r);
 
+/* ------------------------------------------------------------------ batched variants, gradients */
+/* Many parameter variants of one or more networks (of different sizes) in one persistent launch.
+ * No counterpart in the reference, which bakes $variables into the generated code and needs one
+ * process and one compilation per variant (src/parser/expressions.cpp:211-214). Networks must have
+ * rates of the form `rate_up = @logic ? U : 0; rate_down = @logic ? 0 : D` (U, D expressions of
+ * $variables), at most 2048 nodes, at most 12 logic inputs per node. Variants take exact float
+ * variable values (no 6-digit rounding) and run the fast-mode algorithm; a variant without
+ * overrides equals MB_MODE_FUSED_FAST of the same model bit for bit. Trajectory i of a variant uses
+ * random stream first_traj + i of `seed`: variants with equal first_traj share random numbers. */
+typedef struct mb_batch_s* mb_batch;
+mb_status mb_batch_create(mb_context c, mb_batch* out);
+mb_status mb_batch_free(mb_batch b);
+mb_status mb_batch_add_model(mb_batch b, mb_model m, int* net);
+mb_status mb_batch_add_variant(mb_batch b, int net, const char* const* names, const float* values, int n_values,
+                               long long n_traj, unsigned long long first_traj, int* variant);
+mb_status mb_batch_run(mb_batch b, unsigned long long seed, float* kernel_ms);
+/* a copy of variant `v`'s statistics after mb_batch_run */
+mb_status mb_batch_result(mb_batch b, int v, mb_result* out);
+
+/* Score-function (likelihood-ratio) gradient of L = sum_{w,s} cotangent[w * 2^k + s] * P_w(s) with
+ * respect to the $variables `params` (set to `values`), P_w(s) the window probabilities of
+ * n_traj trajectories (fast-mode algorithm, seed `seed`, streams 0..n_traj-1): grad[p] = dL/dparam_p,
+ * estimated on the same trajectories as the forward statistics written to *forward (optional).
+ * Continuous time: causal score sum_{jumps <= t} dlog a_j - int_0^t d a_0 weighted by the
+ * occupancy; discrete time: step score sum (dlog a_j - d a_0 / a_0). No counterpart in the reference. */
+mb_status mb_gradient(mb_context c, mb_model m, const char* const* params, const float* values, int n_params,
+                      long long n_traj, unsigned long long seed, const double* cotangent, double* grad,
+                      mb_result* forward);
+
 /* ------------------------------------------------------------------ results */
 mb_status mb_result_free(mb_result r);
 /* dims: windows, bins (2^k), non-internal count k, state words W, node count N */

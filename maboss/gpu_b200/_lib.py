@@ -73,6 +73,14 @@ def _declare(L: C.CDLL) -> None:
         "mb_runner_result": (i32, [vp, vp, P(vp)]),
         "mb_runner_kernel_launches": (i32, [vp, P(C.c_uint)]),
         "mb_runner_free": (i32, [vp]),
+        "mb_batch_create": (i32, [vp, P(vp)]),
+        "mb_batch_free": (i32, [vp]),
+        "mb_batch_add_model": (i32, [vp, vp, P(i32)]),
+        "mb_batch_add_variant": (i32, [vp, i32, P(C.c_char_p), P(f32), i32, i64, u64, P(i32)]),
+        "mb_batch_run": (i32, [vp, u64, P(f32)]),
+        "mb_batch_result": (i32, [vp, i32, P(vp)]),
+        "mb_gradient": (i32, [vp, vp, P(C.c_char_p), P(f32), i32, i64, u64, vp, vp, P(vp)]),
+        "mb_fixed_states_noalloc": (i32, [vp, i32, i32, i32, vp, vp, vp, vp, i32, P(i32)]),
         "mb_result_free": (i32, [vp]),
         "mb_result_dims": (i32, [vp, P(i32), P(i32), P(i32), P(i32), P(i32)]),
         "mb_result_transitions": (i32, [vp, P(u64)]),

@@ -9,6 +9,7 @@
 #include <memory>
 #include <string>
 
+#include "batch.h"
 #include "codegen.h"
 #include "model.h"
 #include "output.h"
@@ -37,6 +38,11 @@ struct mb_stats_s
 struct mb_runner_s
 {
 	std::unique_ptr<mb::runner> rn;
+};
+struct mb_batch_s
+{
+	std::unique_ptr<mb::batch_engine> b;
+	bool ran = false;
 };
 
 namespace {
@@ -562,6 +568,106 @@ mb_status mb_run(mb_module mod, const mb_run_config* cfg, mb_result* out)
 		auto r = std::make_unique<mb_result_s>();
 		r->res = mb::run(*mod->mod, c);
 		*out = r.release();
+	});
+}
+
+// ------------------------------------------------------------------ batches and gradients
+
+mb_status mb_batch_create(mb_context c, mb_batch* out)
+{
+	return guard([&] {
+		need(c && out, "null argument");
+		auto b = std::make_unique<mb_batch_s>();
+		b->b = std::make_unique<mb::batch_engine>(*c->ctx);
+		*out = b.release();
+	});
+}
+
+mb_status mb_batch_free(mb_batch b)
+{
+	delete b;
+	return MB_OK;
+}
+
+mb_status mb_batch_add_model(mb_batch b, mb_model m, int* net)
+{
+	return guard([&] {
+		need(b && m && net, "null argument");
+		*net = b->b->add_model(m->model);
+	});
+}
+
+namespace {
+std::map<std::string, float> overrides_of(const char* const* names, const float* values, int n)
+{
+	std::map<std::string, float> o;
+	for (int i = 0; i < n; i++)
+	{
+		need(names && names[i] && values, "null variable name or value");
+		o[names[i]] = values[i];
+	}
+	return o;
+}
+} // namespace
+
+mb_status mb_batch_add_variant(mb_batch b, int net, const char* const* names, const float* values, int n_values,
+							   long long n_traj, unsigned long long first_traj, int* variant)
+{
+	return guard([&] {
+		need(b && variant && n_values >= 0, "bad argument");
+		*variant = b->b->add_variant(net, overrides_of(names, values, n_values), n_traj, first_traj);
+	});
+}
+
+mb_status mb_batch_run(mb_batch b, unsigned long long seed, float* kernel_ms)
+{
+	return guard([&] {
+		need(b, "null batch");
+		b->b->run(seed);
+		b->ran = true;
+		if (kernel_ms)
+			*kernel_ms = b->b->kernel_ms;
+	});
+}
+
+mb_status mb_batch_result(mb_batch b, int v, mb_result* out)
+{
+	return guard([&] {
+		need(b && out && b->ran, "run the batch first");
+		need(v >= 0 && v < (int)b->b->vars_.size(), "bad variant index");
+		auto r = std::make_unique<mb_result_s>();
+		r->res = std::make_unique<mb::result>(*b->b->vars_[v]->res);
+		*out = r.release();
+	});
+}
+
+mb_status mb_gradient(mb_context c, mb_model m, const char* const* params, const float* values, int n_params,
+					  long long n_traj, unsigned long long seed, const double* cotangent, double* grad,
+					  mb_result* forward)
+{
+	return guard([&] {
+		need(c && m && cotangent && n_params >= 0 && (grad || n_params == 0), "bad argument");
+		mb::batch_engine be(*c->ctx);
+		const int net = be.add_model(m->model);
+		std::vector<std::string> names;
+		for (int i = 0; i < n_params; i++)
+		{
+			need(params && params[i], "null parameter name");
+			names.push_back(params[i]);
+		}
+		const int v = be.add_variant(net, overrides_of(params, values, n_params), n_traj, 0, names);
+		const mb::model_layout& L = be.nets[net]->L;
+		const size_t cells = (size_t)L.windows() << L.noninternal_nodes.size();
+		std::vector<std::vector<double>> cot(1, std::vector<double>(cotangent, cotangent + cells));
+		be.run(seed, &cot);
+		for (int i = 0; i < n_params; i++)
+			grad[i] = be.vars_[v]->grad[i];
+		if (forward)
+		{
+			auto r = std::make_unique<mb_result_s>();
+			r->res = std::move(be.vars_[v]->res);
+			*forward = r.release();
+		}
 	});
 }
 

@@ -229,13 +229,14 @@ void emit_array(std::ostream& os, const char* type, const char* name, const std:
 	os << "};" << std::endl;
 }
 
-// Tables of the incremental fast-mode kernel (kernels/engine.cuh, MBG_INCREMENTAL):
-//   mbg_inc_node[i]   = {q_up, q_down, first dependent record, dependents | (ni_pos + 1) << 16}
-//   dependent records (node i's own logic record first is not assumed; mbg_inc_self[i] points to it):
-//   mbg_inc_rec_hdr[r] = {k | m << 16 | (ni_pos(k) + 1) << 21, q_up(k), q_down(k), truth table or offset}
-//   mbg_inc_rec_in[r]  = inputs 0..7 of k's logic as 16-bit node indices, mbg_inc_rec_in2[r] = inputs 8..15
+// Tables of the incremental fast-mode kernel (kernels/engine.cuh, MBG_INCREMENTAL), built by
+// build_incremental_tables:
+//   node[i]    = {q_up, q_down, first dependent record, dependents | (ni_pos + 1) << 16}
+//   hdr[r]     = {k | m << 16 | (ni_pos(k) + 1) << 21, q_up(k), q_down(k), truth table or offset}
+//   in1[r]     = inputs 0..7 of k's logic as 16-bit node indices, in2[r] = inputs 8..15
+//   self[i]    = the record of node i's own logic
 // The truth table of k is inline when it has at most 5 inputs (32 patterns), else an offset into
-// mbg_inc_tt. Records keep everything one dependent re-evaluation needs in two 16-byte loads.
+// tt. Records keep everything one dependent re-evaluation needs in two 16-byte loads.
 void emit_incremental_tables(std::ostream& ss, const model_layout& L)
 {
 	ss << std::endl << "// ---- incremental engine tables" << std::endl;
@@ -244,54 +245,22 @@ void emit_incremental_tables(std::ostream& ss, const model_layout& L)
 		ss << "constexpr int mbg_inc_rate_shift = 0;" << std::endl;
 		return;
 	}
-	const int N = L.state_size;
-	std::vector<int> ni_pos(N, -1);
-	for (size_t k = 0; k < L.noninternal_nodes.size(); k++)
-		ni_pos[L.noninternal_nodes[k]] = (int)k;
-
-	std::vector<std::string> node, hdr, in1, in2;
-	std::vector<unsigned> tt_big;
-	std::vector<int> self(N, -1);
-	auto u4 = [](unsigned a, unsigned b, unsigned c, unsigned d) {
-		return "{" + std::to_string(a) + "u, " + std::to_string(b) + "u, " + std::to_string(c) + "u, " +
-			   std::to_string(d) + "u}";
+	const incremental_tables t = build_incremental_tables(L, L.up, L.down);
+	auto u4 = [](const std::vector<unsigned>& v) {
+		std::vector<std::string> out;
+		for (size_t i = 0; i + 3 < v.size(); i += 4)
+			out.push_back("{" + std::to_string(v[i]) + "u, " + std::to_string(v[i + 1]) + "u, " +
+						  std::to_string(v[i + 2]) + "u, " + std::to_string(v[i + 3]) + "u}");
+		return out;
 	};
-	for (int j = 0; j < N; j++)
-	{
-		const int d0 = L.dep_ptr[j], d1 = L.dep_ptr[j + 1];
-		node.push_back(u4(L.q_up[j], L.q_down[j], (unsigned)d0, (unsigned)(d1 - d0) | ((unsigned)(ni_pos[j] + 1) << 16)));
-		for (int d = d0; d < d1; d++)
-		{
-			const int k = L.dep_idx[d];
-			if (k == j)
-				self[j] = d;
-			const int a0 = L.in_ptr[k], m = L.in_ptr[k + 1] - a0;
-			unsigned tt;
-			const int t0 = L.tt_ptr[k], nt = L.tt_ptr[k + 1] - t0;
-			if (m <= 5)
-				tt = L.tt_words[t0];
-			else
-			{
-				tt = (unsigned)tt_big.size();
-				tt_big.insert(tt_big.end(), L.tt_words.begin() + t0, L.tt_words.begin() + t0 + nt);
-			}
-			hdr.push_back(u4((unsigned)k | ((unsigned)m << 16) | ((unsigned)(ni_pos[k] + 1) << 21), L.q_up[k],
-							 L.q_down[k], tt));
-			unsigned in[16] = { 0 };
-			for (int t = 0; t < m; t++)
-				in[t] = (unsigned)L.in_idx[a0 + t];
-			in1.push_back(u4(in[0] | in[1] << 16, in[2] | in[3] << 16, in[4] | in[5] << 16, in[6] | in[7] << 16));
-			in2.push_back(u4(in[8] | in[9] << 16, in[10] | in[11] << 16, in[12] | in[13] << 16, in[14] | in[15] << 16));
-		}
-	}
 	ss << "#define MBG_INCREMENTAL 1" << std::endl;
-	ss << "constexpr int mbg_inc_rate_shift = " << L.rate_shift << ";" << std::endl;
-	emit_array(ss, "uint4", "mbg_inc_node", node);
-	emit_array(ss, "uint4", "mbg_inc_rec_hdr", hdr);
-	emit_array(ss, "uint4", "mbg_inc_rec_in", in1);
-	emit_array(ss, "uint4", "mbg_inc_rec_in2", in2);
-	emit_array(ss, "unsigned", "mbg_inc_tt", tt_big);
-	emit_array(ss, "int", "mbg_inc_self", self);
+	ss << "constexpr int mbg_inc_rate_shift = " << t.rate_shift << ";" << std::endl;
+	emit_array(ss, "uint4", "mbg_inc_node", u4(t.node));
+	emit_array(ss, "uint4", "mbg_inc_rec_hdr", u4(t.hdr));
+	emit_array(ss, "uint4", "mbg_inc_rec_in", u4(t.in1));
+	emit_array(ss, "uint4", "mbg_inc_rec_in2", u4(t.in2));
+	emit_array(ss, "unsigned", "mbg_inc_tt", t.tt);
+	emit_array(ss, "int", "mbg_inc_self", t.self);
 	std::vector<std::string> f_up, f_down, f_ul, f_dl;
 	for (int i : L.noninternal_nodes)
 	{
@@ -306,6 +275,65 @@ void emit_incremental_tables(std::ostream& ss, const model_layout& L)
 	emit_array(ss, "float", "mbg_inc_ni_ul", f_ul);
 	emit_array(ss, "float", "mbg_inc_ni_dl", f_dl);
 	emit_array(ss, "int", "mbg_inc_ni_node", L.noninternal_nodes);
+}
+
+// forward-mode derivative of the float evaluation (expressions.cpp evaluate) w.r.t. one variable
+struct dual
+{
+	float v = 0, d = 0;
+};
+
+dual eval_dual(const model_t& m, const expr& e, const std::map<std::string, float>& vars, const std::string& p)
+{
+	using K = expr::kind_t;
+	switch (e.kind)
+	{
+		case K::literal: return { e.value, 0.f };
+		case K::variable:
+		{
+			auto it = vars.find(e.name);
+			if (it == vars.end())
+				throw model_error("unknown variable " + e.name);
+			return { it->second, e.name == p ? 1.f : 0.f };
+		}
+		case K::paren: return eval_dual(m, *e.a, vars, p);
+		case K::ternary:
+		{
+			const dual c = eval_dual(m, *e.a, vars, p);
+			return c.v != 0.f ? eval_dual(m, *e.b, vars, p) : eval_dual(m, *e.c, vars, p);
+		}
+		case K::unary:
+		{
+			const dual a = eval_dual(m, *e.a, vars, p);
+			if (e.op == op_t::MINUS)
+				return { -a.v, -a.d };
+			if (e.op == op_t::NOT)
+				return { (float)!a.v, 0.f };
+			return a;
+		}
+		case K::binary:
+		{
+			const dual a = eval_dual(m, *e.a, vars, p), b = eval_dual(m, *e.b, vars, p);
+			switch (e.op)
+			{
+				case op_t::PLUS: return { a.v + b.v, a.d + b.d };
+				case op_t::MINUS: return { a.v - b.v, a.d - b.d };
+				case op_t::STAR: return { a.v * b.v, a.d * b.v + a.v * b.d };
+				case op_t::SLASH: return { a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v) };
+				case op_t::AND: return { (float)(a.v && b.v), 0.f };
+				case op_t::OR: return { (float)(a.v || b.v), 0.f };
+				case op_t::XOR: return { (float)((a.v != 0.f) != (b.v != 0.f)), 0.f };
+				case op_t::EQ: return { (float)(a.v == b.v), 0.f };
+				case op_t::NE: return { (float)(a.v != b.v), 0.f };
+				case op_t::LE: return { (float)(a.v <= b.v), 0.f };
+				case op_t::LT: return { (float)(a.v < b.v), 0.f };
+				case op_t::GE: return { (float)(a.v >= b.v), 0.f };
+				case op_t::GT: return { (float)(a.v > b.v), 0.f };
+				default: throw model_error("Unknown binary operator");
+			}
+		}
+		default: throw model_error("node or alias in a rate constant");
+	}
 }
 
 } // namespace
@@ -472,6 +500,122 @@ model_layout analyze_model(const model_t& m)
 		}
 	}
 	return L;
+}
+
+rate_set fast_rates(const model_t& m, const std::map<std::string, float>& variables,
+					const std::vector<std::string>& params)
+{
+	const int N = (int)m.nodes.size();
+	rate_set r;
+	r.up.assign(N, 0.f);
+	r.down.assign(N, 0.f);
+	r.grad_ptr.assign(1, 0);
+	model_t mm = m;
+	mm.variables = variables;
+	for (int i = 0; i < N; i++)
+	{
+		const node_t& node = m.nodes[i];
+		float u = 0, d = 0;
+		if (!(is_logic_ternary(mm, node.find_attr("rate_up"), true, u) &&
+			  is_logic_ternary(mm, node.find_attr("rate_down"), false, d) && node.find_attr("logic")))
+			throw model_error("node " + node.name + " is not of the form rate_up = @logic ? U : 0; rate_down = @logic ? 0 : D");
+		const expr& ue = *node.find_attr("rate_up")->b;	  // middle of rate_up
+		const expr& de = *node.find_attr("rate_down")->c; // right of rate_down
+		for (int dir = 0; dir < 2; dir++)
+		{
+			const expr& e = dir ? de : ue;
+			const dual v = eval_dual(mm, e, variables, "");
+			(dir ? r.down[i] : r.up[i]) = v.v;
+			for (size_t p = 0; p < params.size(); p++)
+			{
+				const dual g = eval_dual(mm, e, variables, params[p]);
+				if (g.d != 0.f)
+				{
+					r.grad_p.push_back((int)p);
+					r.grad_d.push_back(g.d);
+				}
+			}
+			r.grad_ptr.push_back((int)r.grad_p.size());
+		}
+	}
+	return r;
+}
+
+incremental_tables build_incremental_tables(const model_layout& L, const std::vector<float>& up,
+											const std::vector<float>& down)
+{
+	incremental_tables t;
+	const int N = L.state_size;
+	// fixed-point scale: every word's largest possible rate sum stays below 2^31
+	double worst = 0;
+	for (int w = 0; w < L.state_words; w++)
+	{
+		double sw = 0;
+		for (int i = 32 * w; i < std::min(N, 32 * w + 32); i++)
+			sw += std::max((double)up[i], (double)down[i]);
+		worst = std::max(worst, sw);
+	}
+	int shift = 30;
+	while (shift > 0 && worst * std::ldexp(1.0, shift) >= 2147483648.0)
+		shift--;
+	t.rate_shift = shift;
+	t.ok = true;
+	std::vector<unsigned> qu(N), qd(N);
+	for (int i = 0; i < N; i++)
+	{
+		for (int which = 0; which < 2; which++)
+		{
+			const double r = which ? down[i] : up[i];
+			if (!(r >= 0.0))
+				t.ok = false;
+			const double q = std::nearbyint(std::max(0.0, r) * std::ldexp(1.0, shift));
+			if (r > 0 && q < 1024.0)
+				t.ok = false;
+			(which ? qd[i] : qu[i]) = (unsigned)q;
+		}
+		t.q.push_back(qu[i]);
+		t.q.push_back(qd[i]);
+	}
+	std::vector<int> ni_pos(N, -1);
+	for (size_t k = 0; k < L.noninternal_nodes.size(); k++)
+		ni_pos[L.noninternal_nodes[k]] = (int)k;
+	t.self.assign(N, -1);
+	auto push4 = [](std::vector<unsigned>& v, unsigned a, unsigned b, unsigned c, unsigned d) {
+		v.push_back(a);
+		v.push_back(b);
+		v.push_back(c);
+		v.push_back(d);
+	};
+	for (int j = 0; j < N; j++)
+	{
+		const int d0 = L.dep_ptr[j], d1 = L.dep_ptr[j + 1];
+		push4(t.node, qu[j], qd[j], (unsigned)d0, (unsigned)(d1 - d0) | ((unsigned)(ni_pos[j] + 1) << 16));
+		for (int d = d0; d < d1; d++)
+		{
+			const int k = L.dep_idx[d];
+			if (k == j)
+				t.self[j] = d;
+			const int a0 = L.in_ptr[k], m = L.in_ptr[k + 1] - a0;
+			const int t0 = L.tt_ptr[k], nt = L.tt_ptr[k + 1] - t0;
+			unsigned ttw;
+			if (m <= 5)
+				ttw = L.tt_words[t0];
+			else
+			{
+				ttw = (unsigned)t.tt.size();
+				t.tt.insert(t.tt.end(), L.tt_words.begin() + t0, L.tt_words.begin() + t0 + nt);
+			}
+			push4(t.hdr, (unsigned)k | ((unsigned)m << 16) | ((unsigned)(ni_pos[k] + 1) << 21), qu[k], qd[k], ttw);
+			unsigned in[16] = { 0 };
+			for (int x = 0; x < m; x++)
+				in[x] = (unsigned)L.in_idx[a0 + x];
+			push4(t.in1, in[0] | in[1] << 16, in[2] | in[3] << 16, in[4] | in[5] << 16, in[6] | in[7] << 16);
+			push4(t.in2, in[8] | in[9] << 16, in[10] | in[11] << 16, in[12] | in[13] << 16, in[14] | in[15] << 16);
+		}
+	}
+	if (t.tt.empty())
+		t.tt.push_back(0);
+	return t;
 }
 
 std::string generate_code(const model_t& m)

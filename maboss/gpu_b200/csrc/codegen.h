@@ -53,6 +53,32 @@ struct model_layout
 // Analyse a parsed model (throws model_error on semantic errors such as unknown nodes).
 model_layout analyze_model(const model_t& m);
 
+// Rates of the fast-path nodes for given variable values (exact floats, not the 6-digit literals of
+// the generated code), with their derivatives with respect to the listed variables: entry 2i is
+// node i's up rate, 2i+1 its down rate; grad_ptr/grad_p/grad_d are a CSR of (parameter, d rate / d
+// parameter) pairs. Throws if a node is not of the fast-path form.
+struct rate_set
+{
+	std::vector<float> up, down;
+	std::vector<int> grad_ptr, grad_p;
+	std::vector<float> grad_d;
+};
+rate_set fast_rates(const model_t& m, const std::map<std::string, float>& variables,
+					const std::vector<std::string>& params);
+
+// Tables of the incremental kernels for given rates (see codegen.cpp: emit_incremental_tables).
+struct incremental_tables
+{
+	int rate_shift = 0;
+	bool ok = false; // rates representable (every positive rate >= 2^10 units)
+	std::vector<unsigned> node, hdr, in1, in2; // uint4 records, 4 words each
+	std::vector<unsigned> tt;
+	std::vector<int> self;
+	std::vector<unsigned> q; // (q_up, q_down) per node
+};
+incremental_tables build_incremental_tables(const model_layout& L, const std::vector<float>& up,
+											const std::vector<float>& down);
+
 // The generated CUDA source for a model (model-specific part only).
 std::string generate_code(const model_t& m);
 

@@ -1,0 +1,545 @@
+// Batched incremental kernel: one persistent launch over many (network, parameter variant,
+// trajectory) work items, with optional score-function (likelihood-ratio) gradients.
+//
+// It runs the same algorithm as the incremental fast kernel of kernels/engine.cuh (integer rates
+// 2^-shift, one Philox block per step, flips drawn with a 64-bit uniform walking groups -> words ->
+// unstable bits, warp-cooperative trajectory start), but nothing is compiled into it: network
+// sizes, dependency records, truth tables and rates are runtime data. Networks of different sizes
+// and any number of rate variants therefore share one launch, and rates change without
+// recompilation. With equal rates and seeds it reproduces the NVRTC-compiled fast kernel.
+//
+// Gradients. For a path with jumps of rates a_j and total rate a_0, the score up to time t is
+//   S(t) = sum_{jumps <= t} d log a_j / d theta  -  int_0^t d a_0 / d theta ds,
+// and d E[int_window 1{x(t) = s} dt] / d theta = E[int_window 1{x(t) = s} S(t) dt] (the path after t
+// does not change the occupancy at t). Given a cotangent c[w][s] (the gradient of a loss with
+// respect to the window probabilities), each trajectory adds to grad[p]
+//   sum over recorded slices [u, v] of state s in window w:  c[w][s] * int_u^v S_p(t) dt,
+// i.e. the vector-Jacobian product. S_p is kept lazily: S_p(t) = S_p - D_p (t - tp_p), where
+// D_p = d a_0 / d theta_p of the current state and tp_p the time D_p last changed; jumps add
+// (d rate / d theta_p) / rate. Discrete time uses the step score sum (d log a_j - d a_0 / a_0).
+
+struct mb_net
+{
+	int N, W, k, discrete;
+	float max_time, tick; // simulation constants (as the generated code of the network has them)
+	const uint4* node;	  // {-, -, first record, dependents | (ni_pos + 1) << 16}
+	const uint4* hdr;	  // {k | m << 16 | (ni_pos + 1) << 21, -, -, truth table or offset}
+	const uint4* in1;
+	const uint4* in2;
+	const unsigned* tt;
+	const int* self;
+	const int* ni_node; // [k]
+};
+
+struct mb_variant
+{
+	int net;
+	int rate_shift;
+	const uint2* q;		  // [N] (q_up, q_down) integer rates
+	const float* rate;	  // [2N] (up, down) float rates
+	const float* istate;  // [N]
+	unsigned long long begin; // first global work index of this variant
+	unsigned long long first_traj; // random stream of the variant's trajectory 0
+	unsigned n_traj;
+	mb_stats_params st;	  // this variant's accumulators (entropy sums in global memory)
+	unsigned long long* transitions;
+	// gradient (cot == nullptr: off)
+	const double* cot;	  // [T * S]
+	const int* g_ptr;	  // [2N + 1] CSR of (parameter, d rate / d parameter) per node direction
+	const int* g_p;
+	const float* g_d;
+	double* grad;		  // [P]
+};
+
+struct mb_batch_params
+{
+	const mb_net* nets;
+	const mb_variant* vars;
+	int n_vars;
+	int max_W;			  // shared memory rows per lane
+	int P;				  // gradient parameters (rows of gradient scratch), 0 = none
+	unsigned long long total;
+	unsigned long long seed;
+	unsigned long long* next;
+	unsigned* errors;
+};
+
+constexpr int MBB_GROUPS = 16; // register group sums; words per group = ceil(W / 16)
+
+struct mbb_lane
+{
+	uint32_t* st;
+	uint32_t* un;
+	uint32_t* ws;
+	float* gS;	// [P] score at gT
+	float* gD;	// [P] d a0 / d theta
+	float* gT;	// [P] time of the last change of gD
+	float* gG;	// [P] accumulated vector-Jacobian product of the trajectory
+	int stride;
+	__device__ __forceinline__ uint32_t& S(int w) const { return st[w * stride]; }
+	__device__ __forceinline__ uint32_t& U(int w) const { return un[w * stride]; }
+	__device__ __forceinline__ uint32_t& Q(int w) const { return ws[w * stride]; }
+	__device__ __forceinline__ float& GS(int p) const { return gS[p * stride]; }
+	__device__ __forceinline__ float& GD(int p) const { return gD[p * stride]; }
+	__device__ __forceinline__ float& GT(int p) const { return gT[p * stride]; }
+	__device__ __forceinline__ float& GG(int p) const { return gG[p * stride]; }
+};
+
+__device__ __forceinline__ bool mbb_logic(const mb_net& net, const mbb_lane& v, int r, const uint4& hdr,
+										  const uint4& in)
+{
+	const int m = (hdr.x >> 16) & 31;
+	const unsigned ins[4] = { in.x, in.y, in.z, in.w };
+	unsigned p = 0;
+#pragma unroll
+	for (int t = 0; t < 8; t++)
+	{
+		if (t < m)
+		{
+			const unsigned node = (ins[t >> 1] >> ((t & 1) * 16)) & 0xffffu;
+			p |= ((v.S(node >> 5) >> (node & 31)) & 1u) << t;
+		}
+	}
+	if (m > 8)
+	{
+		const uint4 in2 = __ldg(net.in2 + r);
+		const unsigned ins2[4] = { in2.x, in2.y, in2.z, in2.w };
+#pragma unroll
+		for (int t = 8; t < 16; t++)
+		{
+			if (t < m)
+			{
+				const unsigned node = (ins2[(t - 8) >> 1] >> ((t & 1) * 16)) & 0xffffu;
+				p |= ((v.S(node >> 5) >> (node & 31)) & 1u) << t;
+			}
+		}
+	}
+	const unsigned ttw = m <= 5 ? hdr.w : __ldg(net.tt + hdr.w + (p >> 5));
+	return (ttw >> (p & 31)) & 1u;
+}
+
+__device__ __forceinline__ void mbb_group_add(unsigned long long (&gs)[MBB_GROUPS], int g, long long d)
+{
+#pragma unroll
+	for (int i = 0; i < MBB_GROUPS; i++)
+		gs[i] += (i == g) ? (unsigned long long)d : 0ull;
+}
+
+__device__ __forceinline__ float mbb_entropy(const mb_net& net, const mb_variant& var, const mbb_lane& v)
+{
+	float t = 0.f, tl = 0.f;
+	for (int k = 0; k < net.k; k++)
+	{
+		const int i = __ldg(net.ni_node + k);
+		const uint32_t bit = 1u << (i & 31);
+		if (v.U(i >> 5) & bit)
+		{
+			const bool up = (v.S(i >> 5) & bit) != 0;
+			const float r = __ldg(var.rate + 2 * i + (up ? 1 : 0));
+			t += r;
+			tl += r > 0.f ? r * log2f(r) : 0.f;
+		}
+	}
+	if (!(t > 0.f))
+		return 0.f;
+	const float h = log2f(t) - tl / t;
+	return h > 0.f ? h : 0.f;
+}
+
+// d a_0 changes by `sign` times node k's rate derivatives in direction `dir` at time `now`
+__device__ __forceinline__ void mbb_grad_active(const mb_variant& var, const mbb_lane& v, int k, int dir, float sign,
+												float now, bool discrete)
+{
+	const int a = __ldg(var.g_ptr + 2 * k + dir), b = __ldg(var.g_ptr + 2 * k + dir + 1);
+	for (int e = a; e < b; e++)
+	{
+		const int p = __ldg(var.g_p + e);
+		if (!discrete)
+		{
+			v.GS(p) -= v.GD(p) * (now - v.GT(p));
+			v.GT(p) = now;
+		}
+		v.GD(p) += sign * __ldg(var.g_d + e);
+	}
+}
+
+// the slice [u, w1] of window `w` in state `idx` contributes c * int S dt (continuous) or c * S (discrete)
+__device__ __forceinline__ void mbb_grad_slice(const mb_variant& var, const mbb_lane& v, int P, int w, unsigned idx,
+											   float u, float w1, bool discrete)
+{
+	const double c = var.cot[(size_t)w * var.st.n_bins + idx];
+	if (c == 0.0)
+		return;
+	const float cf = (float)c;
+	if (discrete)
+	{
+		for (int p = 0; p < P; p++)
+			v.GG(p) += cf * v.GS(p);
+		return;
+	}
+	const float len = w1 - u, mid = 0.5f * (u + w1);
+	for (int p = 0; p < P; p++)
+		v.GG(p) += cf * len * (v.GS(p) - v.GD(p) * (mid - v.GT(p)));
+}
+
+template <bool GRAD>
+__device__ __forceinline__ void mbb_record(const mb_variant& var, const mbb_lane& v, int P, mb_win_acc& acc,
+										   unsigned idx, float t0, float t1, float h, bool discrete, float tick)
+{
+	if (t1 == 0.f)
+		return;
+	if (discrete)
+	{
+		mb_record_disc(var.st, var.st.win_h, idx, t0, h);
+		if (GRAD)
+		{
+			const int w = (int)lroundf(t0 / tick);
+			if (w >= 0 && w < var.st.n_windows)
+				mbb_grad_slice(var, v, P, w, idx, t0, t1, true);
+		}
+		return;
+	}
+	mb_record_cont(acc, var.st, var.st.win_h, idx, t0, t1, h);
+	if (GRAD)
+	{
+		// the same window slices as mb_record_cont
+		float sb = t0;
+		int w = (int)floorf(sb / tick);
+		for (int guard = 0; t1 > sb && guard <= var.st.n_windows + 2; guard++)
+		{
+			const float we = (float)(w + 1) * tick;
+			const float se = fminf(t1, we);
+			if (w >= 0 && w < var.st.n_windows)
+				mbb_grad_slice(var, v, P, w, idx, sb, se, false);
+			w++;
+			sb = se;
+		}
+	}
+}
+
+template <bool GRAD>
+__device__ void mbb_body(const mb_batch_params& B)
+{
+	extern __shared__ uint32_t mbb_smem[];
+	const int bs = blockDim.x, lane = threadIdx.x & 31;
+	const int MW = B.max_W, P = GRAD ? B.P : 0;
+	mbb_lane v;
+	v.stride = bs;
+	v.st = mbb_smem + threadIdx.x;
+	v.un = mbb_smem + (size_t)MW * bs + threadIdx.x;
+	v.ws = mbb_smem + (size_t)2 * MW * bs + threadIdx.x;
+	float* gbase = reinterpret_cast<float*>(mbb_smem + (size_t)3 * MW * bs);
+	v.gS = gbase + threadIdx.x;
+	v.gD = gbase + (size_t)P * bs + threadIdx.x;
+	v.gT = gbase + (size_t)2 * P * bs + threadIdx.x;
+	v.gG = gbase + (size_t)3 * P * bs + threadIdx.x;
+
+	mb_win_acc acc;
+	mb_acc_init(acc);
+	int acc_var = -1; // variant whose accumulators `acc` refers to
+
+	bool working = true, running = false;
+	int vi = 0; // current variant of this lane
+	unsigned long long gs[MBB_GROUPS];
+	unsigned long long total = 0;
+	uint32_t idx = 0;
+	float time = 0.f, h = 0.f;
+	unsigned long long trans = 0;
+	curandStatePhilox4_32_10_t rng;
+
+	while (__any_sync(0xffffffffu, working || running))
+	{
+		unsigned long long t = 0;
+		int tv = 0;
+		bool starting = false;
+		if (working && !running)
+		{
+			t = atomicAdd(B.next, 1ull);
+			if (t < B.total)
+			{
+				// variant of work item t (variants are laid out back to back)
+				int lo = 0, hi = B.n_vars - 1;
+				while (lo < hi)
+				{
+					const int mid = (lo + hi + 1) >> 1;
+					if (B.vars[mid].begin <= t)
+						lo = mid;
+					else
+						hi = mid - 1;
+				}
+				tv = lo;
+				starting = true;
+			}
+			else
+				working = false;
+		}
+		unsigned pending = __ballot_sync(0xffffffffu, starting);
+		while (pending)
+		{
+			const int src = __ffs(pending) - 1;
+			pending &= pending - 1u;
+			const unsigned long long ts = __shfl_sync(0xffffffffu, t, src);
+			const int vs = __shfl_sync(0xffffffffu, tv, src);
+			const mb_variant& var = B.vars[vs];
+			const mb_net& net = B.nets[var.net];
+			const unsigned long long stream = var.first_traj + (ts - var.begin);
+			mbb_lane c = v;
+			const int off = (int)threadIdx.x - ((threadIdx.x & ~31) + src);
+			c.st = v.st - off;
+			c.un = v.un - off;
+			c.ws = v.ws - off;
+			for (int w = 0; w < net.W; w++)
+			{
+				const int i = 32 * w + lane;
+				bool on = false;
+				if (i < net.N)
+				{
+					curandStatePhilox4_32_10_t r;
+					curand_init(B.seed, stream, (unsigned long long)i, &r);
+					on = curand_uniform(&r) <= __ldg(var.istate + i);
+				}
+				const uint32_t word = __ballot_sync(0xffffffffu, on);
+				if (lane == 0)
+					c.S(w) = word;
+			}
+			__syncwarp();
+			unsigned long long gsx[MBB_GROUPS];
+#pragma unroll
+			for (int g = 0; g < MBB_GROUPS; g++)
+				gsx[g] = 0;
+			unsigned long long tot = 0;
+			uint32_t ix = 0;
+			const int wpg = (net.W + MBB_GROUPS - 1) / MBB_GROUPS;
+			for (int w = 0; w < net.W; w++)
+			{
+				const int i = 32 * w + lane;
+				const bool on = (c.S(w) >> lane) & 1u;
+				bool unstable = false;
+				uint32_t q = 0, nibit = 0;
+				if (i < net.N)
+				{
+					const int r = __ldg(net.self + i);
+					const uint4 hdr = __ldg(net.hdr + r);
+					unstable = on != mbb_logic(net, c, r, hdr, __ldg(net.in1 + r));
+					const uint2 qq = __ldg(var.q + i);
+					q = unstable ? (on ? qq.y : qq.x) : 0u;
+					const int pos = (int)((hdr.x >> 21) & 31u) - 1;
+					nibit = (pos >= 0 && on) ? (1u << pos) : 0u;
+				}
+				const uint32_t um = __ballot_sync(0xffffffffu, unstable);
+				const uint32_t qw = __reduce_add_sync(0xffffffffu, q);
+				ix |= __reduce_or_sync(0xffffffffu, nibit);
+				if (lane == 0)
+				{
+					c.U(w) = um;
+					c.Q(w) = qw;
+				}
+				mbb_group_add(gsx, w / wpg, qw);
+				tot += qw;
+			}
+			__syncwarp();
+			if (lane == src)
+			{
+#pragma unroll
+				for (int g = 0; g < MBB_GROUPS; g++)
+					gs[g] = gsx[g];
+				total = tot;
+				idx = ix;
+			}
+		}
+		if (starting)
+		{
+			vi = tv;
+			const mb_variant& var = B.vars[vi];
+			const mb_net& net = B.nets[var.net];
+			const unsigned long long stream = var.first_traj + (t - var.begin);
+			curand_init(B.seed, stream, (unsigned long long)((net.N + 3) & ~3), &rng);
+			h = mbb_entropy(net, var, v);
+			time = 0.f;
+			running = true;
+			if (acc_var != vi)
+			{
+				if (acc_var >= 0)
+					mb_acc_flush(acc, B.vars[acc_var].st, B.vars[acc_var].st.win_h);
+				acc_var = vi;
+			}
+			if (GRAD)
+			{
+				for (int p = 0; p < P; p++)
+				{
+					v.GS(p) = 0.f;
+					v.GD(p) = 0.f;
+					v.GT(p) = 0.f;
+					v.GG(p) = 0.f;
+				}
+				// d a0 / d theta of the initial state: every unstable node's active-direction derivatives
+				for (int w = 0; w < net.W; w++)
+				{
+					uint32_t um = v.U(w);
+					const uint32_t sw = v.S(w);
+					while (um)
+					{
+						const int b = __ffs(um) - 1;
+						um &= um - 1u;
+						mbb_grad_active(var, v, 32 * w + b, (sw >> b) & 1u, 1.f, 0.f, net.discrete);
+					}
+				}
+			}
+		}
+
+		if (running)
+		{
+			const mb_variant& var = B.vars[vi];
+			const mb_net& net = B.nets[var.net];
+			const bool discrete = net.discrete != 0;
+			const float max_time = net.max_time, tick = net.tick;
+			const uint4 rb = curand4(&rng);
+			float tn;
+			if (total == 0)
+				tn = max_time;
+			else
+			{
+				if (discrete)
+				{
+					tn = time + tick;
+					tn = max_time - tick < tn ? max_time : tn;
+				}
+				else
+				{
+					const float u = (float)((rb.x >> 8) + 1u) * 5.9604644775390625e-8f;
+					tn = time + -logf(u) / ((float)total * (1.0f / (float)(1u << var.rate_shift)));
+				}
+				tn = fminf(tn, max_time);
+			}
+			trans += (tn != 0.f) ? 1ull : 0ull;
+			mbb_record<GRAD>(var, v, P, acc, idx, time, tn, total == 0 ? 0.f : h, discrete, var.st.win_tick);
+			time = tn;
+			if (time >= max_time)
+			{
+				running = false;
+				atomicAdd(var.st.final_cnt + idx, 1u);
+				if (total == 0)
+				{
+					unsigned st[64];
+					const int W = net.W < 64 ? net.W : 64;
+					for (int w = 0; w < W; w++)
+						st[w] = v.S(w);
+					mb_fixed_insert_rt(var.st, st, W);
+				}
+				if (GRAD)
+					for (int p = 0; p < P; p++)
+						atomicAdd(var.grad + p, (double)v.GG(p));
+				atomicAdd(var.transitions, trans);
+				trans = 0;
+			}
+			else
+			{
+				const unsigned long long r = __umul64hi(((unsigned long long)rb.y << 32) | rb.z, total);
+				const int wpg = (net.W + MBB_GROUPS - 1) / MBB_GROUPS;
+				unsigned long long cum = 0;
+				int g = -1;
+#pragma unroll
+				for (int i = 0; i < MBB_GROUPS; i++)
+				{
+					const bool hit = g < 0 && r < cum + gs[i];
+					g = hit ? i : g;
+					cum += (g < 0) ? gs[i] : 0ull;
+				}
+				if (g < 0)
+					g = 0; // unreachable: the group sums add up to total
+				int word = g * wpg;
+				for (int i = 0; i < wpg; i++)
+				{
+					const int w = g * wpg + i;
+					if (w >= net.W)
+						break;
+					word = w;
+					const uint32_t q = v.Q(w);
+					if (r < cum + q)
+						break;
+					cum += q;
+				}
+				const uint32_t sw = v.S(word);
+				uint32_t um = v.U(word);
+				int j = 32 * word + 31 - __clz(um | 1u);
+				while (um)
+				{
+					const int b = __ffs(um) - 1;
+					const int i = 32 * word + b;
+					const uint2 qq = __ldg(var.q + i);
+					const uint32_t q = ((sw >> b) & 1u) ? qq.y : qq.x;
+					j = i;
+					if (r < cum + q)
+						break;
+					cum += q;
+					um &= um - 1u;
+				}
+				const int jdir = (sw >> (j & 31)) & 1u; // 0: j switches on (up rate), 1: off (down rate)
+				if (GRAD)
+				{
+					const float rj = __ldg(var.rate + 2 * j + jdir);
+					const int a = __ldg(var.g_ptr + 2 * j + jdir), b = __ldg(var.g_ptr + 2 * j + jdir + 1);
+					for (int e = a; e < b; e++)
+						v.GS(__ldg(var.g_p + e)) += __ldg(var.g_d + e) / rj;
+					if (discrete)
+					{
+						const float a0 = (float)total * (1.0f / (float)(1u << var.rate_shift));
+						for (int p = 0; p < P; p++)
+							v.GS(p) -= v.GD(p) / a0;
+					}
+				}
+
+				// flip j and re-evaluate it and the nodes whose logic reads it
+				v.S(j >> 5) ^= 1u << (j & 31);
+				const uint4 nj = __ldg(net.node + j);
+				const int pj = (int)(nj.w >> 16) - 1;
+				if (pj >= 0)
+					idx ^= 1u << pj;
+				bool ni_changed = pj >= 0;
+				const int d0 = (int)nj.z, d1 = d0 + (int)(nj.w & 0xffffu);
+				for (int d = d0; d < d1; d++)
+				{
+					const uint4 hdr = __ldg(net.hdr + d);
+					const uint4 in = __ldg(net.in1 + d);
+					const int k = (int)(hdr.x & 0xffffu);
+					const int wk = k >> 5;
+					const uint32_t bk = 1u << (k & 31);
+					const bool on = (v.S(wk) & bk) != 0;
+					const bool was_on = (k == j) ? !on : on;
+					const uint32_t uw = v.U(wk);
+					const bool was_unstable = (uw & bk) != 0;
+					const bool unstable = on != mbb_logic(net, v, d, hdr, in);
+					const uint2 qq = __ldg(var.q + k);
+					const uint32_t qo = was_unstable ? (was_on ? qq.y : qq.x) : 0u;
+					const uint32_t qn = unstable ? (on ? qq.y : qq.x) : 0u;
+					if (unstable != was_unstable)
+						v.U(wk) = uw ^ bk;
+					if (qn != qo)
+					{
+						const long long dq = (long long)qn - (long long)qo;
+						v.Q(wk) += (uint32_t)dq;
+						mbb_group_add(gs, wk / wpg, dq);
+						total += (unsigned long long)dq;
+					}
+					if (GRAD && (unstable != was_unstable || on != was_on))
+					{
+						if (was_unstable)
+							mbb_grad_active(var, v, k, was_on ? 1 : 0, -1.f, time, discrete);
+						if (unstable)
+							mbb_grad_active(var, v, k, on ? 1 : 0, 1.f, time, discrete);
+					}
+					if (qn != qo || unstable != was_unstable)
+						ni_changed |= ((hdr.x >> 21) & 31u) != 0u;
+				}
+				if (ni_changed)
+					h = mbb_entropy(net, var, v);
+			}
+		}
+		__syncwarp();
+	}
+	if (acc_var >= 0)
+		mb_acc_flush(acc, B.vars[acc_var].st, B.vars[acc_var].st.win_h);
+}
+
+extern "C" __global__ void __launch_bounds__(128) mb_batched_fast(mb_batch_params B) { mbb_body<false>(B); }
+extern "C" __global__ void __launch_bounds__(128) mb_batched_grad(mb_batch_params B) { mbb_body<true>(B); }

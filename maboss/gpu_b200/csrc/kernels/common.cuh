@@ -1,0 +1,151 @@
+// Device helpers that do not depend on the model: hashing, fixed-point window accumulation and a
+// runtime-width fixed-point hash insert. Shared by the NVRTC-compiled engine (kernels/engine.cuh)
+// and the ahead-of-time compiled batched kernels (kernels/batched.cuh).
+#pragma once
+
+__device__ __forceinline__ unsigned long long mb_mix64(unsigned long long x)
+{
+	x ^= x >> 30;
+	x *= 0xbf58476d1ce4e5b9ull;
+	x ^= x >> 27;
+	x *= 0x94d049bb133111ebull;
+	x ^= x >> 31;
+	return x;
+}
+
+// ---------------------------------------------------------------- window accumulation
+
+// Per-thread run-length accumulator: consecutive slices that fall into the same
+// (window, non-internal state) bin are summed in a register before one atomic.
+struct mb_win_acc
+{
+	int ow;
+	uint32_t oi;
+	long long oq;
+	int hw;
+	long long hq;
+};
+
+__device__ __forceinline__ void mb_acc_init(mb_win_acc& a)
+{
+	a.ow = -1;
+	a.oi = 0;
+	a.oq = 0;
+	a.hw = -1;
+	a.hq = 0;
+}
+
+__device__ __forceinline__ void mb_add_h(long long* hsink, int w, long long v)
+{
+	if (v != 0)
+		atomicAdd(reinterpret_cast<unsigned long long*>(hsink + w), (unsigned long long)v);
+}
+
+__device__ __forceinline__ void mb_acc_flush(mb_win_acc& a, const mb_stats_params& p, long long* hsink)
+{
+	if (a.ow >= 0 && a.oq != 0)
+		atomicAdd(reinterpret_cast<unsigned long long*>(p.win_occ + (size_t)a.ow * p.n_bins + a.oi),
+				  (unsigned long long)a.oq);
+	if (a.hw >= 0)
+		mb_add_h(hsink, a.hw, a.hq);
+	mb_acc_init(a);
+}
+
+// Continuous time: the state `idx` occupies (t0, t1]; split it over windows exactly like
+// window_average_small.cu:66-92 and add each slice (and h * slice) to its window.
+__device__ __forceinline__ void mb_record_cont(mb_win_acc& a, const mb_stats_params& p, long long* hsink,
+											   uint32_t idx, float t0, float t1, float h)
+{
+	float sb = t0;
+	int w = (int)floorf(sb / p.win_tick);
+	for (int guard = 0; t1 > sb && guard <= p.n_windows + 2; guard++)
+	{
+		const float we = (float)(w + 1) * p.win_tick;
+		const float se = fminf(t1, we);
+		const float sl = se - sb;
+		if (w >= 0 && w < p.n_windows)
+		{
+			const long long q = __double2ll_rn((double)sl * p.fx);
+			if (w == a.ow && idx == a.oi)
+				a.oq += q;
+			else
+			{
+				if (a.ow >= 0 && a.oq != 0)
+					atomicAdd(reinterpret_cast<unsigned long long*>(p.win_occ + (size_t)a.ow * p.n_bins + a.oi),
+							  (unsigned long long)a.oq);
+				a.ow = w;
+				a.oi = idx;
+				a.oq = q;
+			}
+			const long long hq = __double2ll_rn((double)__fmul_rn(h, sl) * p.fx_h);
+			if (w == a.hw)
+				a.hq += hq;
+			else
+			{
+				if (a.hw >= 0)
+					mb_add_h(hsink, a.hw, a.hq);
+				a.hw = w;
+				a.hq = hq;
+			}
+		}
+		w++;
+		sb = se;
+	}
+}
+
+// Discrete time: count the state at window lround(t0 / tick) (window_average_small.cu:117-130).
+__device__ __forceinline__ void mb_record_disc(const mb_stats_params& p, long long* hsink, uint32_t idx, float t0,
+											   float h)
+{
+	const int w = (int)lroundf(t0 / p.win_tick);
+	if (w >= 0 && w < p.n_windows)
+	{
+		atomicAdd(p.win_cnt + (size_t)w * p.n_bins + idx, 1u);
+		mb_add_h(hsink, w, __double2ll_rn((double)h * p.fx_h));
+	}
+}
+
+// Fixed-point hash insert for a state of `words` words (runtime width; same keys and probing as
+// mb_fixed_insert of the engine, so both produce the same table layout).
+__device__ inline void mb_fixed_insert_rt(const mb_stats_params& p, const unsigned* st, int words)
+{
+	mb_key128 k;
+	if (words <= 3)
+	{
+		k.lo = (unsigned long long)st[0] | (words > 1 ? (unsigned long long)st[1] << 32 : 0ull);
+		k.hi = (words > 2 ? (unsigned long long)st[2] : 0ull) | (1ull << 63);
+	}
+	else
+	{
+		unsigned long long a = 0x243f6a8885a308d3ull, b = 0x13198a2e03707344ull;
+		for (int w = 0; w < words; w++)
+		{
+			a = mb_mix64(a ^ ((unsigned long long)st[w] + 0x9e3779b97f4a7c15ull * (w + 1)));
+			b = mb_mix64(b + ((unsigned long long)st[w] ^ (0xc2b2ae3d27d4eb4full * (w + 7))));
+		}
+		k.lo = a;
+		k.hi = b | (1ull << 63);
+	}
+	const unsigned h = (unsigned)mb_mix64(k.lo ^ mb_mix64(k.hi));
+	mb_key128 empty;
+	empty.lo = 0;
+	empty.hi = 0;
+	for (unsigned probe = 0; probe <= p.fp_mask; probe++)
+	{
+		const unsigned slot = (h + probe) & p.fp_mask;
+		const mb_key128 prev = atomicCAS(p.fp_keys + slot, empty, k);
+		if (prev.lo == 0ull && prev.hi == 0ull)
+		{
+			for (int w = 0; w < words; w++)
+				p.fp_states[(size_t)slot * words + w] = st[w];
+			atomicAdd(p.fp_counts + slot, 1u);
+			return;
+		}
+		if (prev.lo == k.lo && prev.hi == k.hi)
+		{
+			atomicAdd(p.fp_counts + slot, 1u);
+			return;
+		}
+	}
+	atomicAdd(p.fp_overflow, 1u);
+}

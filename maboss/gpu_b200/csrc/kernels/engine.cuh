@@ -48,16 +48,6 @@ __device__ __forceinline__ void mb_init_state(state_word_t* st, RNG& rng, const 
 	}
 }
 
-__device__ __forceinline__ unsigned long long mb_mix64(unsigned long long x)
-{
-	x ^= x >> 30;
-	x *= 0xbf58476d1ce4e5b9ull;
-	x ^= x >> 27;
-	x *= 0x94d049bb133111ebull;
-	x ^= x >> 31;
-	return x;
-}
-
 // 128-bit fixed-point key: the state itself when it fits in 96 bits, else two independent
 // 64-bit hashes. The top bit is always set so that 0 marks an empty slot.
 __device__ __forceinline__ mb_key128 mb_state_key(const state_word_t* st)
@@ -110,98 +100,6 @@ __device__ void mb_fixed_insert(const mb_stats_params& p, const state_word_t* st
 		}
 	}
 	atomicAdd(p.fp_overflow, 1u);
-}
-
-// ---------------------------------------------------------------- window accumulation
-
-// Per-thread run-length accumulator: consecutive slices that fall into the same
-// (window, non-internal state) bin are summed in a register before one atomic.
-struct mb_win_acc
-{
-	int ow;
-	uint32_t oi;
-	long long oq;
-	int hw;
-	long long hq;
-};
-
-__device__ __forceinline__ void mb_acc_init(mb_win_acc& a)
-{
-	a.ow = -1;
-	a.oi = 0;
-	a.oq = 0;
-	a.hw = -1;
-	a.hq = 0;
-}
-
-__device__ __forceinline__ void mb_add_h(long long* hsink, int w, long long v)
-{
-	if (v != 0)
-		atomicAdd(reinterpret_cast<unsigned long long*>(hsink + w), (unsigned long long)v);
-}
-
-__device__ __forceinline__ void mb_acc_flush(mb_win_acc& a, const mb_stats_params& p, long long* hsink)
-{
-	if (a.ow >= 0 && a.oq != 0)
-		atomicAdd(reinterpret_cast<unsigned long long*>(p.win_occ + (size_t)a.ow * p.n_bins + a.oi),
-				  (unsigned long long)a.oq);
-	if (a.hw >= 0)
-		mb_add_h(hsink, a.hw, a.hq);
-	mb_acc_init(a);
-}
-
-// Continuous time: the state `idx` occupies (t0, t1]; split it over windows exactly like
-// window_average_small.cu:66-92 and add each slice (and h * slice) to its window.
-__device__ __forceinline__ void mb_record_cont(mb_win_acc& a, const mb_stats_params& p, long long* hsink,
-											   uint32_t idx, float t0, float t1, float h)
-{
-	float sb = t0;
-	int w = (int)floorf(sb / p.win_tick);
-	for (int guard = 0; t1 > sb && guard <= p.n_windows + 2; guard++)
-	{
-		const float we = (float)(w + 1) * p.win_tick;
-		const float se = fminf(t1, we);
-		const float sl = se - sb;
-		if (w >= 0 && w < p.n_windows)
-		{
-			const long long q = __double2ll_rn((double)sl * p.fx);
-			if (w == a.ow && idx == a.oi)
-				a.oq += q;
-			else
-			{
-				if (a.ow >= 0 && a.oq != 0)
-					atomicAdd(reinterpret_cast<unsigned long long*>(p.win_occ + (size_t)a.ow * p.n_bins + a.oi),
-							  (unsigned long long)a.oq);
-				a.ow = w;
-				a.oi = idx;
-				a.oq = q;
-			}
-			const long long hq = __double2ll_rn((double)__fmul_rn(h, sl) * p.fx_h);
-			if (w == a.hw)
-				a.hq += hq;
-			else
-			{
-				if (a.hw >= 0)
-					mb_add_h(hsink, a.hw, a.hq);
-				a.hw = w;
-				a.hq = hq;
-			}
-		}
-		w++;
-		sb = se;
-	}
-}
-
-// Discrete time: count the state at window lround(t0 / tick) (window_average_small.cu:117-130).
-__device__ __forceinline__ void mb_record_disc(const mb_stats_params& p, long long* hsink, uint32_t idx, float t0,
-											   float h)
-{
-	const int w = (int)lroundf(t0 / p.win_tick);
-	if (w >= 0 && w < p.n_windows)
-	{
-		atomicAdd(p.win_cnt + (size_t)w * p.n_bins + idx, 1u);
-		mb_add_h(hsink, w, __double2ll_rn((double)h * p.fx_h));
-	}
 }
 
 __device__ __forceinline__ void mb_record(mb_win_acc& a, const mb_stats_params& p, long long* hsink,

@@ -239,6 +239,66 @@ class Runner:
         return n.value
 
 
+def _names_values(params: dict[str, float] | None):
+    params = params or {}
+    names = (C.c_char_p * max(1, len(params)))(*[k.encode() for k in params])
+    values = (C.c_float * max(1, len(params)))(*[float(v) for v in params.values()])
+    return names, values, len(params)
+
+
+class Batch:
+    """Parameter variants of one or more networks in one persistent launch (fast-mode algorithm)."""
+
+    def __init__(self, ctx: Context):
+        h = C.c_void_p()
+        check(lib().mb_batch_create(ctx._h, C.byref(h)))
+        self._h = h
+        self.ctx = ctx
+        self._models = []
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().mb_batch_free(h)
+            self._h = None
+
+    def add_model(self, model: Model) -> int:
+        n = C.c_int()
+        check(lib().mb_batch_add_model(self._h, model._h, C.byref(n)))
+        self._models.append(model)
+        return n.value
+
+    def add_variant(self, net: int, n_traj: int, params: dict[str, float] | None = None,
+                    first_traj: int = 0) -> int:
+        names, values, k = _names_values(params)
+        v = C.c_int()
+        check(lib().mb_batch_add_variant(self._h, net, names, values, k, n_traj, first_traj, C.byref(v)))
+        return v.value
+
+    def run(self, seed: int = 0) -> float:
+        ms = C.c_float()
+        check(lib().mb_batch_run(self._h, seed, C.byref(ms)))
+        return ms.value
+
+    def result(self, variant: int) -> "Result":
+        h = C.c_void_p()
+        check(lib().mb_batch_result(self._h, variant, C.byref(h)))
+        return Result(h)
+
+
+def gradient(ctx: Context, model: Model, params: dict[str, float], cotangent: np.ndarray, n_traj: int,
+             seed: int = 0) -> tuple[np.ndarray, "Result"]:
+    """d/dparams of sum(cotangent * window_probs) by the score-function estimator (same trajectories
+    as the forward statistics, which are returned too)."""
+    names, values, k = _names_values(params)
+    cot = np.ascontiguousarray(cotangent, dtype=np.float64).ravel()
+    grad = np.zeros(max(1, k), np.float64)
+    h = C.c_void_p()
+    check(lib().mb_gradient(ctx._h, model._h, names, values, k, n_traj, seed, cot.ctypes.data, grad.ctypes.data,
+                            C.byref(h)))
+    return grad[:k], Result(h)
+
+
 def rand_state_size() -> int:
     return int(lib().mb_rand_state_size())
 

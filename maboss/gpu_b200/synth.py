@@ -144,20 +144,45 @@ def c4(seed: int = 0, sample_count: int = 1_000_000, sim_seed: int = 0) -> tuple
 
 
 def c5_base(index: int, sample_count: int = 10_000, sim_seed: int = 0) -> tuple[str, str]:
-    """Base network `index` (0..7) of the batched sweep: 20-500 nodes, 2-4 inputs, 8 outputs."""
+    """Base network `index` (0..7) of the batched sweep: 20-500 nodes, 2-4 inputs, 8 outputs, node
+    rates given by variables $u_i / $d_i (lognormal(0, 0.5)) so that variants can rescale them."""
     rng = np.random.default_rng(1000 + index)
     n = int(np.round(np.exp(rng.uniform(np.log(20), np.log(500)))))
     kin = int(rng.integers(2, 5))
     names = [f"B{index}_{i}" for i in range(n)]
+    variables = {}
     bnd = ""
     for i in range(n):
         inputs = [names[j] for j in rng.choice(n, kin, replace=False)]
         up, down = np.exp(rng.normal(0.0, 0.5, 2))
-        bnd += _node(names[i], _tree(rng, inputs), _g6(up), _g6(down))
+        variables[f"$u_{i}"], variables[f"$d_{i}"] = float(_g6(up)), float(_g6(down))
+        bnd += _node(names[i], _tree(rng, inputs), f"$u_{i}", f"$d_{i}")
     max_time = float(rng.choice([20.0, 50.0, 100.0, 200.0]))
     internal = [i >= 8 for i in range(n)]
-    cfg = _cfg(names, internal, 0.5, sample_count, max_time, max_time / 40, False, sim_seed)
+    cfg = _cfg(names, internal, 0.5, sample_count, max_time, max_time / 40, False, sim_seed, variables)
     return bnd, cfg
+
+
+def c5_sweep(n_variants: int = 256, seed: int = 0):
+    """The batched sweep: (base network index, variable overrides, trajectories) per variant, with
+    lognormal(0, 0.3) multipliers on every rate and trajectories uniform in [1e3, 1e5]."""
+    rng = np.random.default_rng(seed)
+    bases = [c5_base(i) for i in range(8)]
+    base_vars = []
+    for bnd, cfg in bases:
+        vals = {}
+        for line in cfg.splitlines():
+            if line.startswith("$"):
+                k, v = line.rstrip(";").split(" = ")
+                vals[k] = float(v)
+        base_vars.append(vals)
+    variants = []
+    for v in range(n_variants):
+        net = v % 8
+        mult = np.exp(rng.normal(0.0, 0.3, len(base_vars[net])))
+        params = {k: float(np.float32(x * m)) for (k, x), m in zip(base_vars[net].items(), mult)}
+        variants.append((net, params, int(rng.integers(1_000, 100_001))))
+    return bases, variants
 
 
 WORKLOADS = {"c1": c1, "c2": c2, "c3": c3, "c4": c4}

@@ -672,6 +672,7 @@ struct compiled
 	std::vector<char> fast;			// fast-path form (generator.cpp:57-82)
 	std::vector<float> up, down;	// fast-path rate values as compiled
 	std::vector<float> ul, dl;		// r * log2(r) constants of the fast-mode entropy
+	std::vector<P> up_expr, down_expr; // U and D expressions of fast-path nodes
 	std::vector<flat> logic, rup, rdown;
 	// truth tables of fast-path logic (exactly the flat evaluation, tabulated over the inputs)
 	std::vector<std::vector<int>> tt_in;
@@ -744,6 +745,8 @@ float print6(float v)
 	return (float)std::strtod(buf, nullptr);
 }
 
+void setup_integer_rates(compiled& c);
+
 std::unique_ptr<compiled> compile(const std::string& bnd, const std::string& cfg)
 {
 	auto c = std::make_unique<compiled>();
@@ -772,6 +775,8 @@ std::unique_ptr<compiled> compile(const std::string& bnd, const std::string& cfg
 		const bool f =
 			n.attr("logic") && c->logic_ternary(n.attr("rate_up"), true, u) && c->logic_ternary(n.attr("rate_down"), false, d);
 		c->fast[i] = f;
+		c->up_expr.push_back(f ? n.attr("rate_up")->b : nullptr);
+		c->down_expr.push_back(f ? n.attr("rate_down")->c : nullptr);
 		if (f)
 		{
 			c->up[i] = (float)printed(u).get();
@@ -825,8 +830,23 @@ std::unique_ptr<compiled> compile(const std::string& bnd, const std::string& cfg
 		c->tt_in[i] = in;
 		c->tt[i] = t;
 	}
-	// integer-rate eligibility and fixed-point scale: largest per-32-node-word sum of
-	// max(up, down) below 2^31
+	setup_integer_rates(*c);
+	c->discrete = c->constant("discrete_time") != 0;
+	c->max_time_f = c->constant("max_time");
+	c->tick_f = c->constant("time_tick");
+	c->max_time_sim = print6(c->max_time_f);
+	c->tick_sim = print6(c->tick_f);
+	c->sample_count = (long long)c->constant("sample_count");
+	c->seed = (unsigned long long)c->constant("seed_pseudorandom");
+	c->T = (int)std::ceil(c->max_time_f / c->tick_f);
+	return c;
+}
+
+// integer-rate eligibility and fixed-point scale: largest per-32-node-word sum of max(up, down)
+// below 2^31 (the engine's build_incremental_tables)
+void setup_integer_rates(compiled& cc)
+{
+	compiled* c = &cc;
 	c->integer_rates = c->N > 0;
 	for (int i = 0; i < c->N; i++)
 		if (!c->fast[i] || c->tt_in[i].size() > 12 || c->tt[i].empty())
@@ -857,16 +877,8 @@ std::unique_ptr<compiled> compile(const std::string& bnd, const std::string& cfg
 			c->q_down[i] = (unsigned)qd;
 		}
 	}
-	c->discrete = c->constant("discrete_time") != 0;
-	c->max_time_f = c->constant("max_time");
-	c->tick_f = c->constant("time_tick");
-	c->max_time_sim = print6(c->max_time_f);
-	c->tick_sim = print6(c->tick_f);
-	c->sample_count = (long long)c->constant("sample_count");
-	c->seed = (unsigned long long)c->constant("seed_pseudorandom");
-	c->T = (int)std::ceil(c->max_time_f / c->tick_f);
-	return c;
 }
+
 
 // ------------------------------------------------------------------ simulation
 
@@ -1249,6 +1261,30 @@ int oracle_model_dims(const oracle_model* m, int* nodes, int* words, int* nonint
 	*seed = c.seed;
 	*tick = c.tick_f;
 	*max_time = c.max_time_f;
+	return 0;
+}
+
+// Set $variables and recompute the rates of @logic-form nodes as exact floats (no 6-digit
+// rounding), as the engine's batched runs do. Returns 0, or -1 for an unknown variable.
+int oracle_model_set_variables(oracle_model* m, const char* const* names, const float* values, int n)
+{
+	compiled& c = *m->c;
+	for (int i = 0; i < n; i++)
+	{
+		if (!c.m.vars.count(names[i]))
+			return -1;
+		c.m.vars[names[i]] = values[i];
+	}
+	for (int i = 0; i < c.N; i++)
+	{
+		if (!c.fast[i])
+			continue;
+		c.up[i] = feval(c.m, *c.up_expr[i]);
+		c.down[i] = feval(c.m, *c.down_expr[i]);
+		c.ul[i] = c.up[i] > 0 ? (float)((double)c.up[i] * std::log2((double)c.up[i])) : 0.f;
+		c.dl[i] = c.down[i] > 0 ? (float)((double)c.down[i] * std::log2((double)c.down[i])) : 0.f;
+	}
+	setup_integer_rates(c);
 	return 0;
 }
 

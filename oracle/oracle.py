@@ -45,6 +45,8 @@ def lib() -> C.CDLL:
                                         C.POINTER(C.c_ulonglong), C.POINTER(C.c_double)]
         L.oracle_result_num_fixed.argtypes = [C.c_void_p]
         L.oracle_result_fixed.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_model_set_variables.restype = C.c_int
+        L.oracle_model_set_variables.argtypes = [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int]
         L.oracle_trace.argtypes = [C.c_void_p, C.c_int, C.c_ulonglong, C.c_ulonglong, C.c_int,
                                    C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int]
         _LIB = L
@@ -93,6 +95,13 @@ class OracleModel:
         if getattr(self, "_h", None):
             lib().oracle_model_free(self._h)
             self._h = None
+
+    def set_variables(self, params: dict) -> None:
+        """Set $variables; rates of @logic-form nodes become exact floats (as in batched runs)."""
+        names = (C.c_char_p * max(1, len(params)))(*[k.encode() for k in params])
+        values = (C.c_float * max(1, len(params)))(*[float(v) for v in params.values()])
+        if lib().oracle_model_set_variables(self._h, names, values, len(params)) != 0:
+            raise KeyError("unknown variable")
 
     def rate(self, node: int, state_words) -> float:
         arr = (C.c_uint32 * self.words)(*state_words)

@@ -1,0 +1,155 @@
+"""Batched variants and score-function gradients (kernels/batched.cuh through the C ABI)."""
+import math
+
+import numpy as np
+import pytest
+
+import maboss.gpu_b200 as mb
+from conftest import model_text
+from maboss.gpu_b200 import synth
+from oracle.oracle import OracleModel
+
+pytestmark = pytest.mark.gpu
+
+
+def _same(a: "mb.Result", b: "mb.Result"):
+    ra, rb = a.raw(), b.raw()
+    for k in ("occ", "cnt", "h"):
+        assert np.array_equal(ra[k], rb[k]), k
+    assert np.array_equal(a.final_counts, b.final_counts)
+    assert a.transitions == b.transitions
+    assert [(s.tolist(), c) for s, c in a.fixed] == [(s.tolist(), c) for s, c in b.fixed]
+
+
+@pytest.mark.parametrize("name,n", [("metastasis", 2_000), ("sizek", 1_000), ("cellcycle", 3_000)])
+def test_batch_variant_without_overrides_equals_fast_mode(gpu, name, n):
+    model = mb.Model(*model_text(name))
+    b = mb.Batch(gpu)
+    net = b.add_model(model)
+    v = b.add_variant(net, n)
+    b.run(int(model.constant("seed_pseudorandom")))
+    _same(b.result(v), gpu.compile(model).run(mode="fast", sample_count=n))
+
+
+def test_batch_of_networks_and_variants_matches_oracle(gpu):
+    """Two networks of different sizes, rate variants and stream offsets in one launch; each
+    variant equals the oracle's integer-rate fast mode with the same exact rates."""
+    meta = model_text("metastasis")
+    base = synth.c5_base(2)
+    b = mb.Batch(gpu)
+    nets = [b.add_model(mb.Model(*meta)), b.add_model(mb.Model(*base))]
+    rng = np.random.default_rng(7)
+    cases = []
+    for net, (bnd, cfg) in zip(nets, [meta, base]):
+        o = OracleModel(bnd, cfg)
+        names = [k for k in mb.Model(bnd, cfg).variables][:6]
+        for first in (0, 5_000):
+            params = {k: float(np.float32(mb.Model(bnd, cfg).variable(k) * math.exp(rng.normal(0, 0.3))))
+                      for k in names}
+            n = int(rng.integers(300, 900))
+            cases.append((b.add_variant(net, n, params, first_traj=first), bnd, cfg, params, n, first))
+    seed = 11
+    b.run(seed)
+    for v, bnd, cfg, params, n, first in cases:
+        o = OracleModel(bnd, cfg)
+        o.set_variables(params)
+        r = b.result(v)
+        raw = r.raw()
+        ref = o.run(n=n, mode=1, seed=seed, first=first, occ_exp=raw["occ_exp"], ent_exp=raw["ent_exp"])
+        assert r.transitions == ref["transitions"]
+        assert np.array_equal(r.final_counts, ref["final"])
+        assert len(r.fixed) == len(ref["fixed_counts"])
+        assert np.all(np.abs(r.window_probs - ref["probs"]) <= 1e-5 + 1e-4 * ref["probs"])
+
+
+TWO_STATE = """
+node A { logic = !A; rate_up = @logic ? $u : 0; rate_down = @logic ? 0 : $d; }
+"""
+
+
+def _two_state_window_mean(u, d, p0, a, b):
+    lam = u + d
+    pi = u / lam
+    return pi + (p0 - pi) * (math.exp(-lam * a) - math.exp(-lam * b)) / (lam * (b - a))
+
+
+def test_gradient_of_two_state_chain_matches_analytic(gpu):
+    """A single node switching on at rate u and off at rate d: window probabilities and their
+    derivatives have closed forms; the score-function estimate must agree within its own spread
+    (4 independent seeds)."""
+    u, d, p0, tick, tmax = 1.3, 0.7, 0.25, 0.5, 3.0
+    cfg = f"$u = {u}; $d = {d}; A.istate = {p0}; max_time = {tmax}; time_tick = {tick};"
+    model = mb.Model(TWO_STATE, cfg)
+    T = int(round(tmax / tick))
+    cot = np.zeros((T, 2))
+    cot[:, 1] = 1.0  # L = sum over windows of P(A on)
+    est = []
+    for seed in range(4):
+        g, fwd = mb.gradient(gpu, model, {"$u": u, "$d": d}, cot, 400_000, seed)
+        est.append(g)
+        # forward probabilities of the same run
+        p = fwd.window_probs[:, 1]
+        exact = np.array([_two_state_window_mean(u, d, p0, w * tick, (w + 1) * tick) for w in range(T)])
+        assert np.all(np.abs(p - exact) < 5 * np.sqrt(exact * (1 - exact) / 400_000) + 1e-6)
+    est = np.array(est)
+    h = 1e-6
+
+    def L(uu, dd):
+        return sum(_two_state_window_mean(uu, dd, p0, w * tick, (w + 1) * tick) for w in range(T))
+
+    exact = np.array([(L(u + h, d) - L(u - h, d)) / (2 * h), (L(u, d + h) - L(u, d - h)) / (2 * h)])
+    mean, sem = est.mean(axis=0), est.std(axis=0, ddof=1) / 2.0
+    assert np.all(np.abs(mean - exact) < 4 * sem + 0.01 * np.abs(exact)), (mean, exact, sem)
+
+
+def test_gradient_matches_common_random_number_finite_differences(gpu):
+    """C4-style network: score-function gradients of sum_w P_w(output node 0 on) against central
+    finite differences with common random numbers (variants with the same random streams in one
+    batched launch). Both are Monte-Carlo estimates: over 4 seeds, the means must agree within 4
+    combined standard errors plus 2% of |FD|. The step is 1% of each parameter: with 1e3-fold
+    smaller steps the finite-difference noise at this sample size exceeds most of the gradients."""
+    bnd, cfg = synth.c4()
+    model = mb.Model(bnd, cfg)
+    names = [f"$u_{i}" for i in range(4)] + [f"$d_{i}" for i in range(4)]
+    theta = {k: model.variable(k) for k in names}
+    n = 500_000
+    dims = gpu.compile(model).run(mode="fast", sample_count=10).dims
+    T, S = dims.windows, dims.bins
+    cot = np.zeros((T, S))
+    cot[:, [s for s in range(S) if s & 1]] = 1.0  # output node 0 on
+    sf, fd = [], []
+    for seed in range(4):
+        g, _ = mb.gradient(gpu, model, theta, cot, n, seed=seed)
+        sf.append(g)
+        b = mb.Batch(gpu)
+        net = b.add_model(model)
+        pairs = []
+        for k in names:
+            hk = 1e-2 * theta[k]
+            pairs.append((b.add_variant(net, n, dict(theta, **{k: theta[k] + hk})),
+                          b.add_variant(net, n, dict(theta, **{k: theta[k] - hk})), 2 * hk))
+        b.run(seed)
+        fd.append([((b.result(p).window_probs - b.result(m).window_probs) * cot).sum() / span
+                   for p, m, span in pairs])
+    sf, fd = np.array(sf), np.array(fd)
+    se = np.sqrt(sf.var(axis=0, ddof=1) / 4 + fd.var(axis=0, ddof=1) / 4)
+    diff = np.abs(sf.mean(axis=0) - fd.mean(axis=0))
+    assert np.all(diff <= 4 * se + 0.02 * np.abs(fd.mean(axis=0))), (sf.mean(axis=0), fd.mean(axis=0), se)
+
+
+def test_autograd_function(gpu):
+    import torch
+
+    from maboss.gpu_b200.autograd import window_probabilities
+
+    u, d = 1.3, 0.7
+    model = mb.Model(TWO_STATE, f"$u = {u}; $d = {d}; A.istate = 0.25; max_time = 2; time_tick = 0.5;")
+    theta = torch.tensor([u, d], dtype=torch.float64, requires_grad=True)
+    probs = window_probabilities(theta, gpu, model, ["$u", "$d"], 100_000, seed=5)
+    loss = probs[:, 1].sum()
+    loss.backward()
+    cot = np.zeros(tuple(probs.shape))
+    cot[:, 1] = 1.0
+    g, fwd = mb.gradient(gpu, model, {"$u": u, "$d": d}, cot, 100_000, 5)
+    assert np.allclose(probs.detach().numpy(), fwd.window_probs)
+    assert np.allclose(theta.grad.numpy(), g)
