@@ -261,6 +261,14 @@ void emit_incremental_tables(std::ostream& ss, const model_layout& L)
 	emit_array(ss, "uint4", "mbg_inc_rec_in2", u4(t.in2));
 	emit_array(ss, "unsigned", "mbg_inc_tt", t.tt);
 	emit_array(ss, "int", "mbg_inc_self", t.self);
+	// float rates (up, down) of every node as the generated rate functions return them (exact mode)
+	std::vector<std::string> rate;
+	for (int i = 0; i < L.state_size; i++)
+	{
+		rate.push_back(flit(L.up[i]));
+		rate.push_back(flit(L.down[i]));
+	}
+	emit_array(ss, "float", "mbg_inc_rate", rate);
 	std::vector<std::string> f_up, f_down, f_ul, f_dl;
 	for (int i : L.noninternal_nodes)
 	{

@@ -229,14 +229,8 @@ __device__ __forceinline__ void mb_fused_body(const mb_fused_params& P)
 	}
 }
 
-#ifdef MB_FAMILY_EXACT
-extern "C" __global__ void __launch_bounds__(256) mb_fused_exact(mb_fused_params P) { mb_fused_body<true>(P); }
-#endif
 
-#ifdef MB_FAMILY_FAST
-#ifndef MBG_INCREMENTAL
-extern "C" __global__ void __launch_bounds__(256) mb_fused_fast(mb_fused_params P) { mb_fused_body<false>(P); }
-#else
+#ifdef MBG_INCREMENTAL
 // ---------------------------------------------------------------- incremental fast kernel
 // Fast mode for models whose rates all have the form `@logic ? U : 0` / `@logic ? 0 : D`.
 // A node is unstable when its bit differs from its logic; only unstable nodes have a rate
@@ -388,6 +382,271 @@ __device__ __forceinline__ void mb_incr_start(const mb_fused_params& P, const mb
 	__syncwarp();
 }
 
+#endif // MBG_INCREMENTAL
+
+#ifdef MB_FAMILY_EXACT
+#ifndef MBG_INCREMENTAL
+extern "C" __global__ void __launch_bounds__(256) mb_fused_exact(mb_fused_params P) { mb_fused_body<true>(P); }
+#else
+// Exact mode for models whose rates all have the @logic form. Bit-identical to the reference
+// algorithm (XORWOW streams, draw order, fp32 operation order, epoch boundary), but without
+// evaluating all N rate functions per step: a stable node's rate is exactly 0 and x + 0.0f == x,
+// so the reference's sequential fp32 sum over all nodes equals the sequential sum over the unstable
+// nodes in node order, and its prefix-count flip selection always stops at an unstable node
+// (simulation.cu:9-21: the first prefix sum reaching r belongs to a node with a non-zero rate).
+// Unstable masks are kept incrementally as in the fast kernel; rates are the float values of the
+// generated code (mbg_inc_rate).
+extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params P)
+{
+	extern __shared__ uint32_t mb_smem_u32[];
+	const int B = blockDim.x;
+	const int lane = threadIdx.x & 31;
+	mb_incr_view v;
+	v.stride = B;
+	v.st = mb_smem_u32 + threadIdx.x;
+	v.un = mb_smem_u32 + (size_t)state_words * B + threadIdx.x;
+	v.ws = v.un; // word sums are not used in exact mode
+	long long* hsink = P.st.win_h;
+	long long* smem_h = reinterpret_cast<long long*>(mb_smem_u32 + (size_t)2 * state_words * B);
+	if (P.st.h_in_smem)
+	{
+		for (int i = threadIdx.x; i < P.st.n_windows; i += B)
+			smem_h[i] = 0;
+		__syncthreads();
+		hsink = smem_h;
+	}
+
+	unsigned long long trans = 0;
+	mb_win_acc acc;
+	mb_acc_init(acc);
+	bool working = true, running = false;
+	uint32_t idx = 0;
+	float time = 0.f;
+	int slot = 1;
+	curandState rng;
+
+	while (__any_sync(0xffffffffu, working || running))
+	{
+		bool starting = false;
+		if (working && !running)
+		{
+			const unsigned long long t = atomicAdd(P.next_traj, 1ull);
+			if (t < P.n_traj)
+			{
+				starting = true;
+				curand_init(P.seed, P.first_traj + t, 0ull, &rng);
+				// initial state: one uniform per node in node order (simulation.cu:51-53)
+				for (int w = 0; w < state_words; w++)
+				{
+					uint32_t sw = 0;
+					const int nb = (w == state_words - 1) ? state_size - 32 * w : 32;
+					for (int b = 0; b < nb; b++)
+						if (curand_uniform(&rng) <= __ldg(P.istate + 32 * w + b))
+							sw |= 1u << b;
+					v.S(w) = sw;
+				}
+			}
+			else
+				working = false;
+		}
+		__syncwarp();
+		unsigned pending = __ballot_sync(0xffffffffu, starting);
+		while (pending)
+		{
+			// unstable masks and non-internal index of lane src's initial state, one node per lane
+			const int src = __ffs(pending) - 1;
+			pending &= pending - 1u;
+			mb_incr_view c = v;
+			const int off = (int)threadIdx.x - ((int)(threadIdx.x & ~31u) + src);
+			c.st = v.st - off;
+			c.un = v.un - off;
+			uint32_t ix = 0;
+			for (int w = 0; w < state_words; w++)
+			{
+				const int i = 32 * w + lane;
+				const bool on = (c.S(w) >> lane) & 1u;
+				bool unstable = false;
+				uint32_t nibit = 0;
+				if (i < state_size)
+				{
+					const int r = __ldg(mbg_inc_self + i);
+					const uint4 hdr = __ldg(mbg_inc_rec_hdr + r);
+					unstable = on != mb_incr_logic(c, r, hdr, __ldg(mbg_inc_rec_in + r));
+					const int pos = (int)((hdr.x >> 21) & 31u) - 1;
+					nibit = (pos >= 0 && on) ? (1u << pos) : 0u;
+				}
+				const uint32_t um = __ballot_sync(0xffffffffu, unstable);
+				ix |= __reduce_or_sync(0xffffffffu, nibit);
+				if (lane == 0)
+					c.U(w) = um;
+			}
+			__syncwarp();
+			if (lane == src)
+				idx = ix;
+		}
+		if (starting)
+		{
+			time = 0.f;
+			slot = 1;
+			running = true;
+		}
+
+		float total = 0.f, h = 0.f, tn = 0.f;
+		if (running)
+		{
+			// compute_transition_rates: sequential fp32 sum over the unstable nodes in node order
+			for (int w = 0; w < state_words; w++)
+			{
+				uint32_t um = v.U(w);
+				const uint32_t sw = v.S(w);
+				while (um)
+				{
+					const int b = __ffs(um) - 1;
+					um &= um - 1u;
+					total += __ldg(mbg_inc_rate + 2 * (32 * w + b) + ((sw >> b) & 1u));
+				}
+			}
+			if (isinf(total))
+			{
+				// an infinite total rate gives zero waiting times forever: stop this trajectory
+				atomicAdd(P.errors, 1u);
+				running = false;
+				atomicAdd(P.st.final_cnt + idx, 1u);
+			}
+			else if (total == 0.f)
+				tn = max_time;
+			else
+			{
+				if (discrete_time)
+				{
+					tn = time + time_tick;
+					tn = max_time - time_tick < tn ? max_time : tn;
+				}
+				else
+					tn = time + -logf(curand_uniform(&rng)) / total;
+				tn = fminf(tn, max_time);
+				// compute_transition_entropy over the non-internal rates
+				float ni_total = 0.f;
+				for (int k = 0; k < mbg_noninternal_count; k++)
+				{
+					const int i = __ldg(mbg_inc_ni_node + k);
+					const uint32_t bit = 1u << (i & 31);
+					if (v.U(i >> 5) & bit)
+						ni_total += __ldg(mbg_inc_rate + 2 * i + ((v.S(i >> 5) & bit) ? 1 : 0));
+				}
+				if (ni_total != 0.f)
+				{
+					float entropy = 0.f;
+					for (int k = 0; k < mbg_noninternal_count; k++)
+					{
+						const int i = __ldg(mbg_inc_ni_node + k);
+						const uint32_t bit = 1u << (i & 31);
+						const float r =
+							(v.U(i >> 5) & bit) ? __ldg(mbg_inc_rate + 2 * i + ((v.S(i >> 5) & bit) ? 1 : 0)) : 0.f;
+						const float tmp_prob = r / ni_total;
+						entropy -= (tmp_prob == 0.f) ? 0.f : log2f(tmp_prob) * tmp_prob;
+					}
+					h = entropy;
+				}
+			}
+		}
+		if (running)
+		{
+			trans += (tn != 0.f) ? 1ull : 0ull;
+			if (tn != 0.f)
+			{
+				if (discrete_time)
+					mb_record_disc(P.st, hsink, idx, time, h);
+				else
+					mb_record_cont(acc, P.st, hsink, idx, time, tn, h);
+			}
+			time = tn;
+			if (time >= max_time)
+			{
+				running = false;
+				atomicAdd(P.st.final_cnt + idx, 1u);
+				if (total == 0.f)
+				{
+					state_word_t st[state_words];
+#pragma unroll
+					for (int w = 0; w < state_words; w++)
+						st[w] = v.S(w);
+					mb_fixed_insert(P.st, st);
+				}
+			}
+			else if (P.traj_len > 1 && ++slot >= P.traj_len)
+				slot = 1; // epoch boundary: the next epoch re-evaluates the same state
+			else
+			{
+				// select_flip_bit: the first node whose running fp32 sum reaches r
+				const float r = curand_uniform(&rng) * total;
+				float sum = 0.f;
+				int j = -1, last = -1;
+				for (int w = 0; w < state_words && j < 0; w++)
+				{
+					uint32_t um = v.U(w);
+					const uint32_t sw = v.S(w);
+					while (um)
+					{
+						const int b = __ffs(um) - 1;
+						um &= um - 1u;
+						last = 32 * w + b;
+						sum += __ldg(mbg_inc_rate + 2 * last + ((sw >> b) & 1u));
+						if (!(sum < r))
+						{
+							j = last;
+							break;
+						}
+					}
+				}
+				if (j < 0)
+					j = last; // unreachable: the last prefix sum equals total >= r
+
+				// flip j and re-evaluate it and the nodes whose logic reads it
+				v.S(j >> 5) ^= 1u << (j & 31);
+				const uint4 nj = __ldg(mbg_inc_node + j);
+				const int pj = (int)(nj.w >> 16) - 1;
+				if (pj >= 0)
+					idx ^= 1u << pj;
+				const int d0 = (int)nj.z, d1 = d0 + (int)(nj.w & 0xffffu);
+				for (int d = d0; d < d1; d++)
+				{
+					const uint4 hdr = __ldg(mbg_inc_rec_hdr + d);
+					const int k = (int)(hdr.x & 0xffffu);
+					const uint32_t bk = 1u << (k & 31);
+					const bool on = (v.S(k >> 5) & bk) != 0;
+					const bool unstable = on != mb_incr_logic(v, d, hdr, __ldg(mbg_inc_rec_in + d));
+					const uint32_t uw = v.U(k >> 5);
+					if (unstable != ((uw & bk) != 0))
+						v.U(k >> 5) = uw ^ bk;
+				}
+			}
+		}
+		__syncwarp();
+	}
+	mb_acc_flush(acc, P.st, hsink);
+
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+		trans += __shfl_down_sync(0xffffffffu, trans, o);
+	if (lane == 0 && trans)
+		atomicAdd(P.transitions, trans);
+
+	if (P.st.h_in_smem)
+	{
+		__syncthreads();
+		for (int i = threadIdx.x; i < P.st.n_windows; i += B)
+			if (smem_h[i] != 0)
+				atomicAdd(reinterpret_cast<unsigned long long*>(P.st.win_h + i), (unsigned long long)smem_h[i]);
+	}
+}
+#endif // MBG_INCREMENTAL
+#endif // MB_FAMILY_EXACT
+
+#ifdef MB_FAMILY_FAST
+#ifndef MBG_INCREMENTAL
+extern "C" __global__ void __launch_bounds__(256) mb_fused_fast(mb_fused_params P) { mb_fused_body<false>(P); }
+#else
 extern "C" __global__ void __launch_bounds__(128, 4) mb_fused_fast(mb_fused_params P)
 {
 	extern __shared__ uint32_t mb_smem_u32[];

@@ -607,16 +607,17 @@ void launch_fused(module& m, const run_config& c, stats_state& st, long long n, 
 	CUfunction f = c.mode == MB_MODE_FUSED_EXACT ? m.fused_exact : m.fused_fast;
 	int block = c.block;
 	size_t smem = st.h_smem();
-	if (c.mode == MB_MODE_FUSED_FAST && m.incremental)
+	if (m.incremental)
 	{
-		// per thread: state words, unstable masks and word rate sums in shared memory
+		// per thread in shared memory: state words and unstable masks (+ word rate sums in fast mode)
+		const size_t per_word = c.mode == MB_MODE_FUSED_FAST ? 12 : 8;
 		constexpr size_t max_smem = 227 * 1024;
 		block = std::min(block, 128);
-		while (block > 32 && (size_t)12 * m.state_words * block + smem > max_smem)
+		while (block > 32 && per_word * m.state_words * block + smem > max_smem)
 			block -= 32;
-		if ((size_t)12 * m.state_words * block + smem > max_smem)
+		if (per_word * m.state_words * block + smem > max_smem)
 			throw engine_error(MB_ERR_LIMIT, "model too large for the incremental kernel's shared memory");
-		smem += (size_t)12 * m.state_words * block;
+		smem += per_word * m.state_words * block;
 	}
 	const int per_sm = c.blocks_per_sm > 0 ? c.blocks_per_sm : occupancy_blocks(f, block, smem);
 	const long long needed = (n + block - 1) / block;

@@ -59,7 +59,7 @@ def test_exact_mode_matches_oracle_on_reference_models(gpu, name, n):
 
 @pytest.mark.parametrize("gen,kw,n", [(synth.c1, {}, 20_000), (synth.c2, dict(noninternal=20), 300),
                                       (synth.c2, dict(noninternal=12, discrete=True), 2_000),
-                                      (synth.c4, {}, 2_000), (synth.c3, {}, 40)])
+                                      (synth.c4, {}, 2_000), (synth.c3, {}, 300)])
 def test_exact_mode_matches_oracle_on_synthetic_networks(gpu, gen, kw, n):
     bnd, cfg = gen(**kw)
     model, res, raw, o, ref = _run_both(gpu, bnd, cfg, n)
@@ -106,6 +106,38 @@ def test_epoch_mode_is_identical_to_fused_exact(gpu, name, n):
     assert np.array_equal(a.final_counts, b.final_counts)
     assert a.transitions == b.transitions
     assert [(s.tolist(), c) for s, c in a.fixed] == [(s.tolist(), c) for s, c in b.fixed]
+
+
+@pytest.mark.parametrize("gen,kw,n", [(synth.c1, {}, 5_000), (synth.c2, dict(noninternal=12, discrete=True), 2_000),
+                                      (synth.c3, {}, 200)])
+def test_epoch_mode_is_identical_to_fused_exact_on_synthetic_networks(gpu, gen, kw, n):
+    """The same identity on @logic-form networks, whose exact kernel keeps incremental unstable sets."""
+    model = mb.Model(*gen(**kw))
+    mod = gpu.compile(model)
+    a, b = mod.run(mode="exact", sample_count=n), mod.run(mode="epoch", sample_count=n)
+    ra, rb = a.raw(), b.raw()
+    for k in ("occ", "cnt", "h"):
+        assert np.array_equal(ra[k], rb[k]), k
+    assert np.array_equal(a.final_counts, b.final_counts)
+    assert a.transitions == b.transitions
+    assert [(s.tolist(), c) for s, c in a.fixed] == [(s.tolist(), c) for s, c in b.fixed]
+
+
+@pytest.mark.parametrize("name,traj_len", [("metastasis", 2), ("metastasis", 7), ("Montagud2022_Prostate_Cancer", 5)])
+def test_exact_mode_epoch_boundary_length(gpu, name, traj_len):
+    """The epoch boundary (every traj_len-1 steps the reference re-evaluates the current state with a
+    fresh draw) is part of the exact semantics; other lengths than the default must match too."""
+    bnd, cfg = model_text(name)
+    model = mb.Model(bnd, cfg)
+    mod = gpu.compile(model)
+    n = 1_000
+    res = mod.run(mode="exact", sample_count=n, traj_len=traj_len)
+    raw = res.raw()
+    o = OracleModel(bnd, cfg)
+    ref = o.run(n=n, mode=0, traj_len=traj_len, occ_exp=raw["occ_exp"], ent_exp=raw["ent_exp"])
+    _assert_same(res, raw, ref, o.discrete)
+    ep = mod.run(mode="epoch", sample_count=n, traj_len=traj_len)
+    assert np.array_equal(ep.final_counts, res.final_counts) and ep.transitions == res.transitions
 
 
 def test_epoch_refill_beyond_batch_limit(gpu):
