@@ -388,6 +388,24 @@ __device__ __forceinline__ void mb_incr_start(const mb_fused_params& P, const mb
 #ifndef MBG_INCREMENTAL
 extern "C" __global__ void __launch_bounds__(256) mb_fused_exact(mb_fused_params P) { mb_fused_body<true>(P); }
 #else
+// Running fp32 sum over the unstable nodes of state word w, in node order, starting from `run`
+// (adds of 0.f for the missing second node of a pair leave a non-negative sum unchanged).
+__device__ __forceinline__ float mb_exact_word_sum(float run, uint32_t um, uint32_t sw, int w)
+{
+	while (um)
+	{
+		const int b0 = __ffs(um) - 1;
+		um &= um - 1u;
+		const int b1 = __ffs(um) - 1;
+		um &= um - 1u;
+		const float r0 = __ldg(mbg_inc_rate + 2 * (32 * w + b0) + ((sw >> b0) & 1u));
+		const float r1 = b1 >= 0 ? __ldg(mbg_inc_rate + 2 * (32 * w + b1) + ((sw >> b1) & 1u)) : 0.f;
+		run += r0;
+		run += r1;
+	}
+	return run;
+}
+
 // Exact mode for models whose rates all have the @logic form. Bit-identical to the reference
 // algorithm (XORWOW streams, draw order, fp32 operation order, epoch boundary), but without
 // evaluating all N rate functions per step: a stable node's rate is exactly 0 and x + 0.0f == x,
@@ -395,7 +413,11 @@ extern "C" __global__ void __launch_bounds__(256) mb_fused_exact(mb_fused_params
 // nodes in node order, and its prefix-count flip selection always stops at an unstable node
 // (simulation.cu:9-21: the first prefix sum reaching r belongs to a node with a non-zero rate).
 // Unstable masks are kept incrementally as in the fast kernel; rates are the float values of the
-// generated code (mbg_inc_rate).
+// generated code (mbg_inc_rate). The running sum at the end of every state word is kept in shared
+// memory: after a flip only the words from the lowest changed one are re-summed (the running sum
+// up to an unchanged prefix is the same fp32 value), and the flip is found by a binary search over
+// the word-end sums (non-decreasing, all rates being >= 0) and a scan of one word from the
+// previous word-end sum, which reproduces the reference's running comparisons exactly.
 extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params P)
 {
 	extern __shared__ uint32_t mb_smem_u32[];
@@ -405,9 +427,9 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 	v.stride = B;
 	v.st = mb_smem_u32 + threadIdx.x;
 	v.un = mb_smem_u32 + (size_t)state_words * B + threadIdx.x;
-	v.ws = v.un; // word sums are not used in exact mode
+	v.ws = mb_smem_u32 + (size_t)2 * state_words * B + threadIdx.x; // word-end running sums (float bits)
 	long long* hsink = P.st.win_h;
-	long long* smem_h = reinterpret_cast<long long*>(mb_smem_u32 + (size_t)2 * state_words * B);
+	long long* smem_h = reinterpret_cast<long long*>(mb_smem_u32 + (size_t)3 * state_words * B);
 	if (P.st.h_in_smem)
 	{
 		for (int i = threadIdx.x; i < P.st.n_windows; i += B)
@@ -423,6 +445,7 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 	uint32_t idx = 0;
 	float time = 0.f;
 	int slot = 1;
+	int lo = 0; // lowest state word changed since the word-end sums were computed
 	curandState rng;
 
 	while (__any_sync(0xffffffffu, working || running))
@@ -488,6 +511,7 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 		{
 			time = 0.f;
 			slot = 1;
+			lo = 0;
 			running = true;
 		}
 
@@ -495,17 +519,13 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 		if (running)
 		{
 			// compute_transition_rates: sequential fp32 sum over the unstable nodes in node order
-			for (int w = 0; w < state_words; w++)
+			total = lo > 0 ? __uint_as_float(v.Q(lo - 1)) : 0.f;
+			for (int w = lo; w < state_words; w++)
 			{
-				uint32_t um = v.U(w);
-				const uint32_t sw = v.S(w);
-				while (um)
-				{
-					const int b = __ffs(um) - 1;
-					um &= um - 1u;
-					total += __ldg(mbg_inc_rate + 2 * (32 * w + b) + ((sw >> b) & 1u));
-				}
+				total = mb_exact_word_sum(total, v.U(w), v.S(w), w);
+				v.Q(w) = __float_as_uint(total);
 			}
+			lo = state_words;
 			if (isinf(total))
 			{
 				// an infinite total rate gives zero waiting times forever: stop this trajectory
@@ -578,32 +598,35 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 				slot = 1; // epoch boundary: the next epoch re-evaluates the same state
 			else
 			{
-				// select_flip_bit: the first node whose running fp32 sum reaches r
+				// select_flip_bit: the first node whose running fp32 sum reaches r; its word is the
+				// first whose word-end sum reaches r (total = last word-end sum >= r)
 				const float r = curand_uniform(&rng) * total;
-				float sum = 0.f;
-				int j = -1, last = -1;
-				for (int w = 0; w < state_words && j < 0; w++)
+				int wl = 0, wh = state_words - 1;
+				while (wl < wh)
 				{
-					uint32_t um = v.U(w);
-					const uint32_t sw = v.S(w);
-					while (um)
-					{
-						const int b = __ffs(um) - 1;
-						um &= um - 1u;
-						last = 32 * w + b;
-						sum += __ldg(mbg_inc_rate + 2 * last + ((sw >> b) & 1u));
-						if (!(sum < r))
-						{
-							j = last;
-							break;
-						}
-					}
+					const int mid = (wl + wh) >> 1;
+					if (__uint_as_float(v.Q(mid)) < r)
+						wl = mid + 1;
+					else
+						wh = mid;
 				}
-				if (j < 0)
-					j = last; // unreachable: the last prefix sum equals total >= r
+				float sum = wl > 0 ? __uint_as_float(v.Q(wl - 1)) : 0.f;
+				uint32_t um = v.U(wl);
+				const uint32_t sw = v.S(wl);
+				int j = -1;
+				while (um)
+				{
+					const int b = __ffs(um) - 1;
+					um &= um - 1u;
+					j = 32 * wl + b;
+					sum += __ldg(mbg_inc_rate + 2 * j + ((sw >> b) & 1u));
+					if (!(sum < r))
+						break;
+				}
 
 				// flip j and re-evaluate it and the nodes whose logic reads it
 				v.S(j >> 5) ^= 1u << (j & 31);
+				lo = j >> 5;
 				const uint4 nj = __ldg(mbg_inc_node + j);
 				const int pj = (int)(nj.w >> 16) - 1;
 				if (pj >= 0)
@@ -618,7 +641,10 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 					const bool unstable = on != mb_incr_logic(v, d, hdr, __ldg(mbg_inc_rec_in + d));
 					const uint32_t uw = v.U(k >> 5);
 					if (unstable != ((uw & bk) != 0))
+					{
 						v.U(k >> 5) = uw ^ bk;
+						lo = min(lo, k >> 5);
+					}
 				}
 			}
 		}

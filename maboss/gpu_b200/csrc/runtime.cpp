@@ -609,8 +609,8 @@ void launch_fused(module& m, const run_config& c, stats_state& st, long long n, 
 	size_t smem = st.h_smem();
 	if (m.incremental)
 	{
-		// per thread in shared memory: state words and unstable masks (+ word rate sums in fast mode)
-		const size_t per_word = c.mode == MB_MODE_FUSED_FAST ? 12 : 8;
+		// per thread in shared memory: state words, unstable masks and word rate sums
+		const size_t per_word = 12;
 		constexpr size_t max_smem = 227 * 1024;
 		block = std::min(block, 128);
 		while (block > 32 && per_word * m.state_words * block + smem > max_smem)
