@@ -85,6 +85,9 @@ mb_status mb_model_get_variable(mb_model m, const char* name, float* value);
 mb_status mb_model_set_variable(mb_model m, const char* name, float value);
 mb_status mb_model_num_variables(mb_model m, int* n);
 mb_status mb_model_variable_name(mb_model m, int i, char* buf, size_t cap, size_t* len);
+/* Names of driver::constants in map order (the defaults of src/parser/driver.cpp:7-14 included). */
+mb_status mb_model_num_constants(mb_model m, int* n);
+mb_status mb_model_constant_name(mb_model m, int i, char* buf, size_t cap, size_t* len);
 
 /* generator::generate_code(), src/generator.cpp:11-55. Writes the generated CUDA source
  * (NUL-terminated, truncated to cap) and its full length. */
@@ -112,6 +115,18 @@ mb_status mb_module_state_size(mb_module mod, int* state_size, int* state_words)
 /* NVRTC log of the compilation (may be empty). */
 mb_status mb_module_log(mb_module mod, char* buf, size_t cap, size_t* len);
 
+/* Device memory and synchronisation on the context's device, so that host code above this ABI
+ * needs no CUDA runtime of its own (the reference allocates with thrust::device_malloc and copies
+ * with cudaMemcpy, src/simulation_runner.cu:65-98). mb_memcpy copies in any direction (host or
+ * device pointers) on `stream` and waits for it; mb_synchronize waits for all work on the device. */
+mb_status mb_device_malloc(mb_context c, size_t bytes, void** ptr);
+mb_status mb_device_free(mb_context c, void* ptr);
+mb_status mb_memcpy(mb_context c, void* stream, void* dst, const void* src, size_t bytes);
+mb_status mb_memset_async(mb_context c, void* stream, void* ptr, int value, size_t bytes);
+mb_status mb_synchronize(mb_context c);
+/* The context a module was compiled for. */
+mb_status mb_module_context(mb_module mod, mb_context* out);
+
 /* ------------------------------------------------------------------ kernel entry points (kernel_wrapper) */
 /* Size in bytes of one per-trajectory random state (curandState, XORWOW). */
 size_t mb_rand_state_size(void);
@@ -138,6 +153,18 @@ typedef struct mb_stats_s* mb_stats;
 mb_status mb_stats_create(mb_module mod, float time_tick, float max_time, int discrete_time,
                           const int* noninternal_nodes, int n_noninternal, long long sample_count,
                           mb_stats* out);
+/* The same with only some of the three accumulators (a bitwise OR of MB_STATS_*): one stats plugin
+ * of src/statistics/ each (window_average_small_stats, final_states_stats, fixed_states_stats)
+ * without the device memory of the other two. Launching the statistics of a missing section returns
+ * MB_ERR_INVALID. time_tick, max_time and the non-internal nodes are ignored without MB_STATS_WINDOWS
+ * and MB_STATS_FINAL (pass 1, 1 and none). */
+#define MB_STATS_WINDOWS 1u
+#define MB_STATS_FINAL 2u
+#define MB_STATS_FIXED 4u
+#define MB_STATS_ALL 7u
+mb_status mb_stats_create_sections(mb_module mod, float time_tick, float max_time, int discrete_time,
+                                   const int* noninternal_nodes, int n_noninternal, long long sample_count,
+                                   unsigned sections, mb_stats* out);
 mb_status mb_stats_free(mb_stats st);
 /* window_average_small{,_discrete}, src/jit_kernels/window_average_small.cu:50-136 */
 mb_status mb_launch_window_average_stats(mb_stats st, void* stream, int n, int stride, int traj_len,
@@ -151,6 +178,19 @@ mb_status mb_launch_fixed_states_stats(mb_stats st, void* stream, int n, int str
                                        const uint32_t* last_states, const uint8_t* statuses);
 /* stats::finalize (device -> host); the result is independent of the stats object. */
 mb_status mb_stats_finalize(mb_stats st, long long n_trajectories, mb_result* out);
+
+/* The epoch batch's partition, src/simulation_runner.cu:126-139 (thrust::stable_partition of
+ * last_states and thrust::partition of last_times and the random states by status == CONTINUE):
+ * copies the CONTINUE trajectories of [0, n), in their order, to the front of a second buffer set
+ * (out_states SoA [word * stride + j], out_times, out_rands; these must not overlap the inputs) and
+ * writes their number to the device word *kept. `scratch` is device memory of
+ * mb_partition_scratch_size(n) bytes. Finished slots are not carried over: new trajectories get
+ * fresh random states from mb_launch_initialize_random (the reference reuses a freed slot's state). */
+size_t mb_partition_scratch_size(int n);
+mb_status mb_launch_partition(mb_module mod, void* stream, int n, int stride, const uint8_t* statuses,
+                              const uint32_t* last_states, const float* last_times, const void* rands,
+                              uint32_t* out_states, float* out_times, void* out_rands, void* scratch,
+                              unsigned* kept);
 
 /* Fixed-point statistics for callers that cannot allocate device memory. No counterpart in the
  * reference. Same result as mb_launch_fixed_states_stats followed by mb_stats_finalize (the
@@ -194,6 +234,23 @@ mb_status mb_run_config_default(mb_model m, mb_run_config* cfg);
 /* simulation_runner(n, N, seed, initial_probs).run_simulation(...) with the three built-in stats
  * plugins (src/main.cpp:54-83). The module must come from mb_module_compile_model. */
 mb_status mb_run(mb_module mod, const mb_run_config* cfg, mb_result* out);
+
+/* The run constants of a module compiled from generated code alone (mb_module_compile), which
+ * the reference hands to simulation_runner (src/simulation_runner.h:17: sample count, seed,
+ * initial probabilities) and to the statistics plugins (src/main.cpp:65-74: time_tick, max_time,
+ * discrete_time, non-internal mask). */
+typedef struct mb_run_params_s
+{
+    float time_tick;
+    float max_time;
+    int discrete_time;
+    const float* initial_probs;    /* host, one per node */
+    int n_nodes;
+    const int* noninternal_nodes;  /* host, node indices in increasing order */
+    int n_noninternal;
+} mb_run_params;
+/* mb_run for a module from mb_module_compile: cfg->sample_count and cfg->seed are used as given. */
+mb_status mb_run_module(mb_module mod, const mb_run_config* cfg, const mb_run_params* params, mb_result* out);
 
 /* A run with device buffers allocated once (the reference allocates them per
  * simulation_runner::run_simulation, simulation_runner.cu:65-82). mb_runner_launch clears the
@@ -258,6 +315,17 @@ mb_status mb_result_fixed(mb_result r, int i, uint32_t* state_words, unsigned* c
  * src/main.cpp:85-99). Node names come from the model. */
 mb_status mb_result_write_csv(mb_result r, mb_model m, const char* prefix);
 mb_status mb_result_visualize(mb_result r, mb_model m, char* buf, size_t cap, size_t* len);
+/* One plugin's output with caller-given node names (stats::visualize / stats::write_csv of
+ * src/statistics/stats.h:26-27): section MB_SECTION_FINAL (visualize: "final points:"; csv: empty,
+ * as final_states.cpp:70 writes no file), MB_SECTION_FIXED (fixed_states.cu:127-187) or
+ * MB_SECTION_WINDOWS (window_average_small.cpp:142-250). */
+#define MB_SECTION_FINAL 0
+#define MB_SECTION_FIXED 1
+#define MB_SECTION_WINDOWS 2
+#define MB_FORMAT_VISUALIZE 0
+#define MB_FORMAT_CSV 1
+mb_status mb_result_format(mb_result r, int section, int format, const char* const* node_names, int n_names,
+                           char* buf, size_t cap, size_t* len);
 
 #ifdef __cplusplus
 }

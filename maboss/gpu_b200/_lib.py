@@ -45,7 +45,20 @@ def _declare(L: C.CDLL) -> None:
         "mb_model_set_variable": (i32, [vp, C.c_char_p, f32]),
         "mb_model_num_variables": (i32, [vp, P(i32)]),
         "mb_model_variable_name": (i32, [vp, i32, C.c_char_p, sz, P(sz)]),
+        "mb_model_num_constants": (i32, [vp, P(i32)]),
+        "mb_model_constant_name": (i32, [vp, i32, C.c_char_p, sz, P(sz)]),
         "mb_model_generate_code": (i32, [vp, C.c_char_p, sz, P(sz)]),
+        "mb_device_malloc": (i32, [vp, sz, P(vp)]),
+        "mb_device_free": (i32, [vp, vp]),
+        "mb_memcpy": (i32, [vp, vp, vp, vp, sz]),
+        "mb_memset_async": (i32, [vp, vp, vp, i32, sz]),
+        "mb_synchronize": (i32, [vp]),
+        "mb_module_context": (i32, [vp, P(vp)]),
+        "mb_stats_create_sections": (i32, [vp, f32, f32, i32, P(i32), i32, i64, C.c_uint, P(vp)]),
+        "mb_partition_scratch_size": (sz, [i32]),
+        "mb_launch_partition": (i32, [vp, vp, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+        "mb_run_module": (i32, [vp, vp, vp, P(vp)]),
+        "mb_result_format": (i32, [vp, i32, i32, P(C.c_char_p), i32, C.c_char_p, sz, P(sz)]),
         "mb_context_create": (i32, [i32, P(vp)]),
         "mb_context_free": (i32, [vp]),
         "mb_context_stream": (i32, [vp, P(vp)]),

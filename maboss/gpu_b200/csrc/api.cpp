@@ -26,6 +26,7 @@ struct mb_context_s
 struct mb_module_s
 {
 	std::unique_ptr<mb::module> mod;
+	mb_context ctx = nullptr;
 };
 struct mb_result_s
 {
@@ -242,6 +243,24 @@ mb_status mb_model_variable_name(mb_model m, int i, char* buf, size_t cap, size_
 	});
 }
 
+mb_status mb_model_num_constants(mb_model m, int* n)
+{
+	return guard([&] {
+		need(m && n, "null argument");
+		*n = (int)m->model.constants.size();
+	});
+}
+
+mb_status mb_model_constant_name(mb_model m, int i, char* buf, size_t cap, size_t* len)
+{
+	return guard([&] {
+		need(m && i >= 0 && i < (int)m->model.constants.size(), "bad constant index");
+		auto it = m->model.constants.begin();
+		std::advance(it, i);
+		copy_out(it->first, buf, cap, len);
+	});
+}
+
 mb_status mb_model_generate_code(mb_model m, char* buf, size_t cap, size_t* len)
 {
 	return guard([&] {
@@ -289,6 +308,7 @@ mb_status mb_module_compile(mb_context c, const char* code, mb_module* out)
 	return guard([&] {
 		need(c && code && out, "null argument");
 		auto m = std::make_unique<mb_module_s>();
+		m->ctx = c;
 		m->mod = mb::compile_module(*c->ctx, code);
 		*out = m.release();
 	});
@@ -299,6 +319,7 @@ mb_status mb_module_compile_model(mb_context c, mb_model model, mb_module* out)
 	return guard([&] {
 		need(c && model && out, "null argument");
 		auto m = std::make_unique<mb_module_s>();
+		m->ctx = c;
 		mb::model_layout L = mb::analyze_model(model->model);
 		m->mod = mb::compile_module(*c->ctx, mb::generate_code(model->model));
 		m->mod->layout = std::move(L);
@@ -347,6 +368,76 @@ mb_status mb_module_log(mb_module mod, char* buf, size_t cap, size_t* len)
 	return guard([&] {
 		need(mod, "null module");
 		copy_out(mod->mod->log, buf, cap, len);
+	});
+}
+
+mb_status mb_module_context(mb_module mod, mb_context* out)
+{
+	return guard([&] {
+		need(mod && out, "null argument");
+		*out = mod->ctx;
+	});
+}
+
+mb_status mb_device_malloc(mb_context c, size_t bytes, void** ptr)
+{
+	return guard([&] {
+		need(c && ptr, "null argument");
+		MB_CUDA(cudaSetDevice(c->ctx->device));
+		*ptr = nullptr;
+		if (bytes == 0)
+			return;
+		const cudaError_t e = cudaMalloc(ptr, bytes);
+		if (e == cudaErrorMemoryAllocation)
+		{
+			cudaGetLastError();
+			throw mb::engine_error(MB_ERR_LIMIT, "out of device memory (" + std::to_string(bytes) + " bytes)");
+		}
+		MB_CUDA(e);
+	});
+}
+
+mb_status mb_device_free(mb_context c, void* ptr)
+{
+	return guard([&] {
+		need(c, "null context");
+		if (!ptr)
+			return;
+		MB_CUDA(cudaSetDevice(c->ctx->device));
+		MB_CUDA(cudaFree(ptr));
+	});
+}
+
+mb_status mb_memcpy(mb_context c, void* stream, void* dst, const void* src, size_t bytes)
+{
+	return guard([&] {
+		need(c && (bytes == 0 || (dst && src)), "null argument");
+		if (bytes == 0)
+			return;
+		MB_CUDA(cudaSetDevice(c->ctx->device));
+		cudaStream_t s = stream_of(c->ctx.get(), stream);
+		MB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s));
+		MB_CUDA(cudaStreamSynchronize(s));
+	});
+}
+
+mb_status mb_memset_async(mb_context c, void* stream, void* ptr, int value, size_t bytes)
+{
+	return guard([&] {
+		need(c && (bytes == 0 || ptr), "null argument");
+		if (bytes == 0)
+			return;
+		MB_CUDA(cudaSetDevice(c->ctx->device));
+		MB_CUDA(cudaMemsetAsync(ptr, value, bytes, stream_of(c->ctx.get(), stream)));
+	});
+}
+
+mb_status mb_synchronize(mb_context c)
+{
+	return guard([&] {
+		need(c, "null context");
+		MB_CUDA(cudaSetDevice(c->ctx->device));
+		MB_CUDA(cudaDeviceSynchronize());
 	});
 }
 
@@ -407,8 +498,9 @@ mb_status mb_launch_simulate(mb_module mod, void* stream, int n, int stride, int
 	});
 }
 
-mb_status mb_stats_create(mb_module mod, float time_tick, float max_time, int discrete_time,
-						  const int* noninternal_nodes, int n_noninternal, long long sample_count, mb_stats* out)
+mb_status mb_stats_create_sections(mb_module mod, float time_tick, float max_time, int discrete_time,
+								   const int* noninternal_nodes, int n_noninternal, long long sample_count,
+								   unsigned sections, mb_stats* out)
 {
 	return guard([&] {
 		need(mod && out && n_noninternal >= 0 && (noninternal_nodes || n_noninternal == 0), "bad argument");
@@ -416,10 +508,17 @@ mb_status mb_stats_create(mb_module mod, float time_tick, float max_time, int di
 		MB_CUDA(cudaSetDevice(m.ctx->device));
 		auto s = std::make_unique<mb_stats_s>();
 		std::vector<int> ni(noninternal_nodes, noninternal_nodes + n_noninternal);
-		s->st.init(m, time_tick, max_time, discrete_time != 0, ni, sample_count, 0, m.ctx->stream);
+		s->st.init(m, time_tick, max_time, discrete_time != 0, ni, sample_count, 0, m.ctx->stream, sections);
 		MB_CUDA(cudaStreamSynchronize(m.ctx->stream));
 		*out = s.release();
 	});
+}
+
+mb_status mb_stats_create(mb_module mod, float time_tick, float max_time, int discrete_time,
+						  const int* noninternal_nodes, int n_noninternal, long long sample_count, mb_stats* out)
+{
+	return mb_stats_create_sections(mod, time_tick, max_time, discrete_time, noninternal_nodes, n_noninternal,
+									sample_count, MB_STATS_ALL, out);
 }
 
 mb_status mb_stats_free(mb_stats st)
@@ -478,6 +577,23 @@ mb_status mb_stats_finalize(mb_stats st, long long n_trajectories, mb_result* ou
 		auto r = std::make_unique<mb_result_s>();
 		r->res = st->st.finalize(n_trajectories, st->st.mod->ctx->stream);
 		*out = r.release();
+	});
+}
+
+size_t mb_partition_scratch_size(int n) { return mb::partition_scratch_bytes(n); }
+
+mb_status mb_launch_partition(mb_module mod, void* stream, int n, int stride, const uint8_t* statuses,
+							  const uint32_t* last_states, const float* last_times, const void* rands,
+							  uint32_t* out_states, float* out_times, void* out_rands, void* scratch, unsigned* kept)
+{
+	return guard([&] {
+		need(mod && n >= 0 && stride >= n && kept && scratch, "bad argument");
+		need(n == 0 || (statuses && last_states && last_times && rands && out_states && out_times && out_rands),
+			 "null buffer");
+		mb::module& m = *mod->mod;
+		MB_CUDA(cudaSetDevice(m.ctx->device));
+		mb::partition(m, stream_of(m.ctx, stream), n, stride, statuses, last_states, last_times, rands, out_states,
+					  out_times, out_rands, scratch, kept);
 	});
 }
 
@@ -558,6 +674,39 @@ mb_status mb_runner_free(mb_runner r)
 {
 	delete r;
 	return MB_OK;
+}
+
+mb_status mb_run_module(mb_module mod, const mb_run_config* cfg, const mb_run_params* params, mb_result* out)
+{
+	return guard([&] {
+		need(mod && cfg && params && out, "null argument");
+		const mb::module& m = *mod->mod;
+		need(params->n_nodes == m.state_size && params->initial_probs, "one initial probability per node is needed");
+		need(params->n_noninternal >= 0 && (params->noninternal_nodes || params->n_noninternal == 0),
+			 "bad non-internal nodes");
+		mb::run_config c;
+		c.mode = cfg->mode;
+		c.max_time = params->max_time;
+		c.time_tick = params->time_tick;
+		c.discrete_time = params->discrete_time != 0;
+		c.istate.assign(params->initial_probs, params->initial_probs + params->n_nodes);
+		c.noninternal_nodes.assign(params->noninternal_nodes, params->noninternal_nodes + params->n_noninternal);
+		for (size_t i = 0; i < c.noninternal_nodes.size(); i++)
+			need(c.noninternal_nodes[i] >= 0 && c.noninternal_nodes[i] < m.state_size &&
+					 (i == 0 || c.noninternal_nodes[i] > c.noninternal_nodes[i - 1]),
+				 "non-internal nodes must be increasing node indices");
+		c.sample_count = cfg->sample_count;
+		c.seed = cfg->seed;
+		c.first_traj = cfg->first_traj;
+		c.traj_len = cfg->traj_len > 0 ? cfg->traj_len : 100;
+		c.batch_limit = cfg->batch_limit > 0 ? cfg->batch_limit : 1000000;
+		c.block = cfg->block > 0 ? cfg->block : 256;
+		c.blocks_per_sm = cfg->blocks_per_sm;
+		c.fixed_capacity_log2 = cfg->fixed_capacity_log2;
+		auto r = std::make_unique<mb_result_s>();
+		r->res = mb::run(*mod->mod, c);
+		*out = r.release();
+	});
 }
 
 mb_status mb_run(mb_module mod, const mb_run_config* cfg, mb_result* out)
@@ -723,6 +872,7 @@ mb_status mb_result_window_probs(mb_result r, double* probs)
 	return guard([&] {
 		need(r && probs, "null argument");
 		const mb::result& x = *r->res;
+		need(x.sections & MB_STATS_WINDOWS, "the result has no window statistics");
 		for (int w = 0; w < x.n_windows; w++)
 			for (unsigned b = 0; b < x.n_bins; b++)
 				probs[(size_t)w * x.n_bins + b] = x.n_traj > 0 ? x.window_prob(w, b) : 0.0;
@@ -734,6 +884,7 @@ mb_status mb_result_window_entropy(mb_result r, double* th)
 	return guard([&] {
 		need(r && th, "null argument");
 		const mb::result& x = *r->res;
+		need(x.sections & MB_STATS_WINDOWS, "the result has no window statistics");
 		for (int w = 0; w < x.n_windows; w++)
 			th[w] = x.n_traj > 0 ? x.window_th(w) : 0.0;
 	});
@@ -762,6 +913,7 @@ mb_status mb_result_final_counts(mb_result r, unsigned* counts)
 {
 	return guard([&] {
 		need(r && counts, "null argument");
+		need(r->res->sections & MB_STATS_FINAL, "the result has no final-state statistics");
 		std::memcpy(counts, r->res->final_cnt.data(), r->res->final_cnt.size() * sizeof(unsigned));
 	});
 }
@@ -793,6 +945,7 @@ mb_status mb_result_write_csv(mb_result r, mb_model m, const char* prefix)
 {
 	return guard([&] {
 		need(r && m && prefix, "null argument");
+		need(r->res->sections == MB_STATS_ALL, "the result lacks some of the three statistics");
 		need((int)m->model.nodes.size() == r->res->state_size, "model does not match the result");
 		const auto names = names_of(m->model);
 		{
@@ -810,10 +963,44 @@ mb_status mb_result_write_csv(mb_result r, mb_model m, const char* prefix)
 	});
 }
 
+mb_status mb_result_format(mb_result r, int section, int format, const char* const* node_names, int n_names,
+						   char* buf, size_t cap, size_t* len)
+{
+	return guard([&] {
+		need(r && (node_names || n_names == 0), "null argument");
+		const mb::result& res = *r->res;
+		need(n_names == res.state_size, "one name per node is needed");
+		need(format == MB_FORMAT_VISUALIZE || format == MB_FORMAT_CSV, "unknown format");
+		std::vector<std::string> names(node_names, node_names + n_names);
+		std::string text;
+		switch (section)
+		{
+		case MB_SECTION_FINAL:
+			need(res.sections & MB_STATS_FINAL, "the result has no final-state statistics");
+			if (format == MB_FORMAT_VISUALIZE)
+				text = mb::format_final_visualize(res, names);
+			break;
+		case MB_SECTION_FIXED:
+			need(res.sections & MB_STATS_FIXED, "the result has no fixed-point statistics");
+			text = format == MB_FORMAT_VISUALIZE ? mb::format_fixed_visualize(res, names) : mb::format_fp_csv(res, names);
+			break;
+		case MB_SECTION_WINDOWS:
+			need(res.sections & MB_STATS_WINDOWS, "the result has no window statistics");
+			text = format == MB_FORMAT_VISUALIZE ? mb::format_windows_visualize(res, names)
+												 : mb::format_probtraj_csv(res, names);
+			break;
+		default:
+			need(false, "unknown section");
+		}
+		copy_out(text, buf, cap, len);
+	});
+}
+
 mb_status mb_result_visualize(mb_result r, mb_model m, char* buf, size_t cap, size_t* len)
 {
 	return guard([&] {
 		need(r && m, "null argument");
+		need(r->res->sections == MB_STATS_ALL, "the result lacks some of the three statistics");
 		need((int)m->model.nodes.size() == r->res->state_size, "model does not match the result");
 		copy_out(mb::format_visualize(*r->res, names_of(m->model)), buf, cap, len);
 	});

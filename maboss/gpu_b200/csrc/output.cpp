@@ -113,17 +113,36 @@ std::string format_fp_csv(const result& r, const std::vector<std::string>& names
 	return ofs.str();
 }
 
-std::string format_visualize(const result& r, const std::vector<std::string>& names)
+std::string format_final_visualize(const result& r, const std::vector<std::string>& names)
 {
 	std::ostringstream os;
 	os << "final points:" << std::endl;
-	for (unsigned b = 0; b < r.n_bins; b++)
+	for (unsigned b = 0; b < r.n_bins && b < r.final_cnt.size(); b++)
 		if (r.final_cnt[b] != 0)
 			os << (float)r.final_cnt[b] / (float)r.n_traj << " " << idx_name(r, names, b) << std::endl;
+	return os.str();
+}
+
+std::string format_fixed_visualize(const result& r, const std::vector<std::string>& names)
+{
+	std::ostringstream os;
 	os << "fixed points:" << std::endl;
 	for (size_t i = 0; i < r.fixed_counts.size(); i++)
 		os << (float)r.fixed_counts[i] / (float)r.n_traj << " "
 		   << state_name(names, r.fixed_states.data() + i * r.state_words, r.state_size) << std::endl;
+	return os.str();
+}
+
+std::string format_visualize(const result& r, const std::vector<std::string>& names)
+{
+	return format_final_visualize(r, names) + format_fixed_visualize(r, names) + format_windows_visualize(r, names);
+}
+
+std::string format_windows_visualize(const result& r, const std::vector<std::string>& names)
+{
+	std::ostringstream os;
+	if (!(r.sections & 1u))
+		return os.str();
 	for (int w = 0; w < r.n_windows; w++)
 	{
 		os << "window (" << (float)w * r.time_tick << ", " << (float)(w + 1) * r.time_tick << "]" << std::endl;

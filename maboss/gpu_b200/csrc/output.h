@@ -21,5 +21,9 @@ std::string format_fp_csv(const result& r, const std::vector<std::string>& names
 // stdout output of final_states_stats, fixed_states_stats and window_average_small_stats
 // visualize() in the order of src/main.cpp:65-74.
 std::string format_visualize(const result& r, const std::vector<std::string>& names);
+// The three parts of it: final_states.cpp:53-68, fixed_states.cu:127-152, window_average_small.cpp:142-179.
+std::string format_final_visualize(const result& r, const std::vector<std::string>& names);
+std::string format_fixed_visualize(const result& r, const std::vector<std::string>& names);
+std::string format_windows_visualize(const result& r, const std::vector<std::string>& names);
 
 } // namespace mb

@@ -370,12 +370,15 @@ double result::window_th(int w) const
 // ---------------------------------------------------------------- statistics state
 
 void stats_state::init(module& m, float tick, float tmax, bool discrete, const std::vector<int>& noninternal,
-					   long long n, int fixed_capacity_log2, cudaStream_t s)
+					   long long n, int fixed_capacity_log2, cudaStream_t s, unsigned secs)
 {
 	mod = &m;
+	if (secs == 0 || (secs & ~7u))
+		throw engine_error(MB_ERR_INVALID, "statistics sections must be a non-empty subset of MB_STATS_ALL");
+	sections = secs;
 	m.ensure_any();
 	const int k = (int)noninternal.size();
-	if (m.noninternal_count >= 0 && m.noninternal_count != k)
+	if ((secs & 3u) && m.noninternal_count >= 0 && m.noninternal_count != k)
 		throw engine_error(MB_ERR_INVALID, "the module was generated for " + std::to_string(m.noninternal_count) +
 											   " non-internal nodes, the statistics got " + std::to_string(k));
 	if (k > 20)
@@ -384,6 +387,8 @@ void stats_state::init(module& m, float tick, float tmax, bool discrete, const s
 	for (int i : noninternal)
 		if (i < 0 || i >= m.state_size)
 			throw engine_error(MB_ERR_INVALID, "non-internal node index out of range");
+	if (!(secs & 1u))
+		tick = tmax = 1.f; // no windows: one placeholder window
 	if (!(tick > 0.f) || !(tmax > 0.f))
 		throw engine_error(MB_ERR_INVALID, "max_time and time_tick must be positive");
 	const float q = tmax / tick;
@@ -401,29 +406,38 @@ void stats_state::init(module& m, float tick, float tmax, bool discrete, const s
 	h_in_smem = n_windows * sizeof(long long) <= 48 * 1024 ? 1 : 0;
 
 	const size_t cells = (size_t)n_windows * n_bins;
-	if (discrete)
+	if (sections & 1u)
 	{
-		cnt.alloc(cells * sizeof(unsigned));
-		MB_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes, s));
+		if (discrete)
+		{
+			cnt.alloc(cells * sizeof(unsigned));
+			MB_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes, s));
+		}
+		else
+		{
+			occ.alloc(cells * sizeof(long long));
+			MB_CUDA(cudaMemsetAsync(occ.p, 0, occ.bytes, s));
+		}
+		h.alloc(n_windows * sizeof(long long));
+		MB_CUDA(cudaMemsetAsync(h.p, 0, h.bytes, s));
 	}
-	else
+	if (sections & 2u)
 	{
-		occ.alloc(cells * sizeof(long long));
-		MB_CUDA(cudaMemsetAsync(occ.p, 0, occ.bytes, s));
+		fin.alloc(n_bins * sizeof(unsigned));
+		MB_CUDA(cudaMemsetAsync(fin.p, 0, fin.bytes, s));
 	}
-	h.alloc(n_windows * sizeof(long long));
-	MB_CUDA(cudaMemsetAsync(h.p, 0, h.bytes, s));
-	fin.alloc(n_bins * sizeof(unsigned));
-	MB_CUDA(cudaMemsetAsync(fin.p, 0, fin.bytes, s));
-
-	fp_cap = fixed_capacity_log2 > 0
-				 ? (1u << std::min(fixed_capacity_log2, 28))
-				 : next_pow2((unsigned long long)std::max(1024LL, std::min(std::max(n, 0LL), 1LL << 22) * 2));
-	fp_keys.alloc((size_t)fp_cap * sizeof(mb_key128));
-	fp_counts.alloc((size_t)fp_cap * sizeof(unsigned));
-	fp_states.alloc((size_t)fp_cap * m.state_words * sizeof(unsigned));
-	MB_CUDA(cudaMemsetAsync(fp_keys.p, 0, fp_keys.bytes, s));
-	MB_CUDA(cudaMemsetAsync(fp_counts.p, 0, fp_counts.bytes, s));
+	fp_cap = 0;
+	if (sections & 4u)
+	{
+		fp_cap = fixed_capacity_log2 > 0
+					 ? (1u << std::min(fixed_capacity_log2, 28))
+					 : next_pow2((unsigned long long)std::max(1024LL, std::min(std::max(n, 0LL), 1LL << 22) * 2));
+		fp_keys.alloc((size_t)fp_cap * sizeof(mb_key128));
+		fp_counts.alloc((size_t)fp_cap * sizeof(unsigned));
+		fp_states.alloc((size_t)fp_cap * m.state_words * sizeof(unsigned));
+		MB_CUDA(cudaMemsetAsync(fp_keys.p, 0, fp_keys.bytes, s));
+		MB_CUDA(cudaMemsetAsync(fp_counts.p, 0, fp_counts.bytes, s));
+	}
 	counters.alloc(64);
 	MB_CUDA(cudaMemsetAsync(counters.p, 0, 64, s));
 
@@ -441,21 +455,15 @@ void stats_state::init(module& m, float tick, float tmax, bool discrete, const s
 	p.fp_keys = fp_keys.as<mb_key128>();
 	p.fp_counts = fp_counts.as<unsigned>();
 	p.fp_states = fp_states.as<unsigned>();
-	p.fp_mask = fp_cap - 1;
+	p.fp_mask = fp_cap ? fp_cap - 1 : 0;
 	p.fp_overflow = fp_overflow_ctr();
 }
 
 void stats_state::zero(cudaStream_t s)
 {
-	if (occ.p)
-		MB_CUDA(cudaMemsetAsync(occ.p, 0, occ.bytes, s));
-	if (cnt.p)
-		MB_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes, s));
-	MB_CUDA(cudaMemsetAsync(h.p, 0, h.bytes, s));
-	MB_CUDA(cudaMemsetAsync(fin.p, 0, fin.bytes, s));
-	MB_CUDA(cudaMemsetAsync(fp_keys.p, 0, fp_keys.bytes, s));
-	MB_CUDA(cudaMemsetAsync(fp_counts.p, 0, fp_counts.bytes, s));
-	MB_CUDA(cudaMemsetAsync(counters.p, 0, counters.bytes, s));
+	for (dbuf* b : { &occ, &cnt, &h, &fin, &fp_keys, &fp_counts, &counters })
+		if (b->p)
+			MB_CUDA(cudaMemsetAsync(b->p, 0, b->bytes, s));
 }
 
 void stats_state::set_istate(const std::vector<float>& is, cudaStream_t s)
@@ -469,6 +477,8 @@ void stats_state::set_istate(const std::vector<float>& is, cudaStream_t s)
 void stats_state::window_batch(cudaStream_t s, int n, int stride, int traj_len, const unsigned* traj_states,
 							   const float* traj_times, const float* traj_h)
 {
+	if (!(sections & 1u))
+		throw engine_error(MB_ERR_INVALID, "these statistics were created without the window section");
 	if (n <= 0)
 		return;
 	mb_stats_params sp = p;
@@ -479,6 +489,8 @@ void stats_state::window_batch(cudaStream_t s, int n, int stride, int traj_len, 
 void stats_state::final_batch(cudaStream_t s, int n, int stride, const unsigned* last_states,
 							  const unsigned char* statuses)
 {
+	if (!(sections & 2u))
+		throw engine_error(MB_ERR_INVALID, "these statistics were created without the final-state section");
 	if (n <= 0)
 		return;
 	unsigned* fc = p.final_cnt;
@@ -489,6 +501,8 @@ void stats_state::final_batch(cudaStream_t s, int n, int stride, const unsigned*
 void stats_state::fixed_batch(cudaStream_t s, int n, int stride, const unsigned* last_states,
 							  const unsigned char* statuses)
 {
+	if (!(sections & 4u))
+		throw engine_error(MB_ERR_INVALID, "these statistics were created without the fixed-point section");
 	if (n <= 0)
 		return;
 	mb_stats_params sp = p;
@@ -512,27 +526,35 @@ std::unique_ptr<result> stats_state::finalize(long long n, cudaStream_t s)
 	r.noninternal_nodes = noninternal_nodes;
 	r.fx = fx;
 	r.fx_h = fx_h;
+	r.sections = sections;
 	const size_t cells = (size_t)n_windows * n_bins;
-	if (discrete_time)
+	if ((sections & 1u) && discrete_time)
 	{
 		r.win_cnt.resize(cells);
 		MB_CUDA(cudaMemcpyAsync(r.win_cnt.data(), cnt.p, cells * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
 	}
-	else
+	else if (sections & 1u)
 	{
 		r.win_occ.resize(cells);
 		MB_CUDA(cudaMemcpyAsync(r.win_occ.data(), occ.p, cells * sizeof(long long), cudaMemcpyDeviceToHost, s));
 	}
-	r.win_h.resize(n_windows);
-	MB_CUDA(cudaMemcpyAsync(r.win_h.data(), h.p, n_windows * sizeof(long long), cudaMemcpyDeviceToHost, s));
-	r.final_cnt.resize(n_bins);
-	MB_CUDA(cudaMemcpyAsync(r.final_cnt.data(), fin.p, n_bins * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+	if (sections & 1u)
+	{
+		r.win_h.resize(n_windows);
+		MB_CUDA(cudaMemcpyAsync(r.win_h.data(), h.p, n_windows * sizeof(long long), cudaMemcpyDeviceToHost, s));
+	}
+	if (sections & 2u)
+	{
+		r.final_cnt.resize(n_bins);
+		MB_CUDA(cudaMemcpyAsync(r.final_cnt.data(), fin.p, n_bins * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+	}
 
 	// count occupied fixed-point slots, then compact them on the device and copy the records
 	unsigned ctr[8];
 	MB_CUDA(cudaMemsetAsync(extract_ctr(), 0, sizeof(unsigned), s));
 	dbuf out_counts((size_t)fp_cap * sizeof(unsigned));
 	dbuf out_states((size_t)fp_cap * m.state_words * sizeof(unsigned));
+	if (fp_cap)
 	{
 		unsigned cap = fp_cap;
 		mb_key128* keys = p.fp_keys;
@@ -627,6 +649,42 @@ void launch_fused(module& m, const run_config& c, stats_state& st, long long n, 
 }
 
 // Buffered epochs (simulation_runner.cu:54-180): simulate -> stats -> partition -> refill.
+} // namespace
+
+size_t partition_scratch_bytes(int n)
+{
+	const size_t nb = (size_t)(std::max(n, 1) + 1023) / 1024;
+	return (2 * nb + 1) * sizeof(unsigned);
+}
+
+void partition(module& m, cudaStream_t s, int n, int stride, const unsigned char* statuses, const unsigned* states,
+			   const float* times, const void* rands, unsigned* out_states, float* out_times, void* out_rands,
+			   void* scratch, unsigned* kept)
+{
+	if (n < 0 || stride < n)
+		throw engine_error(MB_ERR_INVALID, "partition: need 0 <= n <= stride");
+	if (n > (1 << 30))
+		throw engine_error(MB_ERR_LIMIT, "partition: batch larger than 2^30 trajectories");
+	m.ensure_any();
+	if (n == 0)
+	{
+		MB_CUDA(cudaMemsetAsync(kept, 0, sizeof(unsigned), s));
+		return;
+	}
+	int nb = (n + 1023) / 1024;
+	unsigned* bcp = static_cast<unsigned*>(scratch);
+	unsigned* bop = bcp + nb;
+	void* a1[] = { &n, &statuses, &bcp };
+	launch(m.compact_count, nb, 1024, 0, s, a1);
+	void* a2[] = { &nb, &bcp, &bop };
+	launch(m.compact_scan, 1, 1024, 0, s, a2);
+	void* a3[] = { &n, &stride, &statuses, &bop, &states, &times, &rands, &out_states, &out_times, &out_rands };
+	launch(m.compact_scatter, nb, 1024, 0, s, a3);
+	MB_CUDA(cudaMemcpyAsync(kept, bop + nb, sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
+}
+
+namespace {
+
 void run_epochs(module& m, const run_config& c, stats_state& st, long long n, cudaStream_t s, int& epochs)
 {
 	const int W = m.state_words;
@@ -639,8 +697,7 @@ void run_epochs(module& m, const run_config& c, stats_state& st, long long n, cu
 	dbuf st0((size_t)W * B * 4), st1((size_t)W * B * 4), t0((size_t)B * 4), t1((size_t)B * 4);
 	dbuf r0((size_t)B * sizeof(curandState)), r1((size_t)B * sizeof(curandState));
 	dbuf ts((size_t)L * W * B * 4), tt((size_t)L * B * 4), th((size_t)L * B * 4), stat((size_t)B);
-	const int nblocks = (B + 1023) / 1024;
-	dbuf bc((size_t)nblocks * 4), bo((size_t)(nblocks + 1) * 4);
+	dbuf scratch(256 + partition_scratch_bytes(B));
 	unsigned long long* trans = st.transitions();
 	float* istate = st.istate.as<float>();
 
@@ -678,20 +735,11 @@ void run_epochs(module& m, const run_config& c, stats_state& st, long long n, cu
 		st.fixed_batch(s, in_batch, stride, ls, stp);
 		st.window_batch(s, in_batch, stride, len, tsp, ttp, thp);
 		// partition CONTINUE trajectories to the front of the other buffer set
-		int nb = (in_batch + 1023) / 1024;
-		unsigned* bcp = bc.as<unsigned>();
-		unsigned* bop = bo.as<unsigned>();
-		void* a1[] = { &in_batch, &stp, &bcp };
-		launch(m.compact_count, nb, 1024, 0, s, a1);
-		void* a2[] = { &nb, &bcp, &bop };
-		launch(m.compact_scan, 1, 1024, 0, s, a2);
-		unsigned* nsp = ns->as<unsigned>();
-		float* ntp = nt->as<float>();
-		void* nrp = nr->p;
-		void* a3[] = { &in_batch, &stride, &stp, &bop, &ls, &lt, &rr, &nsp, &ntp, &nrp };
-		launch(m.compact_scatter, nb, 1024, 0, s, a3);
+		unsigned* kept_dev = scratch.as<unsigned>();
+		partition(m, s, in_batch, stride, stp, ls, lt, rr, ns->as<unsigned>(), nt->as<float>(), nr->p,
+				  scratch.as<char>() + 256, kept_dev);
 		unsigned kept = 0;
-		MB_CUDA(cudaMemcpyAsync(&kept, bop + nb, sizeof kept, cudaMemcpyDeviceToHost, s));
+		MB_CUDA(cudaMemcpyAsync(&kept, kept_dev, sizeof kept, cudaMemcpyDeviceToHost, s));
 		MB_CUDA(cudaStreamSynchronize(s));
 		std::swap(cs, ns);
 		std::swap(ct, nt);

@@ -103,6 +103,14 @@ std::unique_ptr<module> compile_module(context& ctx, const std::string& generate
 std::vector<char> compile_cubin(const std::string& generated_code, std::string& log, int family = FAMILY_FAST);
 
 void launch(CUfunction f, unsigned grid, unsigned block, size_t smem, cudaStream_t s, void** args);
+
+// Stable partition of the CONTINUE trajectories of an epoch batch into another buffer set
+// (last_states SoA [word * stride + i], last_times, random states); the number kept is written to
+// the device word *kept. `scratch` holds partition_scratch_bytes(n) bytes.
+size_t partition_scratch_bytes(int n);
+void partition(module& m, cudaStream_t s, int n, int stride, const unsigned char* statuses, const unsigned* states,
+			   const float* times, const void* rands, unsigned* out_states, float* out_times, void* out_rands,
+			   void* scratch, unsigned* kept);
 int occupancy_blocks(CUfunction f, int block, size_t smem);
 
 struct run_config
@@ -141,6 +149,7 @@ struct result
 	std::vector<unsigned> fixed_counts;
 	unsigned fixed_overflow = 0;
 	unsigned rate_errors = 0; // trajectories stopped on a non-finite total rate
+	unsigned sections = 7;	  // statistics present: 1 windows, 2 final states, 4 fixed points
 	unsigned long long transitions = 0;
 	float kernel_ms = 0; // device time of the simulation kernels
 	float total_ms = 0;	 // device time of the whole run (setup + kernels + result copies)
@@ -168,10 +177,11 @@ struct stats_state
 	double fx = 1, fx_h = 1;
 	int h_in_smem = 0;
 	std::vector<int> noninternal_nodes;
-	mb_stats_params p{}; // device pointers + scales passed to the statistics kernels
+	unsigned sections = 7; // MB_STATS_WINDOWS | MB_STATS_FINAL | MB_STATS_FIXED
+	mb_stats_params p{};   // device pointers + scales passed to the statistics kernels
 
 	void init(module& m, float time_tick, float max_time, bool discrete, const std::vector<int>& noninternal,
-			  long long n_traj, int fixed_capacity_log2, cudaStream_t s);
+			  long long n_traj, int fixed_capacity_log2, cudaStream_t s, unsigned sections = 7);
 	void zero(cudaStream_t s); // clear every accumulator (asynchronous)
 	void set_istate(const std::vector<float>& istate, cudaStream_t s);
 	size_t h_smem() const { return h_in_smem ? (size_t)n_windows * sizeof(long long) : 0; }
