@@ -326,13 +326,20 @@ def run_ours(args) -> None:
     value = float(total_trans.item()) / float(local_time.item())
 
     # end to end through the public API: mb_run with host-side results (H2D of the initial
-    # probabilities, D2H of every statistic), each step synchronised on both sides
+    # probabilities, D2H of every statistic), each step synchronised on both sides; with several
+    # ranks each step is one job of n * world trajectories whose statistics are summed over the
+    # ranks (maboss.gpu_b200.distributed.sharded_run: one all-reduce + one all-gather)
+    from maboss.gpu_b200.distributed import sharded_run
     barrier()
     t = time.perf_counter()
     e2e_trans = 0
     for _ in range(args.steps):
-        res = mod.run(mode=args.mode, sample_count=n, first_traj=rank * n)
-        e2e_trans += res.transitions
+        if world > 1:
+            res = sharded_run(mod, mode=args.mode, sample_count=n * world)
+            e2e_trans += res.transitions / world  # the job's total, counted once over the ranks
+        else:
+            res = mod.run(mode=args.mode, sample_count=n)
+            e2e_trans += res.transitions
         probs = res.window_probs  # host copy of the result
     barrier()
     e2e_s = time.perf_counter() - t
@@ -384,7 +391,8 @@ def run_ours(args) -> None:
                    "nvrtc_compile_s": round(compile_s, 2)},
         "e2e": {"value": float(e2e_total.item()) / float(e2e_time.item()), "unit": "transitions/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "api": "mb_run (Module.run): allocation, H2D, kernel, D2H of all statistics"},
+                "api": "mb_run (Module.run): allocation, H2D, kernel, D2H of all statistics"
+                       + ("; statistics summed over the ranks (distributed.sharded_run)" if world > 1 else "")},
         "gpu_launches": runner.kernel_launches * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if peak else None, "traffic": traffic,

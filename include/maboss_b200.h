@@ -226,6 +226,9 @@ typedef struct mb_run_config_s
     int block;                     /* threads per block (multiple of 32, <= 256) */
     int blocks_per_sm;             /* 0 = occupancy calculator */
     int fixed_capacity_log2;       /* fixed-point table capacity, 0 = automatic */
+    long long stats_trajectories;  /* 0, or the trajectory count of the whole job when this run is one
+                                      shard of it: window sums then use the job's fixed-point scale,
+                                      so that mb_result_merge of the shards is exact */
 } mb_run_config;
 
 /* Defaults from the model's .cfg constants: mode FUSED_EXACT, traj_len 100, batch 1e6. */
@@ -298,6 +301,9 @@ mb_status mb_result_free(mb_result r);
 /* dims: windows, bins (2^k), non-internal count k, state words W, node count N */
 mb_status mb_result_dims(mb_result r, int* windows, int* bins, int* noninternal, int* state_words, int* nodes);
 mb_status mb_result_transitions(mb_result r, unsigned long long* transitions);
+/* Trajectory count, time constants and non-internal node indices ([k], may be NULL) of a result. */
+mb_status mb_result_info(mb_result r, long long* n_trajectories, int* discrete_time, float* time_tick,
+                         float* max_time, int* noninternal_nodes);
 /* kernel_ms: simulation + statistics kernels; total_ms: the whole run on the device */
 mb_status mb_result_timing(mb_result r, float* kernel_ms, float* total_ms, int* epochs);
 /* Window probabilities [windows * bins] (window_average_small.cpp:126-140) and TH [windows]. */
@@ -315,6 +321,39 @@ mb_status mb_result_fixed(mb_result r, int i, uint32_t* state_words, unsigned* c
  * src/main.cpp:85-99). Node names come from the model. */
 mb_status mb_result_write_csv(mb_result r, mb_model m, const char* prefix);
 mb_status mb_result_visualize(mb_result r, mb_model m, char* buf, size_t cap, size_t* len);
+/* A result from raw accumulators (for instance the per-rank sums of a sharded run after a
+ * collective). Window sums are fixed point: occupancy = time * 2^occupancy_exponent (continuous),
+ * entropy = sum of h * slice * 2^entropy_exponent (discrete: h * 2^entropy_exponent); the exponents
+ * are those mb_result_window_raw reports. Fixed points may come in any order and with repeats (their
+ * counts are summed). */
+typedef struct mb_result_desc_s
+{
+    int n_nodes;
+    int n_windows;
+    int discrete_time;
+    float time_tick;
+    float max_time;
+    const int* noninternal_nodes;  /* increasing node indices, at most 20 */
+    int n_noninternal;
+    long long n_trajectories;
+    int occupancy_exponent;
+    int entropy_exponent;
+    const long long* occupancy;    /* continuous: [n_windows * 2^k] */
+    const unsigned* counts;        /* discrete:   [n_windows * 2^k] */
+    const long long* entropy;      /* [n_windows] */
+    const unsigned* final_counts;  /* [2^k] */
+    int n_fixed;
+    const uint32_t* fixed_states;  /* [n_fixed * ceil(n_nodes / 32)] */
+    const unsigned* fixed_counts;  /* [n_fixed] */
+    unsigned long long transitions;
+} mb_result_desc;
+mb_status mb_result_create(const mb_result_desc* desc, mb_result* out);
+/* The statistics of the union of disjoint trajectory sets: the shards of one job, run with the
+ * same mb_run_config.stats_trajectories (the reference has one process per job; its final sum
+ * over shards would be simulation_runner's accumulation across batches). Integer sums, so the
+ * merge of shards [0, a) and [a, n) equals one run of [0, n) bit for bit. */
+mb_status mb_result_merge(const mb_result* parts, int n_parts, mb_result* out);
+
 /* One plugin's output with caller-given node names (stats::visualize / stats::write_csv of
  * src/statistics/stats.h:26-27): section MB_SECTION_FINAL (visualize: "final points:"; csv: empty,
  * as final_states.cpp:70 writes no file), MB_SECTION_FIXED (fixed_states.cu:127-187) or

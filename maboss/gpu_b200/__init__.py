@@ -5,7 +5,8 @@ thin ctypes binding over it. Nothing here computes trajectories: without the lib
 entry point raises.
 """
 from ._lib import EngineError, build, lib
-from .engine import Batch, Context, Model, Module, Result, RunConfig, Stats, gradient, rand_state_size
+from .engine import (Batch, Context, Model, Module, Result, RunConfig, Stats, gradient, merge_results,
+                     rand_state_size)
 
 __all__ = ["EngineError", "build", "lib", "Batch", "Context", "Model", "Module", "Result", "RunConfig", "Stats",
-           "gradient", "rand_state_size"]
+           "gradient", "merge_results", "rand_state_size"]

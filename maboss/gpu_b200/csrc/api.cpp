@@ -6,6 +6,7 @@
 
 #include <cstring>
 #include <fstream>
+#include <map>
 #include <memory>
 #include <string>
 
@@ -613,6 +614,7 @@ mb_status mb_run_config_default(mb_model m, mb_run_config* cfg)
 		c.block = 256;
 		c.blocks_per_sm = 0;
 		c.fixed_capacity_log2 = 0;
+		c.stats_trajectories = 0;
 		*cfg = c;
 	});
 }
@@ -630,6 +632,7 @@ mb::run_config to_config(mb_module mod, const mb_run_config* cfg)
 	c.block = cfg->block > 0 ? cfg->block : 256;
 	c.blocks_per_sm = cfg->blocks_per_sm;
 	c.fixed_capacity_log2 = cfg->fixed_capacity_log2;
+	c.stats_trajectories = cfg->stats_trajectories;
 	return c;
 }
 } // namespace
@@ -703,6 +706,7 @@ mb_status mb_run_module(mb_module mod, const mb_run_config* cfg, const mb_run_pa
 		c.block = cfg->block > 0 ? cfg->block : 256;
 		c.blocks_per_sm = cfg->blocks_per_sm;
 		c.fixed_capacity_log2 = cfg->fixed_capacity_log2;
+		c.stats_trajectories = cfg->stats_trajectories;
 		auto r = std::make_unique<mb_result_s>();
 		r->res = mb::run(*mod->mod, c);
 		*out = r.release();
@@ -960,6 +964,97 @@ mb_status mb_result_write_csv(mb_result r, mb_model m, const char* prefix)
 				throw mb::engine_error(MB_ERR_INVALID, std::string("cannot write ") + prefix + "_fp.csv");
 			f << mb::format_fp_csv(*r->res, names);
 		}
+	});
+}
+
+mb_status mb_result_info(mb_result r, long long* n_trajectories, int* discrete_time, float* time_tick,
+						 float* max_time, int* noninternal_nodes)
+{
+	return guard([&] {
+		need(r, "null result");
+		const mb::result& x = *r->res;
+		if (n_trajectories)
+			*n_trajectories = x.n_traj;
+		if (discrete_time)
+			*discrete_time = x.discrete_time ? 1 : 0;
+		if (time_tick)
+			*time_tick = x.time_tick;
+		if (max_time)
+			*max_time = x.max_time;
+		if (noninternal_nodes)
+			std::copy(x.noninternal_nodes.begin(), x.noninternal_nodes.end(), noninternal_nodes);
+	});
+}
+
+mb_status mb_result_create(const mb_result_desc* d, mb_result* out)
+{
+	return guard([&] {
+		need(d && out, "null argument");
+		need(d->n_nodes > 0 && d->n_windows > 0 && d->n_trajectories >= 0, "bad dimensions");
+		need(d->n_noninternal >= 0 && d->n_noninternal <= 20 && (d->noninternal_nodes || d->n_noninternal == 0),
+			 "at most 20 non-internal nodes");
+		need(d->time_tick > 0.f && d->max_time > 0.f, "max_time and time_tick must be positive");
+		need(d->occupancy_exponent >= 0 && d->occupancy_exponent <= 100 && d->entropy_exponent >= 0 &&
+				 d->entropy_exponent <= 100,
+			 "exponents must be in [0, 100]");
+		need(d->n_fixed >= 0 && (d->n_fixed == 0 || (d->fixed_states && d->fixed_counts)), "bad fixed points");
+		need(d->entropy && d->final_counts && (d->discrete_time ? d->counts != nullptr : d->occupancy != nullptr),
+			 "null accumulator");
+		auto r = std::make_unique<mb::result>();
+		r->state_size = d->n_nodes;
+		r->state_words = (d->n_nodes + 31) / 32;
+		r->n_windows = d->n_windows;
+		r->n_bins = 1u << d->n_noninternal;
+		r->n_traj = d->n_trajectories;
+		r->discrete_time = d->discrete_time != 0;
+		r->time_tick = d->time_tick;
+		r->max_time = d->max_time;
+		r->noninternal_nodes.assign(d->noninternal_nodes, d->noninternal_nodes + d->n_noninternal);
+		for (size_t i = 0; i < r->noninternal_nodes.size(); i++)
+			need(r->noninternal_nodes[i] >= 0 && r->noninternal_nodes[i] < d->n_nodes &&
+					 (i == 0 || r->noninternal_nodes[i] > r->noninternal_nodes[i - 1]),
+				 "non-internal nodes must be increasing node indices");
+		r->fx = std::ldexp(1.0, d->occupancy_exponent);
+		r->fx_h = std::ldexp(1.0, d->entropy_exponent);
+		const size_t cells = (size_t)d->n_windows * r->n_bins;
+		if (r->discrete_time)
+			r->win_cnt.assign(d->counts, d->counts + cells);
+		else
+			r->win_occ.assign(d->occupancy, d->occupancy + cells);
+		r->win_h.assign(d->entropy, d->entropy + d->n_windows);
+		r->final_cnt.assign(d->final_counts, d->final_counts + r->n_bins);
+		r->transitions = d->transitions;
+		std::map<std::vector<unsigned>, unsigned long long> fixed;
+		const int W = r->state_words;
+		for (int j = 0; j < d->n_fixed; j++)
+			fixed[std::vector<unsigned>(d->fixed_states + (size_t)j * W, d->fixed_states + (size_t)(j + 1) * W)] +=
+				d->fixed_counts[j];
+		std::vector<unsigned> st, cn;
+		for (auto& [state, count] : fixed)
+		{
+			st.insert(st.end(), state.begin(), state.end());
+			cn.push_back((unsigned)count);
+		}
+		mb::set_fixed_sorted(*r, st, cn);
+		auto h = std::make_unique<mb_result_s>();
+		h->res = std::move(r);
+		*out = h.release();
+	});
+}
+
+mb_status mb_result_merge(const mb_result* parts, int n_parts, mb_result* out)
+{
+	return guard([&] {
+		need(parts && n_parts > 0 && out, "bad argument");
+		std::vector<const mb::result*> rs;
+		for (int i = 0; i < n_parts; i++)
+		{
+			need(parts[i] && parts[i]->res, "null result");
+			rs.push_back(parts[i]->res.get());
+		}
+		auto h = std::make_unique<mb_result_s>();
+		h->res = mb::merge_results(rs);
+		*out = h.release();
 	});
 }
 

@@ -370,7 +370,7 @@ double result::window_th(int w) const
 // ---------------------------------------------------------------- statistics state
 
 void stats_state::init(module& m, float tick, float tmax, bool discrete, const std::vector<int>& noninternal,
-					   long long n, int fixed_capacity_log2, cudaStream_t s, unsigned secs)
+					   long long n, int fixed_capacity_log2, cudaStream_t s, unsigned secs, long long scale_traj)
 {
 	mod = &m;
 	if (secs == 0 || (secs & ~7u))
@@ -401,8 +401,9 @@ void stats_state::init(module& m, float tick, float tmax, bool discrete, const s
 	time_tick = tick;
 	max_time = tmax;
 	noninternal_nodes = noninternal;
-	fx = std::ldexp(1.0, occupancy_exponent(n, tick, discrete));
-	fx_h = std::ldexp(1.0, entropy_exponent(n, tick, discrete));
+	const long long n_scale = scale_traj > 0 ? scale_traj : n;
+	fx = std::ldexp(1.0, occupancy_exponent(n_scale, tick, discrete));
+	fx_h = std::ldexp(1.0, entropy_exponent(n_scale, tick, discrete));
 	h_in_smem = n_windows * sizeof(long long) <= 48 * 1024 ? 1 : 0;
 
 	const size_t cells = (size_t)n_windows * n_bins;
@@ -582,27 +583,94 @@ std::unique_ptr<result> stats_state::finalize(long long n, cudaStream_t s)
 		MB_CUDA(cudaMemcpyAsync(cn.data(), out_counts.p, cn.size() * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
 		MB_CUDA(cudaStreamSynchronize(s));
 	}
-	// order like std::map<static_state_t> (state.h:43-49: compare from the highest word down)
-	std::vector<unsigned> order(nfp);
-	std::iota(order.begin(), order.end(), 0u);
-	std::sort(order.begin(), order.end(), [&](unsigned a, unsigned b) {
+	set_fixed_sorted(r, st, cn);
+	return rp;
+}
+
+void set_fixed_sorted(result& r, const std::vector<unsigned>& st, const std::vector<unsigned>& cn)
+{
+	const int W = r.state_words;
+	const size_t nfp = cn.size();
+	std::vector<size_t> order(nfp);
+	std::iota(order.begin(), order.end(), size_t(0));
+	std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
 		for (int w = W - 1; w >= 0; w--)
 		{
-			unsigned x = st[(size_t)a * W + w], y = st[(size_t)b * W + w];
+			const unsigned x = st[a * W + w], y = st[b * W + w];
 			if (x != y)
 				return x < y;
 		}
 		return false;
 	});
-	r.fixed_states.resize((size_t)nfp * W);
+	r.fixed_states.resize(nfp * W);
 	r.fixed_counts.resize(nfp);
-	for (unsigned i = 0; i < nfp; i++)
+	for (size_t i = 0; i < nfp; i++)
 	{
-		std::copy(st.begin() + (size_t)order[i] * W, st.begin() + (size_t)(order[i] + 1) * W,
-				  r.fixed_states.begin() + (size_t)i * W);
+		std::copy(st.begin() + order[i] * W, st.begin() + (order[i] + 1) * W, r.fixed_states.begin() + i * W);
 		r.fixed_counts[i] = cn[order[i]];
 	}
-	return rp;
+}
+
+std::unique_ptr<result> merge_results(const std::vector<const result*>& parts)
+{
+	if (parts.empty())
+		throw engine_error(MB_ERR_INVALID, "merge: no results");
+	const result& a = *parts[0];
+	auto out = std::make_unique<result>();
+	result& r = *out;
+	r.state_size = a.state_size;
+	r.state_words = a.state_words;
+	r.n_windows = a.n_windows;
+	r.n_bins = a.n_bins;
+	r.discrete_time = a.discrete_time;
+	r.time_tick = a.time_tick;
+	r.max_time = a.max_time;
+	r.noninternal_nodes = a.noninternal_nodes;
+	r.fx = a.fx;
+	r.fx_h = a.fx_h;
+	r.sections = a.sections;
+	r.win_occ.assign(a.win_occ.size(), 0);
+	r.win_cnt.assign(a.win_cnt.size(), 0);
+	r.win_h.assign(a.win_h.size(), 0);
+	r.final_cnt.assign(a.final_cnt.size(), 0);
+	std::map<std::vector<unsigned>, unsigned long long> fixed;
+	for (const result* p : parts)
+	{
+		const result& b = *p;
+		if (b.state_size != a.state_size || b.n_windows != a.n_windows || b.n_bins != a.n_bins ||
+			b.discrete_time != a.discrete_time || b.time_tick != a.time_tick || b.max_time != a.max_time ||
+			b.noninternal_nodes != a.noninternal_nodes || b.sections != a.sections)
+			throw engine_error(MB_ERR_INVALID, "merge: the results are not shards of the same run");
+		if (b.fx != a.fx || b.fx_h != a.fx_h)
+			throw engine_error(MB_ERR_INVALID, "merge: different fixed-point scales (run every shard with the same "
+											   "stats_trajectories)");
+		r.n_traj += b.n_traj;
+		for (size_t i = 0; i < r.win_occ.size(); i++)
+			r.win_occ[i] += b.win_occ[i];
+		for (size_t i = 0; i < r.win_cnt.size(); i++)
+			r.win_cnt[i] += b.win_cnt[i];
+		for (size_t i = 0; i < r.win_h.size(); i++)
+			r.win_h[i] += b.win_h[i];
+		for (size_t i = 0; i < r.final_cnt.size(); i++)
+			r.final_cnt[i] += b.final_cnt[i];
+		for (size_t j = 0; j < b.fixed_counts.size(); j++)
+			fixed[std::vector<unsigned>(b.fixed_states.begin() + j * b.state_words,
+										b.fixed_states.begin() + (j + 1) * b.state_words)] += b.fixed_counts[j];
+		r.fixed_overflow += b.fixed_overflow;
+		r.rate_errors += b.rate_errors;
+		r.transitions += b.transitions;
+		r.kernel_ms = std::max(r.kernel_ms, b.kernel_ms);
+		r.total_ms = std::max(r.total_ms, b.total_ms);
+		r.epochs = std::max(r.epochs, b.epochs);
+	}
+	std::vector<unsigned> st, cn;
+	for (auto& [state, count] : fixed)
+	{
+		st.insert(st.end(), state.begin(), state.end());
+		cn.push_back((unsigned)count);
+	}
+	set_fixed_sorted(r, st, cn);
+	return out;
 }
 
 // ---------------------------------------------------------------- run drivers
@@ -767,7 +835,10 @@ runner::runner(module& m, const run_config& c) : mod(&m), cfg(c)
 	if (c.mode != MB_MODE_EPOCH && c.mode != MB_MODE_FUSED_EXACT && c.mode != MB_MODE_FUSED_FAST)
 		throw engine_error(MB_ERR_INVALID, "unknown run mode");
 	cudaStream_t s = m.ctx->stream;
-	st.init(m, c.time_tick, c.max_time, c.discrete_time, c.noninternal_nodes, c.sample_count, c.fixed_capacity_log2, s);
+	if (c.stats_trajectories < 0 || (c.stats_trajectories > 0 && c.stats_trajectories < c.sample_count))
+		throw engine_error(MB_ERR_INVALID, "stats_trajectories must be 0 or at least sample_count");
+	st.init(m, c.time_tick, c.max_time, c.discrete_time, c.noninternal_nodes, c.sample_count, c.fixed_capacity_log2, s,
+			7u, c.stats_trajectories);
 	st.set_istate(c.istate, s);
 	MB_CUDA(cudaEventCreate(&ev0));
 	MB_CUDA(cudaEventCreate(&ev1));

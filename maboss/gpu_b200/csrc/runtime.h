@@ -128,6 +128,7 @@ struct run_config
 	int block = 256;
 	int blocks_per_sm = 0;			 // 0 = occupancy calculator
 	int fixed_capacity_log2 = 0;	 // 0 = automatic
+	long long stats_trajectories = 0; // trajectory count the fixed-point scales are chosen for (0 = sample_count)
 };
 
 run_config config_from_layout(const model_layout& L, int mode);
@@ -159,6 +160,14 @@ struct result
 	double window_th(int w) const;				   // TH column (window_average_small.cpp:222-223)
 };
 
+// Fixed points stored in the order of std::map<static_state_t> (state.h:43-49: compared from the
+// highest word down), from `counts.size()` records of r.state_words words.
+void set_fixed_sorted(result& r, const std::vector<unsigned>& states, const std::vector<unsigned>& counts);
+// The statistics of the union of disjoint trajectory sets (shards of one run): integer sums of the
+// accumulators and the union of the fixed points. The parts must share the model's dimensions, the
+// windows and the fixed-point scales (runs with the same stats_trajectories).
+std::unique_ptr<result> merge_results(const std::vector<const result*>& parts);
+
 // Fixed-point exponents (shared with the oracle so that both convert slices identically).
 int occupancy_exponent(long long n_traj, float tick, bool discrete);
 int entropy_exponent(long long n_traj, float tick, bool discrete);
@@ -181,7 +190,8 @@ struct stats_state
 	mb_stats_params p{};   // device pointers + scales passed to the statistics kernels
 
 	void init(module& m, float time_tick, float max_time, bool discrete, const std::vector<int>& noninternal,
-			  long long n_traj, int fixed_capacity_log2, cudaStream_t s, unsigned sections = 7);
+			  long long n_traj, int fixed_capacity_log2, cudaStream_t s, unsigned sections = 7,
+			  long long scale_traj = 0); // scale_traj: trajectories the fixed-point scales are chosen for (0 = n_traj)
 	void zero(cudaStream_t s); // clear every accumulator (asynchronous)
 	void set_istate(const std::vector<float>& istate, cudaStream_t s);
 	size_t h_smem() const { return h_in_smem ? (size_t)n_windows * sizeof(long long) : 0; }

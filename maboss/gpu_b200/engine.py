@@ -24,6 +24,32 @@ class RunConfig(C.Structure):
         ("block", C.c_int),
         ("blocks_per_sm", C.c_int),
         ("fixed_capacity_log2", C.c_int),
+        ("stats_trajectories", C.c_longlong),
+    ]
+
+
+class ResultDesc(C.Structure):
+    """mb_result_desc (include/maboss_b200.h)."""
+
+    _fields_ = [
+        ("n_nodes", C.c_int),
+        ("n_windows", C.c_int),
+        ("discrete_time", C.c_int),
+        ("time_tick", C.c_float),
+        ("max_time", C.c_float),
+        ("noninternal_nodes", C.c_void_p),
+        ("n_noninternal", C.c_int),
+        ("n_trajectories", C.c_longlong),
+        ("occupancy_exponent", C.c_int),
+        ("entropy_exponent", C.c_int),
+        ("occupancy", C.c_void_p),
+        ("counts", C.c_void_p),
+        ("entropy", C.c_void_p),
+        ("final_counts", C.c_void_p),
+        ("n_fixed", C.c_int),
+        ("fixed_states", C.c_void_p),
+        ("fixed_counts", C.c_void_p),
+        ("transitions", C.c_ulonglong),
     ]
 
 
@@ -158,7 +184,7 @@ class Module:
 
     def config(self, mode: str = "exact", sample_count: int | None = None, seed: int | None = None,
                first_traj: int = 0, traj_len: int = 100, batch_limit: int = 1_000_000, block: int = 256,
-               blocks_per_sm: int = 0, fixed_capacity_log2: int = 0) -> RunConfig:
+               blocks_per_sm: int = 0, fixed_capacity_log2: int = 0, stats_trajectories: int = 0) -> RunConfig:
         cfg = RunConfig()
         check(lib().mb_run_config_default(self.model._h, C.byref(cfg)))
         cfg.mode = MODES[mode]
@@ -172,6 +198,7 @@ class Module:
         cfg.block = block
         cfg.blocks_per_sm = blocks_per_sm
         cfg.fixed_capacity_log2 = fixed_capacity_log2
+        cfg.stats_trajectories = stats_trajectories
         return cfg
 
     def run(self, mode: str = "exact", sample_count: int | None = None, **kw) -> "Result":
@@ -299,6 +326,14 @@ def gradient(ctx: Context, model: Model, params: dict[str, float], cotangent: np
     return grad[:k], Result(h)
 
 
+def merge_results(results: list["Result"]) -> "Result":
+    """mb_result_merge: the statistics of the union of disjoint trajectory shards of one job."""
+    hs = (C.c_void_p * len(results))(*[r._h for r in results])
+    out = C.c_void_p()
+    check(lib().mb_result_merge(hs, len(results), C.byref(out)))
+    return Result(out)
+
+
 def rand_state_size() -> int:
     return int(lib().mb_rand_state_size())
 
@@ -413,6 +448,54 @@ class Result:
             check(lib().mb_result_fixed(self._h, i, st.ctypes.data, C.byref(c)))
             out.append((st, c.value))
         return out
+
+    def info(self) -> dict:
+        """mb_result_info: trajectory count, time constants and non-internal nodes."""
+        n, d, t, m = C.c_longlong(), C.c_int(), C.c_float(), C.c_float()
+        ni = np.zeros(max(1, self.dims.noninternal), np.int32)
+        check(lib().mb_result_info(self._h, C.byref(n), C.byref(d), C.byref(t), C.byref(m), ni.ctypes.data))
+        return dict(n_trajectories=n.value, discrete=bool(d.value), time_tick=t.value, max_time=m.value,
+                    noninternal=[int(x) for x in ni[: self.dims.noninternal]])
+
+    @classmethod
+    def from_raw(cls, *, n_nodes: int, n_windows: int, discrete: bool, time_tick: float, max_time: float,
+                 noninternal: list[int], n_trajectories: int, occ_exp: int, ent_exp: int, occ=None, cnt=None,
+                 h=None, final=None, fixed_states=None, fixed_counts=None, transitions: int = 0) -> "Result":
+        """mb_result_create: a result from raw accumulators (window sums in fixed point)."""
+        S = 1 << len(noninternal)
+        keep = []
+
+        def arr(a, dtype, size):
+            x = np.ascontiguousarray(np.asarray(a, dtype).reshape(-1))
+            if x.size != size:
+                raise ValueError(f"expected {size} values, got {x.size}")
+            keep.append(x)
+            return x.ctypes.data
+
+        words = (n_nodes + 31) // 32
+        fs = np.zeros((0, words), np.uint32) if fixed_states is None else np.asarray(fixed_states, np.uint32)
+        fc = np.zeros(0, np.uint32) if fixed_counts is None else np.asarray(fixed_counts, np.uint32)
+        d = ResultDesc()
+        d.n_nodes, d.n_windows, d.discrete_time = n_nodes, n_windows, 1 if discrete else 0
+        d.time_tick, d.max_time = time_tick, max_time
+        d.noninternal_nodes = arr(noninternal, np.int32, len(noninternal)) if noninternal else None
+        d.n_noninternal = len(noninternal)
+        d.n_trajectories = n_trajectories
+        d.occupancy_exponent, d.entropy_exponent = occ_exp, ent_exp
+        if discrete:
+            d.counts = arr(cnt, np.uint32, n_windows * S)
+        else:
+            d.occupancy = arr(occ, np.int64, n_windows * S)
+        d.entropy = arr(h, np.int64, n_windows)
+        d.final_counts = arr(final, np.uint32, S)
+        d.n_fixed = len(fc)
+        if len(fc):
+            d.fixed_states = arr(fs, np.uint32, len(fc) * words)
+            d.fixed_counts = arr(fc, np.uint32, len(fc))
+        d.transitions = transitions
+        h_out = C.c_void_p()
+        check(lib().mb_result_create(C.byref(d), C.byref(h_out)))
+        return cls(h_out)
 
     def write_csv(self, model: Model, prefix: str) -> None:
         check(lib().mb_result_write_csv(self._h, model._h, prefix.encode()))
