@@ -6,7 +6,7 @@ window, final-state and fixed-point statistics). Default workload: the 1000-node
 (32 state words, 10 non-internal nodes, 1e6 trajectories, max_time 50, tick 0.5).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c3]
-                  [--mode fast|exact|epoch]
+                  [--mode fast|exact|epoch|epoch_dense]
 
 Multi-GPU (torchrun, one process per GPU): every rank simulates its own block of trajectories
 (random streams first_traj = rank * n), no collective on the data path (weak scaling); the step
@@ -414,7 +414,7 @@ def main() -> None:
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(EXTRA_WORKLOADS), default="c3")
-    p.add_argument("--mode", choices=["fast", "exact", "epoch"], default="fast")
+    p.add_argument("--mode", choices=["fast", "exact", "epoch", "epoch_dense"], default="fast")
     p.add_argument("--samples", type=int, default=None, help="trajectories per GPU (default: the workload's)")
     p.add_argument("--cpu-sample", type=int, default=2000, help="trajectories of the CPU baseline sample")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")

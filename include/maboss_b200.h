@@ -53,6 +53,8 @@ typedef struct mb_result_s* mb_result;   /* statistics of one run   (reference: 
 #define MB_MODE_FUSED_EXACT 0 /* persistent kernel; bit-exact trajectories with the reference CUDA build */
 #define MB_MODE_FUSED_FAST 1  /* persistent kernel; Philox streams; statistically equivalent */
 #define MB_MODE_EPOCH 2       /* buffered 100-slot epochs through SoA trajectory buffers */
+#define MB_MODE_EPOCH_DENSE 3 /* the same with the reference's per-step evaluation of every node's rate
+                                 function (for comparisons with the reference algorithm; same results) */
 
 /* Trajectory status byte (src/trajectory_status.h:3-8). */
 #define MB_STATUS_CONTINUE 0
@@ -139,7 +141,9 @@ mb_status mb_launch_initialize_initial_state(mb_module mod, void* stream, int n,
                                              const float* initial_probs, uint32_t* last_states,
                                              float* last_times, void* rands);
 /* simulate, src/generator.cpp:189-203 + src/jit_kernels/simulation.cu:77-164 (SoA buffers,
- * `traj_len` slots per epoch); adds the number of recorded steps to *transitions (device u64). */
+ * `traj_len` slots per epoch); adds the number of recorded steps to *transitions (device u64).
+ * For models whose rates all have the @logic form the kernel keeps incremental unstable sets instead
+ * of evaluating every rate function per step; trajectories are the same. */
 mb_status mb_launch_simulate(mb_module mod, void* stream, int n, int stride, int traj_len,
                              uint32_t* last_states, float* last_times, void* rands,
                              uint32_t* traj_states, float* traj_times, float* traj_entropies,
@@ -263,7 +267,7 @@ typedef struct mb_runner_s* mb_runner;
 mb_status mb_runner_create(mb_module mod, const mb_run_config* cfg, mb_runner* out);
 mb_status mb_runner_launch(mb_runner r, void* stream);
 mb_status mb_runner_result(mb_runner r, void* stream, mb_result* out);
-/* number of engine kernels one mb_runner_launch enqueues (fused modes) */
+/* number of engine kernels the last mb_runner_launch enqueued */
 mb_status mb_runner_kernel_launches(mb_runner r, unsigned* n);
 mb_status mb_runner_free(mb_runner r);
 

@@ -492,10 +492,8 @@ mb_status mb_launch_simulate(mb_module mod, void* stream, int n, int stride, int
 			 "null buffer");
 		mb::module& m = *mod->mod;
 		MB_CUDA(cudaSetDevice(m.ctx->device));
-		m.ensure(mb::FAMILY_EPOCH);
-		void* a[] = { &n,		   &stride,		 &traj_len,		  &last_states, &last_times,  &rands,
-					  &traj_states, &traj_times, &traj_entropies, &statuses,	&transitions };
-		mb::launch(m.sim_epoch, (n + 255) / 256, 256, 0, stream_of(m.ctx, stream), a);
+		mb::simulate_epoch(m, false, stream_of(m.ctx, stream), n, stride, traj_len, last_states, last_times, rands,
+						   traj_states, traj_times, traj_entropies, statuses, transitions);
 	});
 }
 

@@ -202,7 +202,10 @@ __device__ __forceinline__ void mb_fused_body(const mb_fused_params& P)
 		if (EXACT)
 		{
 			curandState rng;
-			curand_init(P.seed, id, 0ull, &rng);
+			if (P.rands)
+				rng = static_cast<const curandState*>(P.rands)[t];
+			else
+				curand_init(P.seed, id, 0ull, &rng);
 			mb_trajectory<true>(P, rng, hsink, trans, acc);
 		}
 		else
@@ -384,10 +387,21 @@ __device__ __forceinline__ void mb_incr_start(const mb_fused_params& P, const mb
 
 #endif // MBG_INCREMENTAL
 
-#ifdef MB_FAMILY_EXACT
-#ifndef MBG_INCREMENTAL
-extern "C" __global__ void __launch_bounds__(256) mb_fused_exact(mb_fused_params P) { mb_fused_body<true>(P); }
-#else
+#if defined(MBG_INCREMENTAL) && (defined(MB_FAMILY_EXACT) || (defined(MB_FAMILY_EPOCH) && !defined(MB_EPOCH_DENSE)))
+// ---- the exact algorithm on incremental unstable sets (models whose rates all have the @logic form)
+//
+// Bit-identical to the reference algorithm (XORWOW streams, draw order, fp32 operation order),
+// without evaluating all N rate functions per step: a stable node's rate is exactly 0 and
+// x + 0.0f == x, so the reference's sequential fp32 sum over all nodes equals the sequential sum over
+// the unstable nodes in node order, and its prefix-count flip selection always stops at an unstable
+// node (simulation.cu:9-21: the first prefix sum reaching r belongs to a node with a non-zero rate).
+// Unstable masks are kept incrementally as in the fast kernel; rates are the float values of the
+// generated code (mbg_inc_rate). The running sum at the end of every state word is kept in shared
+// memory (view slot Q): after a flip only the words from the lowest changed one are re-summed (the
+// running sum up to an unchanged prefix is the same fp32 value), and the flip is found by a binary
+// search over the word-end sums (non-decreasing, all rates being >= 0) and a scan of one word from
+// the previous word-end sum, which reproduces the reference's running comparisons exactly.
+
 // Running fp32 sum over the unstable nodes of state word w, in node order, starting from `run`
 // (adds of 0.f for the missing second node of a pair leave a non-negative sum unchanged).
 __device__ __forceinline__ float mb_exact_word_sum(float run, uint32_t um, uint32_t sw, int w)
@@ -406,28 +420,169 @@ __device__ __forceinline__ float mb_exact_word_sum(float run, uint32_t um, uint3
 	return run;
 }
 
-// Exact mode for models whose rates all have the @logic form. Bit-identical to the reference
-// algorithm (XORWOW streams, draw order, fp32 operation order, epoch boundary), but without
-// evaluating all N rate functions per step: a stable node's rate is exactly 0 and x + 0.0f == x,
-// so the reference's sequential fp32 sum over all nodes equals the sequential sum over the unstable
-// nodes in node order, and its prefix-count flip selection always stops at an unstable node
-// (simulation.cu:9-21: the first prefix sum reaching r belongs to a node with a non-zero rate).
-// Unstable masks are kept incrementally as in the fast kernel; rates are the float values of the
-// generated code (mbg_inc_rate). The running sum at the end of every state word is kept in shared
-// memory: after a flip only the words from the lowest changed one are re-summed (the running sum
-// up to an unchanged prefix is the same fp32 value), and the flip is found by a binary search over
-// the word-end sums (non-decreasing, all rates being >= 0) and a scan of one word from the
-// previous word-end sum, which reproduces the reference's running comparisons exactly.
+// Unstable masks of the states held by the lanes in `lanes`, computed by the whole warp (all 32 lanes
+// call it): one node per lane, one state word at a time. Returns the calling lane's non-internal
+// index when the lane is in `lanes`, else `idx`.
+__device__ __forceinline__ uint32_t mb_exact_masks(const mb_incr_view& v, unsigned lanes, uint32_t idx)
+{
+	const int lane = threadIdx.x & 31;
+	while (lanes)
+	{
+		const int src = __ffs(lanes) - 1;
+		lanes &= lanes - 1u;
+		mb_incr_view c = v;
+		c.st = v.st - (lane - src);
+		c.un = v.un - (lane - src);
+		uint32_t ix = 0;
+		for (int w = 0; w < state_words; w++)
+		{
+			const int i = 32 * w + lane;
+			const bool on = (c.S(w) >> lane) & 1u;
+			bool unstable = false;
+			uint32_t nibit = 0;
+			if (i < state_size)
+			{
+				const int r = __ldg(mbg_inc_self + i);
+				const uint4 hdr = __ldg(mbg_inc_rec_hdr + r);
+				unstable = on != mb_incr_logic(c, r, hdr, __ldg(mbg_inc_rec_in + r));
+				const int pos = (int)((hdr.x >> 21) & 31u) - 1;
+				nibit = (pos >= 0 && on) ? (1u << pos) : 0u;
+			}
+			const uint32_t um = __ballot_sync(0xffffffffu, unstable);
+			ix |= __reduce_or_sync(0xffffffffu, nibit);
+			if (lane == 0)
+				c.U(w) = um;
+		}
+		__syncwarp();
+		if (lane == src)
+			idx = ix;
+	}
+	return idx;
+}
+
+// compute_transition_rates: the total rate, re-summing the word-end sums from word `lo` on.
+__device__ __forceinline__ float mb_exact_total(const mb_incr_view& v, int lo)
+{
+	float total = lo > 0 ? __uint_as_float(v.Q(lo - 1)) : 0.f;
+	for (int w = lo; w < state_words; w++)
+	{
+		total = mb_exact_word_sum(total, v.U(w), v.S(w), w);
+		v.Q(w) = __float_as_uint(total);
+	}
+	return total;
+}
+
+// compute_transition_entropy over the non-internal rates (generator.cpp:146-175).
+__device__ __forceinline__ float mb_exact_entropy(const mb_incr_view& v)
+{
+	float ni_total = 0.f;
+	for (int k = 0; k < mbg_noninternal_count; k++)
+	{
+		const int i = __ldg(mbg_inc_ni_node + k);
+		const uint32_t bit = 1u << (i & 31);
+		if (v.U(i >> 5) & bit)
+			ni_total += __ldg(mbg_inc_rate + 2 * i + ((v.S(i >> 5) & bit) ? 1 : 0));
+	}
+	if (ni_total == 0.f)
+		return 0.f;
+	float entropy = 0.f;
+	for (int k = 0; k < mbg_noninternal_count; k++)
+	{
+		const int i = __ldg(mbg_inc_ni_node + k);
+		const uint32_t bit = 1u << (i & 31);
+		const float r = (v.U(i >> 5) & bit) ? __ldg(mbg_inc_rate + 2 * i + ((v.S(i >> 5) & bit) ? 1 : 0)) : 0.f;
+		const float tmp_prob = r / ni_total;
+		entropy -= (tmp_prob == 0.f) ? 0.f : log2f(tmp_prob) * tmp_prob;
+	}
+	return entropy;
+}
+
+// select_flip_bit: the first node whose running fp32 sum reaches r; its word is the first whose
+// word-end sum reaches r (r <= total = the last word-end sum).
+__device__ __forceinline__ int mb_exact_select(const mb_incr_view& v, float r)
+{
+	int wl = 0, wh = state_words - 1;
+	while (wl < wh)
+	{
+		const int mid = (wl + wh) >> 1;
+		if (__uint_as_float(v.Q(mid)) < r)
+			wl = mid + 1;
+		else
+			wh = mid;
+	}
+	float sum = wl > 0 ? __uint_as_float(v.Q(wl - 1)) : 0.f;
+	uint32_t um = v.U(wl);
+	const uint32_t sw = v.S(wl);
+	int j = -1;
+	while (um)
+	{
+		const int b = __ffs(um) - 1;
+		um &= um - 1u;
+		j = 32 * wl + b;
+		sum += __ldg(mbg_inc_rate + 2 * j + ((sw >> b) & 1u));
+		if (!(sum < r))
+			break;
+	}
+	return j;
+}
+
+// Flips node j, re-evaluates it and the nodes whose logic reads it, updates the non-internal index;
+// returns the lowest state word whose rates changed, and sets ni_changed when the rate of a
+// non-internal node may have changed (the transition entropy depends on nothing else).
+__device__ __forceinline__ int mb_exact_flip(const mb_incr_view& v, int j, uint32_t& idx, bool& ni_changed)
+{
+	v.S(j >> 5) ^= 1u << (j & 31);
+	int lo = j >> 5;
+	const uint4 nj = __ldg(mbg_inc_node + j);
+	const int pj = (int)(nj.w >> 16) - 1;
+	if (pj >= 0)
+		idx ^= 1u << pj;
+	ni_changed |= pj >= 0;
+	const int d0 = (int)nj.z, d1 = d0 + (int)(nj.w & 0xffffu);
+	for (int d = d0; d < d1; d++)
+	{
+		const uint4 hdr = __ldg(mbg_inc_rec_hdr + d);
+		const int k = (int)(hdr.x & 0xffffu);
+		const uint32_t bk = 1u << (k & 31);
+		const bool on = (v.S(k >> 5) & bk) != 0;
+		const bool unstable = on != mb_incr_logic(v, d, hdr, __ldg(mbg_inc_rec_in + d));
+		const uint32_t uw = v.U(k >> 5);
+		if (unstable != ((uw & bk) != 0))
+		{
+			v.U(k >> 5) = uw ^ bk;
+			lo = min(lo, k >> 5);
+			ni_changed |= ((hdr.x >> 21) & 31u) != 0u;
+		}
+	}
+	return lo;
+}
+
+// The per-thread shared-memory view of the exact kernels: state words, unstable masks and word-end
+// running sums, [3 * state_words][blockDim] u32.
+__device__ __forceinline__ mb_incr_view mb_exact_view(uint32_t* smem)
+{
+	const int B = blockDim.x;
+	mb_incr_view v;
+	v.stride = B;
+	v.st = smem + threadIdx.x;
+	v.un = smem + (size_t)state_words * B + threadIdx.x;
+	v.ws = smem + (size_t)2 * state_words * B + threadIdx.x;
+	return v;
+}
+#endif
+
+#ifdef MB_FAMILY_EXACT
+#ifndef MBG_INCREMENTAL
+extern "C" __global__ void __launch_bounds__(256) mb_fused_exact(mb_fused_params P) { mb_fused_body<true>(P); }
+#else
+// Exact mode: persistent, one thread = one trajectory at a time, with the reference's 100-slot epoch
+// boundary (every traj_len - 1 steps the same state is re-evaluated with a fresh draw).
 extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params P)
 {
 	extern __shared__ uint32_t mb_smem_u32[];
 	const int B = blockDim.x;
 	const int lane = threadIdx.x & 31;
-	mb_incr_view v;
-	v.stride = B;
-	v.st = mb_smem_u32 + threadIdx.x;
-	v.un = mb_smem_u32 + (size_t)state_words * B + threadIdx.x;
-	v.ws = mb_smem_u32 + (size_t)2 * state_words * B + threadIdx.x; // word-end running sums (float bits)
+	const mb_incr_view v = mb_exact_view(mb_smem_u32);
 	long long* hsink = P.st.win_h;
 	long long* smem_h = reinterpret_cast<long long*>(mb_smem_u32 + (size_t)3 * state_words * B);
 	if (P.st.h_in_smem)
@@ -445,7 +600,9 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 	uint32_t idx = 0;
 	float time = 0.f;
 	int slot = 1;
-	int lo = 0; // lowest state word changed since the word-end sums were computed
+	int lo = 0;				// lowest state word changed since the word-end sums were computed
+	bool h_stale = true;	// the transition entropy must be recomputed
+	float h_cache = 0.f;
 	curandState rng;
 
 	while (__any_sync(0xffffffffu, working || running))
@@ -457,7 +614,12 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 			if (t < P.n_traj)
 			{
 				starting = true;
-				curand_init(P.seed, P.first_traj + t, 0ull, &rng);
+				// curand_init's skip-ahead is long and a lane starting a trajectory would run it while
+				// the rest of its warp waits: the states come from a parallel init launch when given
+				if (P.rands)
+					rng = static_cast<const curandState*>(P.rands)[t];
+				else
+					curand_init(P.seed, P.first_traj + t, 0ull, &rng);
 				// initial state: one uniform per node in node order (simulation.cu:51-53)
 				for (int w = 0; w < state_words; w++)
 				{
@@ -473,58 +635,20 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 				working = false;
 		}
 		__syncwarp();
-		unsigned pending = __ballot_sync(0xffffffffu, starting);
-		while (pending)
-		{
-			// unstable masks and non-internal index of lane src's initial state, one node per lane
-			const int src = __ffs(pending) - 1;
-			pending &= pending - 1u;
-			mb_incr_view c = v;
-			const int off = (int)threadIdx.x - ((int)(threadIdx.x & ~31u) + src);
-			c.st = v.st - off;
-			c.un = v.un - off;
-			uint32_t ix = 0;
-			for (int w = 0; w < state_words; w++)
-			{
-				const int i = 32 * w + lane;
-				const bool on = (c.S(w) >> lane) & 1u;
-				bool unstable = false;
-				uint32_t nibit = 0;
-				if (i < state_size)
-				{
-					const int r = __ldg(mbg_inc_self + i);
-					const uint4 hdr = __ldg(mbg_inc_rec_hdr + r);
-					unstable = on != mb_incr_logic(c, r, hdr, __ldg(mbg_inc_rec_in + r));
-					const int pos = (int)((hdr.x >> 21) & 31u) - 1;
-					nibit = (pos >= 0 && on) ? (1u << pos) : 0u;
-				}
-				const uint32_t um = __ballot_sync(0xffffffffu, unstable);
-				ix |= __reduce_or_sync(0xffffffffu, nibit);
-				if (lane == 0)
-					c.U(w) = um;
-			}
-			__syncwarp();
-			if (lane == src)
-				idx = ix;
-		}
+		idx = mb_exact_masks(v, __ballot_sync(0xffffffffu, starting), idx);
 		if (starting)
 		{
 			time = 0.f;
 			slot = 1;
 			lo = 0;
+			h_stale = true;
 			running = true;
 		}
 
 		float total = 0.f, h = 0.f, tn = 0.f;
 		if (running)
 		{
-			// compute_transition_rates: sequential fp32 sum over the unstable nodes in node order
-			total = lo > 0 ? __uint_as_float(v.Q(lo - 1)) : 0.f;
-			for (int w = lo; w < state_words; w++)
-			{
-				total = mb_exact_word_sum(total, v.U(w), v.S(w), w);
-				v.Q(w) = __float_as_uint(total);
-			}
+			total = mb_exact_total(v, lo);
 			lo = state_words;
 			if (isinf(total))
 			{
@@ -545,29 +669,10 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 				else
 					tn = time + -logf(curand_uniform(&rng)) / total;
 				tn = fminf(tn, max_time);
-				// compute_transition_entropy over the non-internal rates
-				float ni_total = 0.f;
-				for (int k = 0; k < mbg_noninternal_count; k++)
-				{
-					const int i = __ldg(mbg_inc_ni_node + k);
-					const uint32_t bit = 1u << (i & 31);
-					if (v.U(i >> 5) & bit)
-						ni_total += __ldg(mbg_inc_rate + 2 * i + ((v.S(i >> 5) & bit) ? 1 : 0));
-				}
-				if (ni_total != 0.f)
-				{
-					float entropy = 0.f;
-					for (int k = 0; k < mbg_noninternal_count; k++)
-					{
-						const int i = __ldg(mbg_inc_ni_node + k);
-						const uint32_t bit = 1u << (i & 31);
-						const float r =
-							(v.U(i >> 5) & bit) ? __ldg(mbg_inc_rate + 2 * i + ((v.S(i >> 5) & bit) ? 1 : 0)) : 0.f;
-						const float tmp_prob = r / ni_total;
-						entropy -= (tmp_prob == 0.f) ? 0.f : log2f(tmp_prob) * tmp_prob;
-					}
-					h = entropy;
-				}
+				if (h_stale)
+					h_cache = mb_exact_entropy(v);
+				h_stale = false;
+				h = h_cache;
 			}
 		}
 		if (running)
@@ -597,56 +702,7 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 			else if (P.traj_len > 1 && ++slot >= P.traj_len)
 				slot = 1; // epoch boundary: the next epoch re-evaluates the same state
 			else
-			{
-				// select_flip_bit: the first node whose running fp32 sum reaches r; its word is the
-				// first whose word-end sum reaches r (total = last word-end sum >= r)
-				const float r = curand_uniform(&rng) * total;
-				int wl = 0, wh = state_words - 1;
-				while (wl < wh)
-				{
-					const int mid = (wl + wh) >> 1;
-					if (__uint_as_float(v.Q(mid)) < r)
-						wl = mid + 1;
-					else
-						wh = mid;
-				}
-				float sum = wl > 0 ? __uint_as_float(v.Q(wl - 1)) : 0.f;
-				uint32_t um = v.U(wl);
-				const uint32_t sw = v.S(wl);
-				int j = -1;
-				while (um)
-				{
-					const int b = __ffs(um) - 1;
-					um &= um - 1u;
-					j = 32 * wl + b;
-					sum += __ldg(mbg_inc_rate + 2 * j + ((sw >> b) & 1u));
-					if (!(sum < r))
-						break;
-				}
-
-				// flip j and re-evaluate it and the nodes whose logic reads it
-				v.S(j >> 5) ^= 1u << (j & 31);
-				lo = j >> 5;
-				const uint4 nj = __ldg(mbg_inc_node + j);
-				const int pj = (int)(nj.w >> 16) - 1;
-				if (pj >= 0)
-					idx ^= 1u << pj;
-				const int d0 = (int)nj.z, d1 = d0 + (int)(nj.w & 0xffffu);
-				for (int d = d0; d < d1; d++)
-				{
-					const uint4 hdr = __ldg(mbg_inc_rec_hdr + d);
-					const int k = (int)(hdr.x & 0xffffu);
-					const uint32_t bk = 1u << (k & 31);
-					const bool on = (v.S(k >> 5) & bk) != 0;
-					const bool unstable = on != mb_incr_logic(v, d, hdr, __ldg(mbg_inc_rec_in + d));
-					const uint32_t uw = v.U(k >> 5);
-					if (unstable != ((uw & bk) != 0))
-					{
-						v.U(k >> 5) = uw ^ bk;
-						lo = min(lo, k >> 5);
-					}
-				}
-			}
+				lo = mb_exact_flip(v, mb_exact_select(v, curand_uniform(&rng) * total), idx, h_stale);
 		}
 		__syncwarp();
 	}
@@ -932,7 +988,97 @@ extern "C" __global__ void mb_initialize_initial_state(int n, int stride, const 
 }
 
 #ifdef MB_FAMILY_EPOCH
-// One epoch of at most L-1 recorded steps per trajectory (simulation.cu:77-164).
+#if defined(MBG_INCREMENTAL) && !defined(MB_EPOCH_DENSE)
+// One epoch of at most L-1 recorded steps per trajectory (simulation.cu:77-164) for models whose
+// rates all have the @logic form: the exact algorithm on incremental unstable sets (the same
+// results as the dense per-step evaluation below), each step written to the SoA trajectory buffer
+// (a warp stores 128 contiguous bytes per slot and word). Shared memory: [3 * state_words][blockDim].
+extern "C" __global__ void __launch_bounds__(128)
+	mb_simulate_epoch(int n, int stride, int L, uint32_t* __restrict__ last_states, float* __restrict__ last_times,
+					  curandState* __restrict__ rands, uint32_t* __restrict__ traj_states,
+					  float* __restrict__ traj_times, float* __restrict__ traj_h, uint8_t* __restrict__ statuses,
+					  unsigned long long* __restrict__ transitions)
+{
+	extern __shared__ uint32_t mb_smem_u32[];
+	const int id = blockIdx.x * blockDim.x + threadIdx.x;
+	const bool active = id < n;
+	const mb_incr_view v = mb_exact_view(mb_smem_u32);
+	for (int w = 0; w < state_words; w++)
+		v.S(w) = active ? last_states[(size_t)w * stride + id] : 0u;
+	__syncwarp();
+	uint32_t idx = mb_exact_masks(v, __ballot_sync(0xffffffffu, active), 0u);
+	unsigned long long trans = 0;
+	if (active)
+	{
+		curandState rng = rands[id];
+		float time = last_times[id];
+		trajectory_status status = trajectory_status::CONTINUE;
+		int step = 0;
+		traj_times[(size_t)step * stride + id] = time;
+		step++;
+		int lo = 0;
+		bool h_stale = true;
+		float h_cache = 0.f;
+		for (;;)
+		{
+			const float total = mb_exact_total(v, lo);
+			lo = state_words;
+			float h = 0.f;
+			if (isinf(total))
+			{
+				// an infinite total rate gives zero waiting times forever: end the trajectory
+				time = max_time;
+				break;
+			}
+			if (total == 0.f)
+			{
+				status = trajectory_status::FIXED_POINT;
+				time = max_time;
+			}
+			else
+			{
+				if (discrete_time)
+				{
+					time += time_tick;
+					time = max_time - time_tick < time ? max_time : time;
+				}
+				else
+					time += -logf(curand_uniform(&rng)) / total;
+				time = fminf(time, max_time);
+				if (h_stale)
+					h_cache = mb_exact_entropy(v);
+				h_stale = false;
+				h = h_cache;
+			}
+			for (int w = 0; w < state_words; w++)
+				traj_states[((size_t)step * state_words + w) * stride + id] = v.S(w);
+			traj_times[(size_t)step * stride + id] = time;
+			traj_h[(size_t)step * stride + id] = h;
+			trans += (time != 0.f) ? 1ull : 0ull;
+			step++;
+			if (time >= max_time || step >= L)
+				break;
+			lo = mb_exact_flip(v, mb_exact_select(v, curand_uniform(&rng) * total), idx, h_stale);
+		}
+		for (int s = step; s < L; s++) // empty slots carry the zero-time sentinel
+			traj_times[(size_t)s * stride + id] = 0.f;
+		for (int w = 0; w < state_words; w++)
+			last_states[(size_t)w * stride + id] = v.S(w);
+		rands[id] = rng;
+		last_times[id] = time;
+		if (status != trajectory_status::FIXED_POINT)
+			status = (time >= max_time) ? trajectory_status::FINISHED : trajectory_status::CONTINUE;
+		statuses[id] = (uint8_t)status;
+	}
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+		trans += __shfl_down_sync(0xffffffffu, trans, o);
+	if ((threadIdx.x & 31) == 0 && trans)
+		atomicAdd(transitions, trans);
+}
+#else
+// One epoch of at most L-1 recorded steps per trajectory (simulation.cu:77-164): the reference's
+// per-step algorithm, every node's generated rate function evaluated at every step.
 extern "C" __global__ void __launch_bounds__(256)
 	mb_simulate_epoch(int n, int stride, int L, uint32_t* __restrict__ last_states, float* __restrict__ last_times,
 					  curandState* __restrict__ rands, uint32_t* __restrict__ traj_states,
@@ -1009,6 +1155,7 @@ extern "C" __global__ void __launch_bounds__(256)
 	if ((threadIdx.x & 31) == 0 && trans)
 		atomicAdd(transitions, trans);
 }
+#endif // MBG_INCREMENTAL && !MB_EPOCH_DENSE
 
 #endif // MB_FAMILY_EPOCH
 

@@ -38,4 +38,6 @@ struct mb_fused_params
 	unsigned long long* next_traj;	 // work counter (zeroed by the host)
 	unsigned long long* transitions; // executed simulate iterations
 	unsigned* errors;				 // trajectories stopped because the total rate was not finite
+	void* rands;					 // exact mode: curandState of trajectory t at [t], initialised by a
+									 // separate mb_initialize_random launch, or null (curand_init inline)
 };

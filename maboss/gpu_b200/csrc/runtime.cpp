@@ -196,7 +196,8 @@ module::~module()
 std::vector<char> compile_cubin(const std::string& generated_code, std::string& log, int family)
 {
 	static const char* defines[FAMILY_COUNT] = { "#define MB_FAMILY_EXACT 1\n", "#define MB_FAMILY_FAST 1\n",
-												 "#define MB_FAMILY_EPOCH 1\n" };
+												 "#define MB_FAMILY_EPOCH 1\n",
+												 "#define MB_FAMILY_EPOCH 1\n#define MB_EPOCH_DENSE 1\n" };
 	if (family < 0 || family >= FAMILY_COUNT)
 		throw engine_error(MB_ERR_INVALID, "bad kernel family");
 	const std::string source = generated_code + "\n// ---- engine: kernel parameter blocks\n" + mb_params_source +
@@ -279,6 +280,8 @@ void module::ensure(int family)
 		get(fused_fast, "mb_fused_fast");
 	if (family == FAMILY_EPOCH)
 		get(sim_epoch, "mb_simulate_epoch");
+	if (family == FAMILY_EPOCH_DENSE)
+		get(sim_epoch_dense, "mb_simulate_epoch");
 	if (family != FAMILY_FAST && !init_random)
 		get(init_random, "mb_initialize_random");
 	if (!init_state)
@@ -677,12 +680,14 @@ std::unique_ptr<result> merge_results(const std::vector<const result*>& parts)
 
 namespace {
 
-void launch_fused(module& m, const run_config& c, stats_state& st, long long n, cudaStream_t s)
+// Enqueues the fused kernel (and, in exact mode with `rng`, the parallel XORWOW initialisation);
+// returns the number of kernels launched.
+unsigned launch_fused(module& m, const run_config& c, stats_state& st, long long n, cudaStream_t s, void* rng)
 {
 	if (n > 0xffffffffLL)
 		throw engine_error(MB_ERR_LIMIT, "sample_count above 2^32 - 1");
 	if (n == 0)
-		return;
+		return 0;
 	mb_fused_params P{};
 	P.st = st.p;
 	P.istate = st.istate.as<float>();
@@ -695,6 +700,16 @@ void launch_fused(module& m, const run_config& c, stats_state& st, long long n, 
 	P.errors = st.error_ctr();
 	m.ensure(c.mode == MB_MODE_FUSED_EXACT ? FAMILY_EXACT : FAMILY_FAST);
 	CUfunction f = c.mode == MB_MODE_FUSED_EXACT ? m.fused_exact : m.fused_fast;
+	unsigned launches = 0;
+	if (c.mode == MB_MODE_FUSED_EXACT && rng)
+	{
+		int cnt = (int)n;
+		unsigned long long seed = c.seed, first = c.first_traj;
+		void* a[] = { &cnt, &seed, &first, &rng };
+		launch(m.init_random, (unsigned)((n + 255) / 256), 256, 0, s, a);
+		P.rands = rng;
+		launches++;
+	}
 	int block = c.block;
 	size_t smem = st.h_smem();
 	if (m.incremental)
@@ -714,10 +729,42 @@ void launch_fused(module& m, const run_config& c, stats_state& st, long long n, 
 	const unsigned grid = (unsigned)std::max(1LL, std::min<long long>(needed, (long long)per_sm * m.ctx->sm_count));
 	void* args[] = { &P };
 	launch(f, grid, block, smem, s, args);
+	return launches + 1;
 }
 
 // Buffered epochs (simulation_runner.cu:54-180): simulate -> stats -> partition -> refill.
 } // namespace
+
+void simulate_epoch(module& m, bool dense, cudaStream_t s, int n, int stride, int L, unsigned* last_states,
+					float* last_times, void* rands, unsigned* traj_states, float* traj_times, float* traj_h,
+					unsigned char* statuses, unsigned long long* transitions)
+{
+	if (n <= 0)
+		return;
+	void* a[] = { &n, &stride, &L, &last_states, &last_times, &rands, &traj_states, &traj_times, &traj_h, &statuses,
+				  &transitions };
+	if (dense)
+	{
+		m.ensure(FAMILY_EPOCH_DENSE);
+		launch(m.sim_epoch_dense, (n + 255) / 256, 256, 0, s, a);
+		return;
+	}
+	m.ensure(FAMILY_EPOCH);
+	if (!m.incremental)
+	{
+		launch(m.sim_epoch, (n + 255) / 256, 256, 0, s, a);
+		return;
+	}
+	// per thread in shared memory: state words, unstable masks, word-end running sums
+	constexpr size_t max_smem = 227 * 1024;
+	int block = 128;
+	while (block > 32 && (size_t)12 * m.state_words * block > max_smem)
+		block -= 32;
+	const size_t smem = (size_t)12 * m.state_words * block;
+	if (smem > max_smem)
+		throw engine_error(MB_ERR_LIMIT, "model too large for the incremental epoch kernel's shared memory");
+	launch(m.sim_epoch, (n + block - 1) / block, block, smem, s, a);
+}
 
 size_t partition_scratch_bytes(int n)
 {
@@ -753,13 +800,14 @@ void partition(module& m, cudaStream_t s, int n, int stride, const unsigned char
 
 namespace {
 
-void run_epochs(module& m, const run_config& c, stats_state& st, long long n, cudaStream_t s, int& epochs)
+void run_epochs(module& m, const run_config& c, stats_state& st, long long n, cudaStream_t s, int& epochs,
+				unsigned& launches)
 {
 	const int W = m.state_words;
 	const int L = std::max(2, c.traj_len);
 	if (n <= 0)
 		return;
-	m.ensure(FAMILY_EPOCH);
+	m.ensure(c.mode == MB_MODE_EPOCH_DENSE ? FAMILY_EPOCH_DENSE : FAMILY_EPOCH);
 	const long long Bll = std::min<long long>(std::max(1, c.batch_limit), n);
 	const int B = (int)Bll;
 	dbuf st0((size_t)W * B * 4), st1((size_t)W * B * 4), t0((size_t)B * 4), t1((size_t)B * 4);
@@ -779,6 +827,7 @@ void run_epochs(module& m, const run_config& c, stats_state& st, long long n, cu
 		float* tp = tbuf.as<float>() + offset;
 		void* a2[] = { &cnt, &stride, &istate, &sp, &tp, &rptr };
 		launch(m.init_state, (cnt + 255) / 256, 256, 0, s, a2);
+		launches += 2;
 	};
 
 	init(B, 0, c.first_traj, st0, t0, r0);
@@ -796,8 +845,9 @@ void run_epochs(module& m, const run_config& c, stats_state& st, long long n, cu
 		float* ttp = tt.as<float>();
 		float* thp = th.as<float>();
 		unsigned char* stp = stat.as<unsigned char>();
-		void* as[] = { &in_batch, &stride, &len, &ls, &lt, &rr, &tsp, &ttp, &thp, &stp, &trans };
-		launch(m.sim_epoch, (in_batch + 255) / 256, 256, 0, s, as);
+		simulate_epoch(m, c.mode == MB_MODE_EPOCH_DENSE, s, in_batch, stride, len, ls, lt, rr, tsp, ttp, thp, stp,
+					   trans);
+		launches += 7; // simulate, three statistics, three partition kernels
 		// statistics plugins in the order of main.cpp:65-74
 		st.final_batch(s, in_batch, stride, ls, stp);
 		st.fixed_batch(s, in_batch, stride, ls, stp);
@@ -832,7 +882,8 @@ runner::runner(module& m, const run_config& c) : mod(&m), cfg(c)
 		throw engine_error(MB_ERR_INVALID, "negative sample_count");
 	if (c.block <= 0 || c.block > 256 || (c.block % 32) != 0)
 		throw engine_error(MB_ERR_INVALID, "block size must be a multiple of 32 in [32, 256]");
-	if (c.mode != MB_MODE_EPOCH && c.mode != MB_MODE_FUSED_EXACT && c.mode != MB_MODE_FUSED_FAST)
+	if (c.mode != MB_MODE_EPOCH && c.mode != MB_MODE_EPOCH_DENSE && c.mode != MB_MODE_FUSED_EXACT &&
+		c.mode != MB_MODE_FUSED_FAST)
 		throw engine_error(MB_ERR_INVALID, "unknown run mode");
 	cudaStream_t s = m.ctx->stream;
 	if (c.stats_trajectories < 0 || (c.stats_trajectories > 0 && c.stats_trajectories < c.sample_count))
@@ -840,6 +891,8 @@ runner::runner(module& m, const run_config& c) : mod(&m), cfg(c)
 	st.init(m, c.time_tick, c.max_time, c.discrete_time, c.noninternal_nodes, c.sample_count, c.fixed_capacity_log2, s,
 			7u, c.stats_trajectories);
 	st.set_istate(c.istate, s);
+	if (c.mode == MB_MODE_FUSED_EXACT && c.sample_count > 0 && c.sample_count <= max_rng_states)
+		rng.alloc((size_t)c.sample_count * sizeof(curandState));
 	MB_CUDA(cudaEventCreate(&ev0));
 	MB_CUDA(cudaEventCreate(&ev1));
 	MB_CUDA(cudaStreamSynchronize(s));
@@ -854,7 +907,7 @@ runner::~runner()
 		cudaEventDestroy(ev1);
 }
 
-unsigned runner::kernel_launches() const { return cfg.mode == MB_MODE_EPOCH ? 0u : (cfg.sample_count > 0 ? 1u : 0u); }
+unsigned runner::kernel_launches() const { return launches; }
 
 void runner::launch(cudaStream_t s)
 {
@@ -862,11 +915,12 @@ void runner::launch(cudaStream_t s)
 	st.zero(s);
 	MB_CUDA(cudaEventRecord(ev0, s));
 	epochs = 0;
-	if (cfg.mode == MB_MODE_EPOCH)
-		run_epochs(*mod, cfg, st, cfg.sample_count, s, epochs);
+	launches = 0;
+	if (cfg.mode == MB_MODE_EPOCH || cfg.mode == MB_MODE_EPOCH_DENSE)
+		run_epochs(*mod, cfg, st, cfg.sample_count, s, epochs, launches);
 	else
 	{
-		launch_fused(*mod, cfg, st, cfg.sample_count, s);
+		launches = launch_fused(*mod, cfg, st, cfg.sample_count, s, rng.p);
 		epochs = 1;
 	}
 	MB_CUDA(cudaEventRecord(ev1, s));

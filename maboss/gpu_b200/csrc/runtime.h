@@ -69,15 +69,16 @@ enum kernel_family : int
 {
 	FAMILY_EXACT = 0, // mb_fused_exact
 	FAMILY_FAST = 1,  // mb_fused_fast (incremental or dense)
-	FAMILY_EPOCH = 2, // mb_simulate_epoch
-	FAMILY_COUNT = 3
+	FAMILY_EPOCH = 2, // mb_simulate_epoch (incremental for @logic-form models, else dense)
+	FAMILY_EPOCH_DENSE = 3, // mb_simulate_epoch with every node's rate function evaluated per step
+	FAMILY_COUNT = 4
 };
 
 // Kernel handles resolved from NVRTC-compiled modules.
 struct module
 {
 	context* ctx = nullptr;
-	CUmodule mods[FAMILY_COUNT] = { nullptr, nullptr, nullptr };
+	CUmodule mods[FAMILY_COUNT] = { nullptr, nullptr, nullptr, nullptr };
 	int state_size = 0, state_words = 0;
 	int noninternal_count = -1; // from the generated code (mbg_noninternal_count), -1 if absent
 	bool incremental = false;	// fast mode uses the incremental kernel (generated MBG_INCREMENTAL)
@@ -87,7 +88,7 @@ struct module
 	std::string log;	// NVRTC log
 
 	CUfunction fused_exact = nullptr, fused_fast = nullptr;
-	CUfunction init_random = nullptr, init_state = nullptr, sim_epoch = nullptr;
+	CUfunction init_random = nullptr, init_state = nullptr, sim_epoch = nullptr, sim_epoch_dense = nullptr;
 	CUfunction window_epoch = nullptr, final_epoch = nullptr, fixed_epoch = nullptr;
 	CUfunction compact_count = nullptr, compact_scan = nullptr, compact_scatter = nullptr, fixed_extract = nullptr;
 
@@ -103,6 +104,12 @@ std::unique_ptr<module> compile_module(context& ctx, const std::string& generate
 std::vector<char> compile_cubin(const std::string& generated_code, std::string& log, int family = FAMILY_FAST);
 
 void launch(CUfunction f, unsigned grid, unsigned block, size_t smem, cudaStream_t s, void** args);
+
+// One epoch of the buffered simulation (mb_simulate_epoch) over n trajectories of a batch of capacity
+// `stride`; `dense` selects the reference's per-step evaluation of every rate function.
+void simulate_epoch(module& m, bool dense, cudaStream_t s, int n, int stride, int L, unsigned* last_states,
+					float* last_times, void* rands, unsigned* traj_states, float* traj_times, float* traj_h,
+					unsigned char* statuses, unsigned long long* transitions);
 
 // Stable partition of the CONTINUE trajectories of an epoch batch into another buffer set
 // (last_states SoA [word * stride + i], last_times, random states); the number kept is written to
@@ -219,11 +226,14 @@ struct runner
 	stats_state st;
 	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 	int epochs = 0;
+	unsigned launches = 0; // engine kernels enqueued by the last launch()
+	dbuf rng;			   // exact mode: XORWOW states of every trajectory (empty above max_rng_states)
+	static constexpr long long max_rng_states = 1LL << 24;
 	runner(module& m, const run_config& c);
 	~runner();
 	void launch(cudaStream_t s);
 	std::unique_ptr<result> collect(cudaStream_t s);
-	unsigned kernel_launches() const; // engine kernels enqueued by one launch() (fused modes)
+	unsigned kernel_launches() const; // engine kernels enqueued by the last launch()
 };
 
 // Run a whole simulation with the built-in statistics.

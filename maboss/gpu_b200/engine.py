@@ -8,7 +8,7 @@ import numpy as np
 
 from ._lib import check, lib, read_string
 
-MODES = {"exact": 0, "fast": 1, "epoch": 2}
+MODES = {"exact": 0, "fast": 1, "epoch": 2, "epoch_dense": 3}
 
 
 class RunConfig(C.Structure):

@@ -51,7 +51,7 @@ void simulation_runner::run_simulation(stats_composite& stats_runner, kernel_wra
 		throw std::runtime_error("run_simulation: negative number of trajectories");
 	transitions_ = 0;
 	epochs_ = 0;
-	if (mode != MB_MODE_EPOCH && stats_runner.fusable())
+	if ((mode == MB_MODE_FUSED_EXACT || mode == MB_MODE_FUSED_FAST) && stats_runner.fusable())
 		run_fused(stats_runner, module);
 	else
 		run_buffered(stats_runner, module);

@@ -94,18 +94,25 @@ def test_fast_mode_dense_kernel_for_general_rates(gpu):
     _assert_same(res, raw, ref, False)
 
 
-@pytest.mark.parametrize("name,n", [("cellcycle", 3_000), ("metastasis", 1_000), ("sizek", 1_500)])
-def test_epoch_mode_is_identical_to_fused_exact(gpu, name, n):
-    """Buffered epochs (SoA trajectory buffers + stats kernels) and the fused kernel agree bit for bit."""
-    model = mb.Model(*model_text(name))
-    mod = gpu.compile(model)
-    a, b = mod.run(mode="exact", sample_count=n), mod.run(mode="epoch", sample_count=n)
+def _assert_identical(a, b):
     ra, rb = a.raw(), b.raw()
     for k in ("occ", "cnt", "h"):
         assert np.array_equal(ra[k], rb[k]), k
     assert np.array_equal(a.final_counts, b.final_counts)
     assert a.transitions == b.transitions
     assert [(s.tolist(), c) for s, c in a.fixed] == [(s.tolist(), c) for s, c in b.fixed]
+
+
+@pytest.mark.parametrize("name,n", [("cellcycle", 3_000), ("metastasis", 1_000), ("sizek", 1_500)])
+def test_epoch_mode_is_identical_to_fused_exact(gpu, name, n):
+    """Buffered epochs (SoA trajectory buffers + stats kernels; incremental unstable sets for
+    @logic-form models, or every rate function per step in epoch_dense) and the fused kernel agree
+    bit for bit."""
+    model = mb.Model(*model_text(name))
+    mod = gpu.compile(model)
+    a = mod.run(mode="exact", sample_count=n)
+    for mode in ("epoch", "epoch_dense"):
+        _assert_identical(a, mod.run(mode=mode, sample_count=n))
 
 
 @pytest.mark.parametrize("gen,kw,n", [(synth.c1, {}, 5_000), (synth.c2, dict(noninternal=12, discrete=True), 2_000),
@@ -114,13 +121,9 @@ def test_epoch_mode_is_identical_to_fused_exact_on_synthetic_networks(gpu, gen, 
     """The same identity on @logic-form networks, whose exact kernel keeps incremental unstable sets."""
     model = mb.Model(*gen(**kw))
     mod = gpu.compile(model)
-    a, b = mod.run(mode="exact", sample_count=n), mod.run(mode="epoch", sample_count=n)
-    ra, rb = a.raw(), b.raw()
-    for k in ("occ", "cnt", "h"):
-        assert np.array_equal(ra[k], rb[k]), k
-    assert np.array_equal(a.final_counts, b.final_counts)
-    assert a.transitions == b.transitions
-    assert [(s.tolist(), c) for s, c in a.fixed] == [(s.tolist(), c) for s, c in b.fixed]
+    a = mod.run(mode="exact", sample_count=n)
+    for mode in ("epoch", "epoch_dense"):
+        _assert_identical(a, mod.run(mode=mode, sample_count=n))
 
 
 @pytest.mark.parametrize("name,traj_len", [("metastasis", 2), ("metastasis", 7), ("Montagud2022_Prostate_Cancer", 5)])
@@ -136,19 +139,23 @@ def test_exact_mode_epoch_boundary_length(gpu, name, traj_len):
     o = OracleModel(bnd, cfg)
     ref = o.run(n=n, mode=0, traj_len=traj_len, occ_exp=raw["occ_exp"], ent_exp=raw["ent_exp"])
     _assert_same(res, raw, ref, o.discrete)
-    ep = mod.run(mode="epoch", sample_count=n, traj_len=traj_len)
-    assert np.array_equal(ep.final_counts, res.final_counts) and ep.transitions == res.transitions
+    for mode in ("epoch", "epoch_dense"):
+        _assert_identical(res, mod.run(mode=mode, sample_count=n, traj_len=traj_len))
 
 
 def test_epoch_refill_beyond_batch_limit(gpu):
-    """More trajectories than the batch: refilled slots start fresh streams; totals stay consistent."""
+    """More trajectories than the batch: refilled slots start the streams of their trajectory ids, so
+    the run equals the fused exact run bit for bit."""
     model = mb.Model(*model_text("metastasis"))
     mod = gpu.compile(model)
-    r = mod.run(mode="epoch", sample_count=2_500, batch_limit=1_000)
-    assert r.final_counts.sum() == 2_500
-    assert r.timing[2] >= 3
-    p = r.window_probs
-    assert np.allclose(p.sum(axis=1), 1.0, atol=1e-5)
+    exact = mod.run(mode="exact", sample_count=2_500)
+    for mode in ("epoch", "epoch_dense"):
+        r = mod.run(mode=mode, sample_count=2_500, batch_limit=1_000)
+        assert r.final_counts.sum() == 2_500
+        assert r.timing[2] >= 3
+        p = r.window_probs
+        assert np.allclose(p.sum(axis=1), 1.0, atol=1e-5)
+        _assert_identical(exact, r)
 
 
 def test_fast_mode_statistically_equivalent_to_exact(gpu):
@@ -242,3 +249,14 @@ def test_window_edge_ticks(gpu):
             cfg = internal + tail + " sample_count = 500;"
             model, res, raw, o, ref = _run_both(gpu, bnd, cfg, 500)
             _assert_same(res, raw, ref, False)
+
+
+def test_runner_reports_its_kernel_launches(gpu):
+    """Exact mode: the parallel XORWOW initialisation + the fused kernel; fast mode: the fused kernel;
+    epoch mode: initialisation, then per epoch simulate, three statistics and three partition kernels."""
+    mod = gpu.compile(mb.Model(*model_text("metastasis")))
+    for mode, ok in (("exact", lambda k: k == 2), ("fast", lambda k: k == 1), ("epoch", lambda k: k >= 9)):
+        r = mod.runner(mode=mode, sample_count=1_000)
+        r.launch()
+        r.result()
+        assert ok(r.kernel_launches), (mode, r.kernel_launches)
