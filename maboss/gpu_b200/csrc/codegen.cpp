@@ -256,6 +256,14 @@ void emit_incremental_tables(std::ostream& ss, const model_layout& L)
 	ss << "#define MBG_INCREMENTAL 1" << std::endl;
 	ss << "constexpr int mbg_inc_rate_shift = " << t.rate_shift << ";" << std::endl;
 	emit_array(ss, "uint4", "mbg_inc_node", u4(t.node));
+	// (q_up, q_down) of every node alone: the flip selection scans these (8 bytes per node stay in L1)
+	std::vector<unsigned> q2;
+	for (size_t i = 0; i + 3 < t.node.size(); i += 4)
+	{
+		q2.push_back(t.node[i]);
+		q2.push_back(t.node[i + 1]);
+	}
+	emit_array(ss, "unsigned", "mbg_inc_q", q2);
 	emit_array(ss, "uint4", "mbg_inc_rec_hdr", u4(t.hdr));
 	emit_array(ss, "uint4", "mbg_inc_rec_in", u4(t.in1));
 	emit_array(ss, "uint4", "mbg_inc_rec_in2", u4(t.in2));

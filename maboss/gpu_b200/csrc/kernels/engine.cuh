@@ -880,20 +880,20 @@ extern "C" __global__ void __launch_bounds__(128, 4) mb_fused_fast(mb_fused_para
 				const uint32_t sw = v.S(word);
 				uint32_t um = v.U(word);
 				int j = 32 * word + 31 - __clz(um | 1u);
-				uint4 nj = make_uint4(0u, 0u, 0u, 0u);
+				const uint2* q2 = reinterpret_cast<const uint2*>(mbg_inc_q);
 				while (um)
 				{
 					const int b = __ffs(um) - 1;
 					const int i = 32 * word + b;
-					const uint4 nr = __ldg(mbg_inc_node + i);
-					const uint32_t q = ((sw >> b) & 1u) ? nr.y : nr.x;
+					const uint2 qq = __ldg(q2 + i);
+					const uint32_t q = ((sw >> b) & 1u) ? qq.y : qq.x;
 					j = i;
-					nj = nr;
 					if (r < cum + q)
 						break;
 					cum += q;
 					um &= um - 1u;
 				}
+				const uint4 nj = __ldg(mbg_inc_node + j);
 
 				// flip j and re-evaluate it and the nodes whose logic reads it
 				v.S(j >> 5) ^= 1u << (j & 31);
@@ -902,10 +902,9 @@ extern "C" __global__ void __launch_bounds__(128, 4) mb_fused_fast(mb_fused_para
 					idx ^= 1u << pj;
 				bool ni_changed = pj >= 0;
 				const int d0 = (int)nj.z, d1 = d0 + (int)(nj.w & 0xffffu);
-				for (int d = d0; d < d1; d++)
-				{
-					const uint4 hdr = __ldg(mbg_inc_rec_hdr + d);
-					const uint4 in = __ldg(mbg_inc_rec_in + d);
+				// the dependents of one flip are distinct nodes: their records are evaluated
+				// independently, two at a time so that both records' loads are in flight together
+				auto dependent = [&](int d, const uint4& hdr, const uint4& in) {
 					const int k = (int)(hdr.x & 0xffffu);
 					const int wk = k >> 5;
 					const uint32_t bk = 1u << (k & 31);
@@ -927,6 +926,17 @@ extern "C" __global__ void __launch_bounds__(128, 4) mb_fused_fast(mb_fused_para
 					}
 					if (qn != qo || unstable != was_unstable)
 						ni_changed |= ((hdr.x >> 21) & 31u) != 0u;
+				};
+				for (int d = d0; d < d1; d += 2)
+				{
+					const bool two = d + 1 < d1;
+					const uint4 hdr0 = __ldg(mbg_inc_rec_hdr + d);
+					const uint4 in0 = __ldg(mbg_inc_rec_in + d);
+					const uint4 hdr1 = two ? __ldg(mbg_inc_rec_hdr + d + 1) : make_uint4(0u, 0u, 0u, 0u);
+					const uint4 in1 = two ? __ldg(mbg_inc_rec_in + d + 1) : make_uint4(0u, 0u, 0u, 0u);
+					dependent(d, hdr0, in0);
+					if (two)
+						dependent(d + 1, hdr1, in1);
 				}
 				if (ni_changed)
 					h = mb_incr_entropy(v);

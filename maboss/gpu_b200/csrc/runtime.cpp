@@ -724,6 +724,14 @@ unsigned launch_fused(module& m, const run_config& c, stats_state& st, long long
 			throw engine_error(MB_ERR_LIMIT, "model too large for the incremental kernel's shared memory");
 		smem += per_word * m.state_words * block;
 	}
+	// an explicit block count per SM also fixes the shared-memory carve-out to what those blocks need
+	// (+1 KB reserved per block), leaving the rest of the SM's 256 KB of L1/shared memory to L1
+	// for the model tables; by default the driver picks the carve-out of the highest occupancy
+	int carve = -1;
+	if (c.blocks_per_sm > 0)
+		carve = std::min(100, (int)((c.blocks_per_sm * (smem + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024)));
+	cu_throw(drv().FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_PREFERRED_SHARED_MEMORY_CARVEOUT, carve),
+			 "cuFuncSetAttribute");
 	const int per_sm = c.blocks_per_sm > 0 ? c.blocks_per_sm : occupancy_blocks(f, block, smem);
 	const long long needed = (n + block - 1) / block;
 	const unsigned grid = (unsigned)std::max(1LL, std::min<long long>(needed, (long long)per_sm * m.ctx->sm_count));
