@@ -186,7 +186,7 @@ def run_batched(args) -> None:
     for net, params, n in variants:
         batch.add_variant(nets[net], n, params)
     for _ in range(args.warmup):
-        batch.run(0)
+        batch.run(0)  # the first run tunes the launch shape and captures the CUDA graph
     clocks = ClockSampler(0)
     clocks.start()
     ms, trans = [], 0
@@ -195,11 +195,32 @@ def run_batched(args) -> None:
         trans += sum(batch.result(v).transitions for v in range(len(variants)))
     clk = clocks.stop()
     value = trans / (sum(ms) / 1e3)
+    info = batch.info
+
+    # end to end: whole runs through the public API (graph launch: clears, kernel, extraction, copies
+    # to pinned memory; then every variant's result), wall clock, with and without the graph
+    def wall(b, reps=3):
+        t0 = time.perf_counter()
+        for i in range(reps):
+            b.run(100 + i)
+            for v in range(len(variants)):
+                b.result(v).final_counts
+        return (time.perf_counter() - t0) / reps
+
+    e2e_s = wall(batch)
+    nograph = mb.Batch(ctx)
+    nograph.set_options(use_graph=False, autotune=False)
+    ng_nets = [nograph.add_model(m) for m in models]
+    for net, params, n in variants:
+        nograph.add_variant(ng_nets[net], n, params)
+    nograph.run(0)
+    e2e_nograph_s = wall(nograph)
     # the same variants one launch each (first 32 variants), and with one compilation per variant
     # as the reference needs ($variables are baked into its generated code)
     single_ms, single_trans = 0.0, 0
     for net, params, n in variants[:32]:
         b = mb.Batch(ctx)
+        b.set_options(use_graph=False, autotune=False)
         k = b.add_model(models[net])
         v = b.add_variant(k, n, params)
         b.run(0)
@@ -217,12 +238,18 @@ def run_batched(args) -> None:
                        {"workload": f"c5: {EXTRA_WORKLOADS['c5']}", "mode": "fast (batched kernel)",
                         "variants": len(variants), "trajectories": sum(v[2] for v in variants),
                         "transitions_per_step": trans // args.steps,
-                        "l2": "not flushed (each step re-uploads tables and clears accumulators before the launch)"},
+                        "l2": "not flushed (the per-variant statistics are a few MB; the inputs are tables)",
+                        "launch": {"block": info["block"], "blocks_per_sm": info["blocks_per_sm"],
+                                   "graph_nodes": info["graph_nodes"], "tuned": info["tuning"]}},
                        {"per_variant_launch": {"value": single_trans / (single_ms / 1e3), "variants": 32,
                                                "note": "the first 32 variants, one batched launch each"},
                         "per_variant_compile_and_run": {"value": comp_trans / comp_s, "variants": 4,
                                                         "note": "NVRTC compile + fused fast run per variant, wall time"},
-                        "gpu_launches": args.steps, "clocks": clk})
+                        "e2e": {"value": (trans / args.steps) / e2e_s, "unit": "transitions/s",
+                                "wall_ms_per_run": 1e3 * e2e_s, "wall_ms_per_run_without_graph": 1e3 * e2e_nograph_s,
+                                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": None,
+                                "api": "Batch.run + Batch.result of every variant (graph replay)"},
+                        "gpu_launches": args.steps * (1 + len(variants)), "clocks": clk})
     print(json.dumps(line), flush=True)
 
 

@@ -289,6 +289,19 @@ mb_status mb_batch_add_variant(mb_batch b, int net, const char* const* names, co
 mb_status mb_batch_run(mb_batch b, unsigned long long seed, float* kernel_ms);
 /* a copy of variant `v`'s statistics after mb_batch_run */
 mb_status mb_batch_result(mb_batch b, int v, mb_result* out);
+/* Run options (both on by default). use_graph: the first run of a batch captures everything a run
+ * does on the device (clearing the accumulators, the persistent kernel, the compaction of every
+ * variant's fixed points, the copies of every statistic into pinned host memory) as one CUDA graph,
+ * and later runs replay it with the new seed. autotune: before that capture, the launch shape
+ * (threads per block, resident blocks per SM) is chosen by timing candidates on the batch itself.
+ * Changing the batch (add_model / add_variant) drops the graph and the chosen shape. */
+mb_status mb_batch_set_options(mb_batch b, int use_graph, int autotune);
+/* The launch shape of the last run, the node count of its graph (0 without one) and the number of
+ * launch shapes timed by the autotuner so far. */
+mb_status mb_batch_info(mb_batch b, int* block, int* blocks_per_sm, unsigned* grid, unsigned* graph_nodes,
+                        int* tuned_shapes);
+/* Shape `i` of the autotuner's timings: gradient run or not, threads per block, blocks per SM, kernel ms. */
+mb_status mb_batch_tuning(mb_batch b, int i, int* gradient, int* block, int* blocks_per_sm, float* kernel_ms);
 
 /* Score-function (likelihood-ratio) gradient of L = sum_{w,s} cotangent[w * 2^k + s] * P_w(s) with
  * respect to the $variables `params` (set to `values`), P_w(s) the window probabilities of

@@ -770,6 +770,50 @@ mb_status mb_batch_add_variant(mb_batch b, int net, const char* const* names, co
 	});
 }
 
+mb_status mb_batch_set_options(mb_batch b, int use_graph, int autotune)
+{
+	return guard([&] {
+		need(b, "null batch");
+		b->b->use_graph = use_graph != 0;
+		b->b->autotune = autotune != 0;
+	});
+}
+
+mb_status mb_batch_info(mb_batch b, int* block, int* blocks_per_sm, unsigned* grid, unsigned* graph_nodes,
+						int* tuned_shapes)
+{
+	return guard([&] {
+		need(b, "null batch");
+		const mb::batch_engine& e = *b->b;
+		if (block)
+			*block = e.last_block;
+		if (blocks_per_sm)
+			*blocks_per_sm = e.last_per_sm;
+		if (grid)
+			*grid = e.last_grid;
+		if (graph_nodes)
+			*graph_nodes = e.use_graph ? e.graph_nodes : 0u;
+		if (tuned_shapes)
+			*tuned_shapes = (int)e.tuning.size();
+	});
+}
+
+mb_status mb_batch_tuning(mb_batch b, int i, int* gradient, int* block, int* blocks_per_sm, float* kernel_ms)
+{
+	return guard([&] {
+		need(b && i >= 0 && i < (int)b->b->tuning.size(), "bad tuning index");
+		const auto& t = b->b->tuning[i];
+		if (gradient)
+			*gradient = t.grad ? 1 : 0;
+		if (block)
+			*block = t.block;
+		if (blocks_per_sm)
+			*blocks_per_sm = t.blocks_per_sm;
+		if (kernel_ms)
+			*kernel_ms = t.kernel_ms;
+	});
+}
+
 mb_status mb_batch_run(mb_batch b, unsigned long long seed, float* kernel_ms)
 {
 	return guard([&] {

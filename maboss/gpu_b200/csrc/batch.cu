@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <numeric>
@@ -84,6 +85,7 @@ int batch_engine::add_model(const model_t& m)
 	upload(net->self, t.self, s);
 	upload(net->ni_node, L.noninternal_nodes, s);
 	MB_CUDA(cudaStreamSynchronize(s));
+	invalidate();
 	nets.push_back(std::move(net));
 	return (int)nets.size() - 1;
 }
@@ -124,15 +126,42 @@ int batch_engine::add_variant(int net, const std::map<std::string, float>& overr
 										   "the largest one");
 	var->rate_shift = t.rate_shift;
 	var->q = t.q;
+	invalidate();
 	vars_.push_back(std::move(var));
 	return (int)vars_.size() - 1;
 }
 
-void batch_engine::run(unsigned long long seed, const std::vector<std::vector<double>>* cotangents)
+void batch_engine::invalidate()
 {
+	for (auto& ps : prep)
+		ps.reset();
+}
+
+batch_engine::prepared::~prepared()
+{
+	if (exec)
+		cudaGraphExecDestroy(exec);
+	if (graph)
+		cudaGraphDestroy(graph);
+	if (e0)
+		cudaEventDestroy(e0);
+	if (e1)
+		cudaEventDestroy(e1);
+	if (host)
+		cudaFreeHost(host);
+}
+
+// Device descriptors, per-variant accumulators, extraction buffers and the pinned host arena of one
+// kind of run (forward or gradient); built once and reused until the batch changes.
+batch_engine::prepared& batch_engine::prepare(bool grad)
+{
+	std::unique_ptr<prepared>& slot = prep[grad ? 1 : 0];
+	if (slot)
+		return *slot;
 	MB_CUDA(cudaSetDevice(ctx->device));
 	cudaStream_t s = ctx->stream;
-	const bool grad = cotangents != nullptr;
+	auto ps = std::make_unique<prepared>();
+	ps->grad = grad;
 	int max_W = 1, P = 0;
 	std::vector<mb_net> hnets(nets.size());
 	for (size_t i = 0; i < nets.size(); i++)
@@ -157,16 +186,14 @@ void batch_engine::run(unsigned long long seed, const std::vector<std::vector<do
 	}
 	std::vector<mb_variant> hvars(vars_.size());
 	unsigned long long begin = 0;
+	size_t host_bytes = 0;
+	ps->host_off.resize(vars_.size());
 	for (size_t i = 0; i < vars_.size(); i++)
 	{
 		variant& V = *vars_[i];
 		const model_layout& L = nets[V.net]->L;
 		if (grad)
-		{
-			if ((*cotangents)[i].size() != (size_t)L.windows() << L.noninternal_nodes.size())
-				throw engine_error(MB_ERR_INVALID, "cotangent must have windows * 2^k entries");
 			P = std::max(P, (int)V.grad_params.size());
-		}
 		V.st.init_plain(L.state_words, L.time_tick, L.max_time, L.discrete_time, L.noninternal_nodes, V.n_traj, s);
 		std::vector<uint2> q2(L.state_size);
 		for (int n = 0; n < L.state_size; n++)
@@ -184,11 +211,10 @@ void batch_engine::run(unsigned long long seed, const std::vector<std::vector<do
 		upload(V.d_gp, V.rates.grad_p, s);
 		upload(V.d_gd, V.rates.grad_d, s);
 		V.d_counters.alloc(16);
-		MB_CUDA(cudaMemsetAsync(V.d_counters.p, 0, 16, s));
 		V.d_grad.alloc(std::max<size_t>(1, V.grad_params.size()) * sizeof(double));
-		MB_CUDA(cudaMemsetAsync(V.d_grad.p, 0, V.d_grad.bytes, s));
-		if (grad)
-			upload(V.d_cot, (*cotangents)[i], s);
+		V.d_cot.alloc((size_t)L.windows() * ((size_t)1 << L.noninternal_nodes.size()) * sizeof(double));
+		V.out_states.alloc((size_t)V.st.fp_cap * L.state_words * 4);
+		V.out_counts.alloc((size_t)V.st.fp_cap * 4);
 		mb_variant& d = hvars[i];
 		d.net = V.net;
 		d.rate_shift = V.rate_shift;
@@ -206,70 +232,263 @@ void batch_engine::run(unsigned long long seed, const std::vector<std::vector<do
 		d.g_d = V.d_gd.as<float>();
 		d.grad = V.d_grad.as<double>();
 		begin += (unsigned long long)V.n_traj;
+		// pinned host arena: windows, entropy sums, final counts, stats counters, transitions, gradient
+		host_off_t& o = ps->host_off[i];
+		o.win = host_bytes;
+		host_bytes += V.st.occ.bytes > 8 ? V.st.occ.bytes : V.st.cnt.bytes;
+		o.h = host_bytes;
+		host_bytes += V.st.h.bytes;
+		o.fin = host_bytes;
+		host_bytes += (V.st.fin.bytes + 7) / 8 * 8;
+		o.ctr = host_bytes;
+		host_bytes += 8;
+		o.trans = host_bytes;
+		host_bytes += 8;
+		o.grad = host_bytes;
+		host_bytes += V.d_grad.bytes;
 	}
 	upload(d_nets, hnets, s);
 	upload(d_vars, hvars, s);
-	dbuf counters(64);
-	MB_CUDA(cudaMemsetAsync(counters.p, 0, 64, s));
-
-	mb_batch_params B{};
+	ps->counters.alloc(64);
+	MB_CUDA(cudaHostAlloc(&ps->host, std::max<size_t>(host_bytes, 8), cudaHostAllocDefault));
+	MB_CUDA(cudaEventCreate(&ps->e0));
+	MB_CUDA(cudaEventCreate(&ps->e1));
+	ps->B = std::make_unique<mb_batch_params>();
+	mb_batch_params& B = *ps->B;
 	B.nets = d_nets.as<mb_net>();
 	B.vars = d_vars.as<mb_variant>();
 	B.n_vars = (int)hvars.size();
 	B.max_W = max_W;
 	B.P = P;
 	B.total = begin;
-	B.seed = seed;
-	B.next = counters.as<unsigned long long>();
-	B.errors = counters.as<unsigned>() + 4;
-	const void* fn = grad ? (const void*)mb_batched_grad : (const void*)mb_batched_fast;
-	int block = 128;
-	auto smem_of = [&](int b) { return (size_t)b * (3 * (size_t)max_W + (grad ? 4 * (size_t)P : 0)) * 4; };
-	constexpr size_t max_smem = 227 * 1024;
-	while (block > 32 && smem_of(block) > max_smem)
-		block -= 32;
-	if (smem_of(block) > max_smem)
-		throw engine_error(MB_ERR_LIMIT, "batch too large for shared memory (state words, gradient parameters)");
-	const size_t smem = smem_of(block);
-	if (smem > 48 * 1024)
-		MB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-	int per_sm = 0;
-	MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem));
-	per_sm = std::max(per_sm, 1);
-	const unsigned long long needed = (begin + block - 1) / block;
-	const unsigned grid = (unsigned)std::max<unsigned long long>(
-		1ull, std::min<unsigned long long>(needed, (unsigned long long)per_sm * ctx->sm_count));
-	cudaEvent_t e0, e1;
-	MB_CUDA(cudaEventCreate(&e0));
-	MB_CUDA(cudaEventCreate(&e1));
-	MB_CUDA(cudaEventRecord(e0, s));
-	if (begin > 0)
-	{
-		void* args[] = { &B };
-		MB_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(block), args, smem, s));
-	}
-	MB_CUDA(cudaEventRecord(e1, s));
-	MB_CUDA(cudaEventSynchronize(e1));
-	MB_CUDA(cudaEventElapsedTime(&kernel_ms, e0, e1));
-	cudaEventDestroy(e0);
-	cudaEventDestroy(e1);
-	last_block = block;
-	last_grid = grid;
+	B.next = ps->counters.as<unsigned long long>();
+	B.errors = ps->counters.as<unsigned>() + 4;
+	ps->fn = grad ? (const void*)mb_batched_grad : (const void*)mb_batched_fast;
+	ps->smem_per_thread = (3 * (size_t)max_W + (grad ? 4 * (size_t)P : 0)) * 4;
+	MB_CUDA(cudaStreamSynchronize(s));
+	slot = std::move(ps);
+	return *slot;
+}
 
-	// results
+// Blocks per SM that fit a launch shape, and the shared memory of a block.
+int batch_engine::fit(prepared& ps, int block, size_t& smem) const
+{
+	constexpr size_t max_smem = 227 * 1024;
+	smem = (size_t)block * ps.smem_per_thread;
+	if (smem > max_smem)
+		return 0;
+	if (smem > 48 * 1024)
+		MB_CUDA(cudaFuncSetAttribute(ps.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	MB_CUDA(cudaFuncSetAttribute(ps.fn, cudaFuncAttributePreferredSharedMemoryCarveout, -1));
+	int per_sm = 0;
+	MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ps.fn, block, smem));
+	return per_sm;
+}
+
+void batch_engine::set_shape(prepared& ps, int block, int per_sm)
+{
+	size_t smem = 0;
+	const int max_per_sm = fit(ps, block, smem);
+	if (max_per_sm < 1)
+		throw engine_error(MB_ERR_LIMIT, "batch too large for shared memory (state words, gradient parameters)");
+	per_sm = per_sm > 0 ? std::min(per_sm, max_per_sm) : max_per_sm;
+	// fewer blocks than fit leave the rest of the SM's L1/shared memory to L1 (the network tables)
+	const int carve = per_sm < max_per_sm ? std::min(100, (int)((per_sm * (smem + 1024) * 100 + 228 * 1024 - 1) /
+																 (228 * 1024)))
+										  : -1;
+	MB_CUDA(cudaFuncSetAttribute(ps.fn, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+	const unsigned long long needed = (ps.B->total + block - 1) / block;
+	ps.block = block;
+	ps.per_sm = per_sm;
+	ps.smem = smem;
+	ps.grid = (unsigned)std::max<unsigned long long>(
+		1ull, std::min<unsigned long long>(needed, (unsigned long long)per_sm * ctx->sm_count));
+	if (ps.exec)
+	{
+		cudaGraphExecDestroy(ps.exec);
+		ps.exec = nullptr;
+	}
+	if (ps.graph)
+	{
+		cudaGraphDestroy(ps.graph);
+		ps.graph = nullptr;
+	}
+}
+
+// Everything one run does on the device, in stream order: clear the accumulators, the persistent
+// kernel between the two timing events, per-variant compaction of the fixed points, copies of every
+// statistic into the pinned arena. Capturable as one CUDA graph (no allocation, no host sync).
+void batch_engine::enqueue(prepared& ps, cudaStream_t s, bool capturing)
+{
+	// inside a capture the timing events must become event-record nodes of the graph
+	auto record = [&](cudaEvent_t e) {
+		if (capturing)
+			MB_CUDA(cudaEventRecordWithFlags(e, s, cudaEventRecordExternal));
+		else
+			MB_CUDA(cudaEventRecord(e, s));
+	};
+	for (auto& vp : vars_)
+	{
+		variant& V = *vp;
+		V.st.zero(s);
+		MB_CUDA(cudaMemsetAsync(V.d_counters.p, 0, V.d_counters.bytes, s));
+		MB_CUDA(cudaMemsetAsync(V.d_grad.p, 0, V.d_grad.bytes, s));
+	}
+	MB_CUDA(cudaMemsetAsync(ps.counters.p, 0, ps.counters.bytes, s));
+	record(ps.e0);
+	if (ps.B->total > 0)
+	{
+		void* args[] = { ps.B.get() };
+		MB_CUDA(cudaLaunchKernel(ps.fn, dim3(ps.grid), dim3(ps.block), args, ps.smem, s));
+	}
+	record(ps.e1);
+	char* host = static_cast<char*>(ps.host);
+	for (size_t i = 0; i < vars_.size(); i++)
+	{
+		variant& V = *vars_[i];
+		const host_off_t& o = ps.host_off[i];
+		V.st.extract(s, V.out_states.as<unsigned>(), V.out_counts.as<unsigned>());
+		dbuf& win = V.st.occ.bytes > 8 ? V.st.occ : V.st.cnt;
+		MB_CUDA(cudaMemcpyAsync(host + o.win, win.p, win.bytes, cudaMemcpyDeviceToHost, s));
+		MB_CUDA(cudaMemcpyAsync(host + o.h, V.st.h.p, V.st.h.bytes, cudaMemcpyDeviceToHost, s));
+		MB_CUDA(cudaMemcpyAsync(host + o.fin, V.st.fin.p, V.st.fin.bytes, cudaMemcpyDeviceToHost, s));
+		MB_CUDA(cudaMemcpyAsync(host + o.ctr, V.st.counters.p, 8, cudaMemcpyDeviceToHost, s));
+		MB_CUDA(cudaMemcpyAsync(host + o.trans, V.d_counters.p, 8, cudaMemcpyDeviceToHost, s));
+		MB_CUDA(cudaMemcpyAsync(host + o.grad, V.d_grad.p, V.d_grad.bytes, cudaMemcpyDeviceToHost, s));
+	}
+}
+
+// Times the candidate launch shapes on the batch itself (one run each after a warm-up run) and keeps
+// the fastest: block sizes of 128, 96 and 64 threads, each with the most resident blocks per SM that
+// fit and with one block fewer (which leaves more L1 to the network tables).
+void batch_engine::tune(prepared& ps, cudaStream_t s)
+{
+	std::vector<std::pair<int, int>> cands;
+	for (int block : { 128, 96, 64 })
+	{
+		size_t smem = 0;
+		const int per_sm = fit(ps, block, smem);
+		if (per_sm >= 1)
+			cands.push_back({ block, per_sm });
+		if (per_sm >= 2)
+			cands.push_back({ block, per_sm - 1 });
+	}
+	if (cands.empty())
+		throw engine_error(MB_ERR_LIMIT, "batch too large for shared memory (state words, gradient parameters)");
+	float best = 0.f;
+	std::pair<int, int> pick = cands[0];
+	for (size_t c = 0; c < cands.size(); c++)
+	{
+		set_shape(ps, cands[c].first, cands[c].second);
+		if (c == 0)
+		{
+			enqueue(ps, s, false); // warm-up (first-launch costs)
+			MB_CUDA(cudaStreamSynchronize(s));
+		}
+		enqueue(ps, s, false);
+		MB_CUDA(cudaStreamSynchronize(s));
+		float ms = 0.f;
+		MB_CUDA(cudaEventElapsedTime(&ms, ps.e0, ps.e1));
+		tuning.push_back({ ps.grad, cands[c].first, cands[c].second, ms });
+		if (c == 0 || ms < best)
+		{
+			best = ms;
+			pick = cands[c];
+		}
+	}
+	set_shape(ps, pick.first, pick.second);
+}
+
+void batch_engine::run(unsigned long long seed, const std::vector<std::vector<double>>* cotangents)
+{
+	MB_CUDA(cudaSetDevice(ctx->device));
+	cudaStream_t s = ctx->stream;
+	const bool grad = cotangents != nullptr;
+	prepared& ps = prepare(grad);
+	if (grad)
+		for (size_t i = 0; i < vars_.size(); i++)
+		{
+			variant& V = *vars_[i];
+			const model_layout& L = nets[V.net]->L;
+			if ((*cotangents)[i].size() != (size_t)L.windows() << L.noninternal_nodes.size())
+				throw engine_error(MB_ERR_INVALID, "cotangent must have windows * 2^k entries");
+			MB_CUDA(cudaMemcpyAsync(V.d_cot.p, (*cotangents)[i].data(), V.d_cot.bytes, cudaMemcpyHostToDevice, s));
+		}
+	ps.B->seed = seed;
+	if (ps.block == 0)
+	{
+		if (autotune && ps.B->total > 0)
+			tune(ps, s);
+		else
+			set_shape(ps, 128, 0);
+	}
+	if (use_graph)
+	{
+		if (!ps.exec)
+		{
+			cudaGraph_t g = nullptr;
+			MB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+			enqueue(ps, s, true);
+			MB_CUDA(cudaStreamEndCapture(s, &g));
+			ps.graph = g;
+			MB_CUDA(cudaGraphInstantiate(&ps.exec, g, 0));
+			ps.kernel = nullptr;
+			size_t n_nodes = 0;
+			MB_CUDA(cudaGraphGetNodes(g, nullptr, &n_nodes));
+			std::vector<cudaGraphNode_t> nodes(n_nodes);
+			MB_CUDA(cudaGraphGetNodes(g, nodes.data(), &n_nodes));
+			for (cudaGraphNode_t nd : nodes)
+			{
+				cudaGraphNodeType ty;
+				MB_CUDA(cudaGraphNodeGetType(nd, &ty));
+				if (ty != cudaGraphNodeTypeKernel)
+					continue;
+				cudaKernelNodeParams kp{};
+				MB_CUDA(cudaGraphKernelNodeGetParams(nd, &kp));
+				if (kp.func == ps.fn)
+					ps.kernel = nd;
+			}
+			graph_nodes = (unsigned)n_nodes;
+		}
+		if (ps.kernel)
+		{
+			// this run's seed: the kernel node's parameter block
+			cudaKernelNodeParams kp{};
+			void* args[] = { ps.B.get() };
+			kp.func = const_cast<void*>(ps.fn);
+			kp.gridDim = dim3(ps.grid);
+			kp.blockDim = dim3(ps.block);
+			kp.sharedMemBytes = (unsigned)ps.smem;
+			kp.kernelParams = args;
+			MB_CUDA(cudaGraphExecKernelNodeSetParams(ps.exec, ps.kernel, &kp));
+		}
+		MB_CUDA(cudaGraphLaunch(ps.exec, s));
+	}
+	else
+		enqueue(ps, s, false);
+	MB_CUDA(cudaStreamSynchronize(s));
+	MB_CUDA(cudaEventElapsedTime(&kernel_ms, ps.e0, ps.e1));
+	last_block = ps.block;
+	last_grid = ps.grid;
+	last_per_sm = ps.per_sm;
+
+	// results from the pinned arena (fixed-point records: one copy of the occupied ones)
+	const char* host = static_cast<const char*>(ps.host);
 	for (size_t i = 0; i < vars_.size(); i++)
 	{
 		variant& V = *vars_[i];
 		const network& N = *nets[V.net];
-		V.res = V.st.finalize_plain(V.n_traj, N.L.state_size, s);
+		const host_off_t& o = ps.host_off[i];
+		V.res = V.st.result_from(host + o.win, host + o.h, host + o.fin, host + o.ctr, V.out_states.as<unsigned>(),
+								 V.out_counts.as<unsigned>(), V.n_traj, N.L.state_size);
 		unsigned long long trans = 0;
-		MB_CUDA(cudaMemcpy(&trans, V.d_counters.p, sizeof trans, cudaMemcpyDeviceToHost));
+		std::memcpy(&trans, host + o.trans, sizeof trans);
 		V.res->transitions = trans;
 		V.res->kernel_ms = kernel_ms;
 		V.grad.assign(V.grad_params.size(), 0.0);
 		if (grad && !V.grad_params.empty())
 		{
-			MB_CUDA(cudaMemcpy(V.grad.data(), V.d_grad.p, V.grad.size() * sizeof(double), cudaMemcpyDeviceToHost));
+			std::memcpy(V.grad.data(), host + o.grad, V.grad.size() * sizeof(double));
 			// probabilities are occupancy / (n * tick) (continuous) or count / n (discrete)
 			const double scale = 1.0 / ((double)std::max(1LL, V.n_traj) *
 										(N.L.discrete_time ? 1.0 : (double)N.L.time_tick));
@@ -308,13 +527,7 @@ void plain_stats::init_plain(int words, float tick, float tmax, bool discrete, c
 	fp_counts.alloc((size_t)cap * sizeof(unsigned));
 	fp_states.alloc((size_t)cap * W * sizeof(unsigned));
 	counters.alloc(64);
-	MB_CUDA(cudaMemsetAsync(occ.p, 0, occ.bytes, s));
-	MB_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes, s));
-	MB_CUDA(cudaMemsetAsync(h.p, 0, h.bytes, s));
-	MB_CUDA(cudaMemsetAsync(fin.p, 0, fin.bytes, s));
-	MB_CUDA(cudaMemsetAsync(fp_keys.p, 0, fp_keys.bytes, s));
-	MB_CUDA(cudaMemsetAsync(fp_counts.p, 0, fp_counts.bytes, s));
-	MB_CUDA(cudaMemsetAsync(counters.p, 0, counters.bytes, s));
+	zero(s);
 	p = mb_stats_params{};
 	p.n_windows = n_windows;
 	p.n_bins = n_bins;
@@ -333,7 +546,23 @@ void plain_stats::init_plain(int words, float tick, float tmax, bool discrete, c
 	p.fp_overflow = counters.as<unsigned>();
 }
 
-std::unique_ptr<result> plain_stats::finalize_plain(long long n, int state_size, cudaStream_t s)
+void plain_stats::zero(cudaStream_t s)
+{
+	for (dbuf* b : { &occ, &cnt, &h, &fin, &fp_keys, &fp_counts, &counters })
+		MB_CUDA(cudaMemsetAsync(b->p, 0, b->bytes, s));
+}
+
+void plain_stats::extract(cudaStream_t s, unsigned* out_states, unsigned* out_counts)
+{
+	unsigned* out_n = counters.as<unsigned>() + 1;
+	mbb_fixed_extract<<<(fp_cap + 255) / 256, 256, 0, s>>>(fp_cap, W, p.fp_keys, p.fp_counts, p.fp_states, out_n,
+														  out_states, out_counts);
+	MB_CUDA(cudaGetLastError());
+}
+
+std::unique_ptr<result> plain_stats::result_from(const void* win, const void* hs, const void* fins, const void* ctrs,
+												 const unsigned* out_states, const unsigned* out_counts, long long n,
+												 int state_size)
 {
 	auto r = std::make_unique<result>();
 	r->state_size = state_size;
@@ -351,52 +580,28 @@ std::unique_ptr<result> plain_stats::finalize_plain(long long n, int state_size,
 	if (discrete_time)
 	{
 		r->win_cnt.resize(cells);
-		MB_CUDA(cudaMemcpyAsync(r->win_cnt.data(), cnt.p, cells * 4, cudaMemcpyDeviceToHost, s));
+		std::memcpy(r->win_cnt.data(), win, cells * 4);
 	}
 	else
 	{
 		r->win_occ.resize(cells);
-		MB_CUDA(cudaMemcpyAsync(r->win_occ.data(), occ.p, cells * 8, cudaMemcpyDeviceToHost, s));
+		std::memcpy(r->win_occ.data(), win, cells * 8);
 	}
 	r->win_h.resize(n_windows);
-	MB_CUDA(cudaMemcpyAsync(r->win_h.data(), h.p, n_windows * 8, cudaMemcpyDeviceToHost, s));
+	std::memcpy(r->win_h.data(), hs, n_windows * 8);
 	r->final_cnt.resize(n_bins);
-	MB_CUDA(cudaMemcpyAsync(r->final_cnt.data(), fin.p, n_bins * 4, cudaMemcpyDeviceToHost, s));
-	dbuf on((size_t)fp_cap * W * 4), oc((size_t)fp_cap * 4);
-	unsigned* out_n = counters.as<unsigned>() + 1;
-	mbb_fixed_extract<<<(fp_cap + 255) / 256, 256, 0, s>>>(fp_cap, W, p.fp_keys, p.fp_counts, p.fp_states, out_n,
-														  on.as<unsigned>(), oc.as<unsigned>());
-	MB_CUDA(cudaGetLastError());
-	unsigned ctr[2] = { 0, 0 };
-	MB_CUDA(cudaMemcpyAsync(ctr, counters.p, sizeof ctr, cudaMemcpyDeviceToHost, s));
-	MB_CUDA(cudaStreamSynchronize(s));
+	std::memcpy(r->final_cnt.data(), fins, n_bins * 4);
+	unsigned ctr[2];
+	std::memcpy(ctr, ctrs, sizeof ctr);
 	r->fixed_overflow = ctr[0];
 	const unsigned nfp = ctr[1];
 	std::vector<unsigned> st((size_t)nfp * W), cn(nfp);
 	if (nfp)
 	{
-		MB_CUDA(cudaMemcpy(st.data(), on.p, st.size() * 4, cudaMemcpyDeviceToHost));
-		MB_CUDA(cudaMemcpy(cn.data(), oc.p, cn.size() * 4, cudaMemcpyDeviceToHost));
+		MB_CUDA(cudaMemcpy(st.data(), out_states, st.size() * 4, cudaMemcpyDeviceToHost));
+		MB_CUDA(cudaMemcpy(cn.data(), out_counts, cn.size() * 4, cudaMemcpyDeviceToHost));
 	}
-	std::vector<unsigned> order(nfp);
-	std::iota(order.begin(), order.end(), 0u);
-	std::sort(order.begin(), order.end(), [&](unsigned a, unsigned b) {
-		for (int w = W - 1; w >= 0; w--)
-		{
-			const unsigned x = st[(size_t)a * W + w], y = st[(size_t)b * W + w];
-			if (x != y)
-				return x < y;
-		}
-		return false;
-	});
-	r->fixed_states.resize((size_t)nfp * W);
-	r->fixed_counts.resize(nfp);
-	for (unsigned i = 0; i < nfp; i++)
-	{
-		std::copy(st.begin() + (size_t)order[i] * W, st.begin() + (size_t)(order[i] + 1) * W,
-				  r->fixed_states.begin() + (size_t)i * W);
-		r->fixed_counts[i] = cn[order[i]];
-	}
+	set_fixed_sorted(*r, st, cn);
 	return r;
 }
 

@@ -10,6 +10,8 @@
 #include "model.h"
 #include "runtime.h"
 
+struct mb_batch_params; // kernels/batched.cuh
+
 namespace mb {
 
 // Accumulators of one variant (the layout and fixed-point scales of stats_state, without a
@@ -27,7 +29,13 @@ struct plain_stats
 	mb_stats_params p{};
 	void init_plain(int words, float tick, float tmax, bool discrete, const std::vector<int>& noninternal, long long n,
 					cudaStream_t s);
-	std::unique_ptr<result> finalize_plain(long long n, int state_size, cudaStream_t s);
+	void zero(cudaStream_t s); // clear every accumulator (asynchronous, capturable)
+	// compact the fixed-point table into (state, count) records; their number goes to counters[1]
+	void extract(cudaStream_t s, unsigned* out_states, unsigned* out_counts);
+	// the result from host copies of the accumulators and the device records of the fixed points
+	std::unique_ptr<result> result_from(const void* win, const void* h, const void* fin, const void* counters,
+										const unsigned* out_states, const unsigned* out_counts, long long n,
+										int state_size);
 };
 
 class batch_engine
@@ -49,7 +57,7 @@ public:
 		int rate_shift = 0;
 		std::vector<unsigned> q;
 		plain_stats st;
-		dbuf d_q, d_rate, d_istate, d_gptr, d_gp, d_gd, d_counters, d_grad, d_cot;
+		dbuf d_q, d_rate, d_istate, d_gptr, d_gp, d_gd, d_counters, d_grad, d_cot, out_states, out_counts;
 		std::unique_ptr<result> res;
 		std::vector<double> grad; // d (sum_ws cot[w][s] P_w(s)) / d parameter
 	};
@@ -64,13 +72,56 @@ public:
 	// variant) it also computes the vector-Jacobian products
 	void run(unsigned long long seed, const std::vector<std::vector<double>>* cotangents = nullptr);
 
+	// Runs are captured once as a CUDA graph (clears, kernel, extraction, result copies) and replayed
+	// with the seed updated; the launch shape is chosen by timing candidates on the batch first.
+	bool use_graph = true;
+	bool autotune = true;
+	struct tuning_point
+	{
+		bool grad;
+		int block, blocks_per_sm;
+		float kernel_ms;
+	};
+	std::vector<tuning_point> tuning; // every candidate timed so far
+
 	context* ctx;
 	std::vector<std::unique_ptr<network>> nets;
 	std::vector<std::unique_ptr<variant>> vars_;
 	dbuf d_nets, d_vars;
 	float kernel_ms = 0;
-	int last_block = 0;
+	int last_block = 0, last_per_sm = 0;
 	unsigned last_grid = 0;
+	unsigned graph_nodes = 0; // nodes of the last captured graph
+
+private:
+	struct host_off_t
+	{
+		size_t win = 0, h = 0, fin = 0, ctr = 0, trans = 0, grad = 0;
+	};
+	struct prepared
+	{
+		bool grad = false;
+		std::unique_ptr<mb_batch_params> B; // the kernel's parameter block
+		const void* fn = nullptr;
+		size_t smem_per_thread = 0, smem = 0;
+		int block = 0, per_sm = 0;
+		unsigned grid = 0;
+		dbuf counters;
+		void* host = nullptr; // pinned
+		std::vector<host_off_t> host_off;
+		cudaEvent_t e0 = nullptr, e1 = nullptr;
+		cudaGraph_t graph = nullptr;
+		cudaGraphExec_t exec = nullptr;
+		cudaGraphNode_t kernel = nullptr;
+		~prepared();
+	};
+	std::unique_ptr<prepared> prep[2]; // forward, gradient
+	void invalidate();
+	prepared& prepare(bool grad);
+	int fit(prepared& ps, int block, size_t& smem) const;
+	void set_shape(prepared& ps, int block, int per_sm);
+	void enqueue(prepared& ps, cudaStream_t s, bool capturing);
+	void tune(prepared& ps, cudaStream_t s);
 };
 
 } // namespace mb

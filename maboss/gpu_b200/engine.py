@@ -312,6 +312,23 @@ class Batch:
         check(lib().mb_batch_result(self._h, variant, C.byref(h)))
         return Result(h)
 
+    def set_options(self, use_graph: bool = True, autotune: bool = True) -> None:
+        """mb_batch_set_options: CUDA-graph replay of runs and launch-shape autotuning."""
+        check(lib().mb_batch_set_options(self._h, 1 if use_graph else 0, 1 if autotune else 0))
+
+    @property
+    def info(self) -> dict:
+        """Launch shape of the last run, node count of its CUDA graph, autotuner timings."""
+        b, ps, t = C.c_int(), C.c_int(), C.c_int()
+        g, n = C.c_uint(), C.c_uint()
+        check(lib().mb_batch_info(self._h, C.byref(b), C.byref(ps), C.byref(g), C.byref(n), C.byref(t)))
+        tuning = []
+        for i in range(t.value):
+            gr, bl, bp, ms = C.c_int(), C.c_int(), C.c_int(), C.c_float()
+            check(lib().mb_batch_tuning(self._h, i, C.byref(gr), C.byref(bl), C.byref(bp), C.byref(ms)))
+            tuning.append(dict(gradient=bool(gr.value), block=bl.value, blocks_per_sm=bp.value, kernel_ms=ms.value))
+        return dict(block=b.value, blocks_per_sm=ps.value, grid=g.value, graph_nodes=n.value, tuning=tuning)
+
 
 def gradient(ctx: Context, model: Model, params: dict[str, float], cotangent: np.ndarray, n_traj: int,
              seed: int = 0) -> tuple[np.ndarray, "Result"]:

@@ -153,3 +153,45 @@ def test_autograd_function(gpu):
     g, fwd = mb.gradient(gpu, model, {"$u": u, "$d": d}, cot, 100_000, 5)
     assert np.allclose(probs.detach().numpy(), fwd.window_probs)
     assert np.allclose(theta.grad.numpy(), g)
+
+
+def _sweep_batch(gpu, use_graph, autotune):
+    b = mb.Batch(gpu)
+    b.set_options(use_graph=use_graph, autotune=autotune)
+    bases, variants = synth.c5_sweep(n_variants=12, seed=3)
+    models = [mb.Model(*x) for x in bases]
+    nets = [b.add_model(m) for m in models]
+    for net, params, n in variants:
+        b.add_variant(nets[net], min(n, 4_000), params)
+    return b, len(variants)
+
+
+def test_graph_replay_equals_direct_runs(gpu):
+    """Runs replayed from the captured CUDA graph (seed updated in the kernel node) give the same
+    statistics as runs enqueued directly, seed by seed; the autotuner picks one of the shapes it timed."""
+    g, nv = _sweep_batch(gpu, use_graph=True, autotune=True)
+    d, _ = _sweep_batch(gpu, use_graph=False, autotune=False)
+    for seed in (5, 6, 5):
+        g.run(seed)
+        d.run(seed)
+        for v in range(nv):
+            _same(g.result(v), d.result(v))
+    info = g.info
+    assert info["graph_nodes"] > nv  # clears, kernel, extractions and copies of every variant
+    assert len(info["tuning"]) >= 2
+    assert (info["block"], info["blocks_per_sm"]) in {(t["block"], t["blocks_per_sm"]) for t in info["tuning"]}
+    assert d.info["graph_nodes"] == 0
+
+
+def test_changing_the_batch_rebuilds_the_plan(gpu):
+    """add_variant after a run drops the captured graph: the new variant is simulated and the old
+    ones are unchanged."""
+    b, nv = _sweep_batch(gpu, use_graph=True, autotune=False)
+    b.run(1)
+    before = [b.result(v) for v in range(nv)]
+    model = mb.Model(*model_text("metastasis"))
+    extra = b.add_variant(b.add_model(model), 1_000)
+    b.run(1)
+    for v in range(nv):
+        _same(b.result(v), before[v])
+    _same(b.result(extra), gpu.compile(model).run(mode="fast", sample_count=1_000, seed=1))
