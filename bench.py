@@ -310,7 +310,13 @@ def run_ours(args) -> None:
     t0 = time.perf_counter()
     mod = ctx.compile(model)
     compile_s = time.perf_counter() - t0
-    launch_kw = dict(block=args.block, blocks_per_sm=args.blocks_per_sm)
+    tuned = None
+    if args.block == 0 and args.mode in ("fast", "exact"):
+        # launch shape from the autotuner (probe runs on a slice of this workload, outside the timing)
+        tuned = mod.autotune(mode=args.mode, sample_count=n, first_traj=rank * n)
+        launch_kw = dict(block=tuned["block"], blocks_per_sm=tuned["blocks_per_sm"])
+    else:
+        launch_kw = dict(block=args.block or 256, blocks_per_sm=args.blocks_per_sm)
     runner = mod.runner(mode=args.mode, sample_count=n, first_traj=rank * n, **launch_kw)
     stream = torch.cuda.ExternalStream(ctx.stream, device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=local)  # 256 MiB > 126 MB L2
@@ -416,8 +422,9 @@ def run_ours(args) -> None:
         "config": {"workload": f"{args.workload}: {desc}", "mode": args.mode, "trajectories_per_gpu": n,
                    "nodes": model.num_nodes, "state_words": words, "transitions_per_step": trans_per_step,
                    "l2": "flushed between steps (256 MiB write outside the step events)",
-                   "nvrtc_compile_s": round(compile_s, 2), "block": args.block,
-                   "blocks_per_sm": args.blocks_per_sm or "occupancy calculator"},
+                   "nvrtc_compile_s": round(compile_s, 2), "block": launch_kw["block"],
+                   "blocks_per_sm": launch_kw["blocks_per_sm"] or "occupancy calculator",
+                   "launch_shape": "autotuned (mb_autotune)" if tuned else "given"},
         "e2e": {"value": float(e2e_total.item()) / float(e2e_time.item()), "unit": "transitions/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": "mb_run (Module.run): allocation, H2D, kernel, D2H of all statistics"
@@ -445,7 +452,8 @@ def main() -> None:
     p.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(EXTRA_WORKLOADS), default="c3")
     p.add_argument("--mode", choices=["fast", "exact", "epoch", "epoch_dense"], default="fast")
     p.add_argument("--samples", type=int, default=None, help="trajectories per GPU (default: the workload's)")
-    p.add_argument("--block", type=int, default=256, help="threads per block (the incremental kernels use <= 128)")
+    p.add_argument("--block", type=int, default=0,
+                   help="threads per block (0: chosen by the engine's autotuner, fused modes; 256 otherwise)")
     p.add_argument("--blocks-per-sm", type=int, default=0, help="resident blocks per SM (0: occupancy calculator)")
     p.add_argument("--cpu-sample", type=int, default=2000, help="trajectories of the CPU baseline sample")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")

@@ -259,6 +259,15 @@ typedef struct mb_run_params_s
 /* mb_run for a module from mb_module_compile: cfg->sample_count and cfg->seed are used as given. */
 mb_status mb_run_module(mb_module mod, const mb_run_config* cfg, const mb_run_params* params, mb_result* out);
 
+/* Launch-shape autotuner of the fused modes (no counterpart in the reference, whose launches are
+ * fixed at 256 threads): times candidate shapes (threads per block, resident blocks per SM; fewer
+ * blocks than fit leave more L1 to the model tables) on a slice of the run's own trajectories and
+ * writes the fastest into cfg->block and cfg->blocks_per_sm. *transitions_per_s (optional) is its
+ * probe rate; up to `cap` candidates are reported fastest first in shapes[3 * i + {0, 1}] (block,
+ * blocks per SM) with their rates in rates[i] (both optional). */
+mb_status mb_autotune(mb_module mod, mb_run_config* cfg, float* transitions_per_s, int* shapes, float* rates,
+                      int cap, int* n_shapes);
+
 /* A run with device buffers allocated once (the reference allocates them per
  * simulation_runner::run_simulation, simulation_runner.cu:65-82). mb_runner_launch clears the
  * accumulators and enqueues the simulation on `stream` without synchronising (fused modes; the

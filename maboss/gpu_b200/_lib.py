@@ -61,6 +61,7 @@ def _declare(L: C.CDLL) -> None:
         "mb_result_format": (i32, [vp, i32, i32, P(C.c_char_p), i32, C.c_char_p, sz, P(sz)]),
         "mb_result_create": (i32, [vp, P(vp)]),
         "mb_batch_set_options": (i32, [vp, i32, i32]),
+        "mb_autotune": (i32, [vp, vp, P(f32), P(i32), P(f32), i32, P(i32)]),
         "mb_batch_info": (i32, [vp, P(i32), P(i32), P(C.c_uint), P(C.c_uint), P(i32)]),
         "mb_batch_tuning": (i32, [vp, i32, P(i32), P(i32), P(i32), P(f32)]),
         "mb_result_info": (i32, [vp, P(i64), P(i32), P(f32), P(f32), vp]),

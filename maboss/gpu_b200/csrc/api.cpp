@@ -635,6 +635,32 @@ mb::run_config to_config(mb_module mod, const mb_run_config* cfg)
 }
 } // namespace
 
+mb_status mb_autotune(mb_module mod, mb_run_config* cfg, float* transitions_per_s, int* shapes, float* rates,
+					  int cap, int* n_shapes)
+{
+	return guard([&] {
+		need(mod && cfg, "null argument");
+		const std::vector<mb::tuned_shape> t = mb::autotune(*mod->mod, to_config(mod, cfg));
+		cfg->block = t.front().block;
+		cfg->blocks_per_sm = t.front().blocks_per_sm;
+		if (transitions_per_s)
+			*transitions_per_s = (float)t.front().transitions_per_s;
+		if (n_shapes)
+			*n_shapes = (int)t.size();
+		for (int i = 0; i < cap && i < (int)t.size(); i++)
+		{
+			if (shapes)
+			{
+				shapes[3 * i] = t[i].block;
+				shapes[3 * i + 1] = t[i].blocks_per_sm;
+				shapes[3 * i + 2] = 0;
+			}
+			if (rates)
+				rates[i] = (float)t[i].transitions_per_s;
+		}
+	});
+}
+
 mb_status mb_runner_create(mb_module mod, const mb_run_config* cfg, mb_runner* out)
 {
 	return guard([&] {

@@ -541,5 +541,5 @@ __device__ void mbb_body(const mb_batch_params& B)
 		mb_acc_flush(acc, B.vars[acc_var].st, B.vars[acc_var].st.win_h);
 }
 
-extern "C" __global__ void __launch_bounds__(128) mb_batched_fast(mb_batch_params B) { mbb_body<false>(B); }
+extern "C" __global__ void __launch_bounds__(128, 5) mb_batched_fast(mb_batch_params B) { mbb_body<false>(B); }
 extern "C" __global__ void __launch_bounds__(128) mb_batched_grad(mb_batch_params B) { mbb_body<true>(B); }

@@ -188,6 +188,7 @@ context::~context()
 module::~module()
 {
 	cudaSetDevice(ctx->device);
+	last_runner.reset();
 	for (CUmodule& m : mods)
 		if (m)
 			drv().ModuleUnload(m);
@@ -474,7 +475,8 @@ void stats_state::set_istate(const std::vector<float>& is, cudaStream_t s)
 {
 	if ((int)is.size() != mod->state_size)
 		throw engine_error(MB_ERR_INVALID, "initial probabilities must have one entry per node");
-	istate.alloc(is.size() * sizeof(float));
+	if (istate.bytes != is.size() * sizeof(float))
+		istate.alloc(is.size() * sizeof(float));
 	MB_CUDA(cudaMemcpyAsync(istate.p, is.data(), istate.bytes, cudaMemcpyHostToDevice, s));
 }
 
@@ -556,8 +558,12 @@ std::unique_ptr<result> stats_state::finalize(long long n, cudaStream_t s)
 	// count occupied fixed-point slots, then compact them on the device and copy the records
 	unsigned ctr[8];
 	MB_CUDA(cudaMemsetAsync(extract_ctr(), 0, sizeof(unsigned), s));
-	dbuf out_counts((size_t)fp_cap * sizeof(unsigned));
-	dbuf out_states((size_t)fp_cap * m.state_words * sizeof(unsigned));
+	// compaction buffers, allocated with the first result and kept for the next runs
+	if (fp_cap && out_counts.bytes != (size_t)fp_cap * sizeof(unsigned))
+	{
+		out_counts.alloc((size_t)fp_cap * sizeof(unsigned));
+		out_states.alloc((size_t)fp_cap * m.state_words * sizeof(unsigned));
+	}
 	if (fp_cap)
 	{
 		unsigned cap = fp_cap;
@@ -920,6 +926,7 @@ unsigned runner::kernel_launches() const { return launches; }
 void runner::launch(cudaStream_t s)
 {
 	MB_CUDA(cudaSetDevice(mod->ctx->device));
+	st.set_istate(cfg.istate, s); // the run's input, uploaded by every launch
 	st.zero(s);
 	MB_CUDA(cudaEventRecord(ev0, s));
 	epochs = 0;
@@ -944,8 +951,72 @@ std::unique_ptr<result> runner::collect(cudaStream_t s)
 	return r;
 }
 
+std::vector<tuned_shape> autotune(module& m, const run_config& c)
+{
+	if (c.mode != MB_MODE_FUSED_EXACT && c.mode != MB_MODE_FUSED_FAST)
+		throw engine_error(MB_ERR_INVALID, "the autotuner covers the fused modes");
+	m.ensure(c.mode == MB_MODE_FUSED_EXACT ? FAMILY_EXACT : FAMILY_FAST);
+	CUfunction f = c.mode == MB_MODE_FUSED_EXACT ? m.fused_exact : m.fused_fast;
+	// candidate shapes: the incremental kernels take at most 128 threads and 12 bytes of shared memory
+	// per state word and thread; the dense kernels any multiple of 32 up to 256
+	std::vector<std::pair<int, int>> cands;
+	const std::vector<int> blocks = m.incremental ? std::vector<int>{ 128, 96, 64 } : std::vector<int>{ 256, 128 };
+	for (int block : blocks)
+	{
+		size_t smem = m.incremental ? (size_t)12 * m.state_words * block : 0;
+		if (smem > 227 * 1024)
+			continue;
+		MB_CUDA(cudaSetDevice(m.ctx->device));
+		cu_throw(drv().FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_PREFERRED_SHARED_MEMORY_CARVEOUT, -1), "cuFuncSetAttribute");
+		const int per_sm = occupancy_blocks(f, block, smem + (size_t)std::ceil(std::max(1.0, (double)c.max_time /
+																							   std::max(c.time_tick, 1e-30f))) *
+																  8);
+		cands.push_back({ block, per_sm });
+		if (per_sm >= 2)
+			cands.push_back({ block, per_sm - 1 });
+	}
+	if (cands.empty())
+		throw engine_error(MB_ERR_LIMIT, "model too large for the incremental kernel's shared memory");
+	// a slice of the run: four times what the largest candidate keeps resident, at most the run itself
+	long long resident = 0;
+	for (auto& cd : cands)
+		resident = std::max(resident, (long long)cd.first * cd.second * m.ctx->sm_count);
+	run_config probe = c;
+	probe.sample_count = std::max(1LL, std::min(c.sample_count, 4 * resident));
+	probe.stats_trajectories = 0;
+	std::vector<tuned_shape> out;
+	for (size_t i = 0; i < cands.size(); i++)
+	{
+		probe.block = cands[i].first;
+		probe.blocks_per_sm = cands[i].second;
+		runner rn(m, probe);
+		for (int rep = 0; rep < (i == 0 ? 2 : 1); rep++) // the first probe also warms the module up
+		{
+			rn.launch(m.ctx->stream);
+			auto r = rn.collect(m.ctx->stream);
+			if (rep == (i == 0 ? 1 : 0))
+				out.push_back({ cands[i].first, cands[i].second,
+								r->kernel_ms > 0 ? (double)r->transitions / (r->kernel_ms * 1e-3) : 0.0 });
+		}
+	}
+	std::stable_sort(out.begin(), out.end(),
+					 [](const tuned_shape& a, const tuned_shape& b) { return a.transitions_per_s > b.transitions_per_s; });
+	return out;
+}
+
+bool same_run(const run_config& a, const run_config& b)
+{
+	return a.mode == b.mode && a.sample_count == b.sample_count && a.seed == b.seed && a.first_traj == b.first_traj &&
+		   a.max_time == b.max_time && a.time_tick == b.time_tick && a.discrete_time == b.discrete_time &&
+		   a.istate == b.istate && a.noninternal_nodes == b.noninternal_nodes && a.traj_len == b.traj_len &&
+		   a.batch_limit == b.batch_limit && a.block == b.block && a.blocks_per_sm == b.blocks_per_sm &&
+		   a.fixed_capacity_log2 == b.fixed_capacity_log2 && a.stats_trajectories == b.stats_trajectories;
+}
+
 std::unique_ptr<result> run(module& m, const run_config& c)
 {
+	// the module keeps the runner (device buffers) of its last run and reuses it for the same config
+	std::lock_guard<std::mutex> lk(m.run_mu);
 	cudaStream_t s = m.ctx->stream;
 	cudaEvent_t t0, t1;
 	MB_CUDA(cudaSetDevice(m.ctx->device));
@@ -954,7 +1025,12 @@ std::unique_ptr<result> run(module& m, const run_config& c)
 	MB_CUDA(cudaEventRecord(t0, s));
 	std::unique_ptr<result> r;
 	{
-		runner rn(m, c);
+		if (!m.last_runner || !same_run(m.last_runner->cfg, c))
+		{
+			m.last_runner.reset();
+			m.last_runner = std::make_unique<runner>(m, c);
+		}
+		runner& rn = *m.last_runner;
 		rn.launch(s);
 		r = rn.collect(s);
 	}

@@ -7,6 +7,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -85,6 +86,8 @@ struct module
 	bool has_layout = false; // compiled from a model (full layout known)
 	model_layout layout;
 	std::string source; // generated model source that was compiled with the engine
+	std::mutex run_mu;	// whole runs (run()) of this module are serialised
+	std::unique_ptr<struct runner> last_runner; // buffers of the last run(), reused for the same config
 	std::string log;	// NVRTC log
 
 	CUfunction fused_exact = nullptr, fused_fast = nullptr;
@@ -185,6 +188,7 @@ struct stats_state
 {
 	module* mod = nullptr;
 	dbuf occ, cnt, h, fin, fp_keys, fp_counts, fp_states, counters, istate;
+	dbuf out_counts, out_states; // compacted fixed points (finalize)
 	unsigned fp_cap = 0;
 	int n_windows = 0;
 	unsigned n_bins = 0;
@@ -238,5 +242,14 @@ struct runner
 
 // Run a whole simulation with the built-in statistics.
 std::unique_ptr<result> run(module& m, const run_config& cfg);
+
+// Launch-shape autotuner of the fused kernels: times candidate (threads per block, resident blocks per
+// SM) pairs on a slice of the run's own trajectories and returns them fastest first.
+struct tuned_shape
+{
+	int block = 0, blocks_per_sm = 0;
+	double transitions_per_s = 0;
+};
+std::vector<tuned_shape> autotune(module& m, const run_config& cfg);
 
 } // namespace mb

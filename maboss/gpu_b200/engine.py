@@ -201,6 +201,19 @@ class Module:
         cfg.stats_trajectories = stats_trajectories
         return cfg
 
+    def autotune(self, mode: str = "fast", sample_count: int | None = None, **kw) -> dict:
+        """mb_autotune: the fastest launch shape for this run (pass the result to run() / runner())."""
+        cfg = self.config(mode, sample_count, **kw)
+        rate = C.c_float()
+        shapes = (C.c_int * 48)()
+        rates = (C.c_float * 16)()
+        n = C.c_int()
+        check(lib().mb_autotune(self._h, C.byref(cfg), C.byref(rate), shapes, rates, 16, C.byref(n)))
+        cands = [dict(block=shapes[3 * i], blocks_per_sm=shapes[3 * i + 1], transitions_per_s=rates[i])
+                 for i in range(min(n.value, 16))]
+        return dict(block=cfg.block, blocks_per_sm=cfg.blocks_per_sm, transitions_per_s=rate.value,
+                    candidates=cands)
+
     def run(self, mode: str = "exact", sample_count: int | None = None, **kw) -> "Result":
         """simulation_runner::run_simulation with the built-in statistics (synchronous)."""
         cfg = self.config(mode, sample_count, **kw)

@@ -260,3 +260,16 @@ def test_runner_reports_its_kernel_launches(gpu):
         r.launch()
         r.result()
         assert ok(r.kernel_launches), (mode, r.kernel_launches)
+
+
+def test_autotuner_picks_a_timed_shape_and_results_do_not_depend_on_it(gpu):
+    """mb_autotune times shapes on a slice of the run; exact-mode results are the same whatever the
+    launch shape (every trajectory has its own random stream)."""
+    mod = gpu.compile(mb.Model(*synth.c2(noninternal=12)))
+    t = mod.autotune(mode="exact", sample_count=20_000)
+    shapes = {(c["block"], c["blocks_per_sm"]) for c in t["candidates"]}
+    assert (t["block"], t["blocks_per_sm"]) in shapes and len(shapes) >= 2
+    assert all(c["transitions_per_s"] > 0 for c in t["candidates"])
+    a = mod.run(mode="exact", sample_count=3_000, block=t["block"], blocks_per_sm=t["blocks_per_sm"])
+    b = mod.run(mode="exact", sample_count=3_000, block=64, blocks_per_sm=1)
+    _assert_identical(a, b)
