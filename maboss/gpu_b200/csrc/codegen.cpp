@@ -412,7 +412,9 @@ model_layout analyze_model(const model_t& m)
 	}
 
 	// incremental tables (fast-path models with small logic fan-in only)
-	L.incremental_ok = L.all_fast_path && N <= 65535;
+	// the incremental kernels keep 12 bytes of shared memory per state word and thread: at most 600
+	// words (19200 nodes) fit a block of 32 threads; larger models take the dense kernels
+	L.incremental_ok = L.all_fast_path && N <= 65535 && L.state_words <= 600;
 	constexpr int max_inputs = 12;
 	if (L.incremental_ok)
 	{

@@ -59,7 +59,8 @@ def test_exact_mode_matches_oracle_on_reference_models(gpu, name, n):
 
 @pytest.mark.parametrize("gen,kw,n", [(synth.c1, {}, 20_000), (synth.c2, dict(noninternal=20), 300),
                                       (synth.c2, dict(noninternal=12, discrete=True), 2_000),
-                                      (synth.c4, {}, 2_000), (synth.c3, {}, 300)])
+                                      (synth.c4, {}, 2_000), (synth.c3, {}, 300),
+                                      (synth.c3, dict(n=3000, n_out=12), 24)])
 def test_exact_mode_matches_oracle_on_synthetic_networks(gpu, gen, kw, n):
     bnd, cfg = gen(**kw)
     model, res, raw, o, ref = _run_both(gpu, bnd, cfg, n)
@@ -78,7 +79,8 @@ def test_fast_mode_matches_oracle_fast_mode(gpu, name, n):
 
 @pytest.mark.parametrize("gen,kw,n", [(synth.c1, {}, 20_000), (synth.c2, dict(noninternal=20), 500),
                                       (synth.c2, dict(noninternal=12, discrete=True), 2_000),
-                                      (synth.c4, {}, 3_000), (synth.c3, {}, 300)])
+                                      (synth.c4, {}, 3_000), (synth.c3, {}, 300),
+                                      (synth.c3, dict(n=3000, n_out=12), 24)])
 def test_fast_mode_matches_oracle_on_synthetic_networks(gpu, gen, kw, n):
     bnd, cfg = gen(**kw)
     model, res, raw, o, ref = _run_both(gpu, bnd, cfg, n, mode="fast")
