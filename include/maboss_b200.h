@@ -233,6 +233,8 @@ typedef struct mb_run_config_s
     long long stats_trajectories;  /* 0, or the trajectory count of the whole job when this run is one
                                       shard of it: window sums then use the job's fixed-point scale,
                                       so that mb_result_merge of the shards is exact */
+    int bin_capacity_log2;         /* more than 20 non-internal nodes: log2 of the sparse-bin table size
+                                      (24 bytes a slot), 0 = automatic (4 (T+1) n slots, 2^16 to 2^28) */
 } mb_run_config;
 
 /* Defaults from the model's .cfg constants: mode FUSED_EXACT, traj_len 100, batch 1e6. */
@@ -324,7 +326,10 @@ mb_status mb_gradient(mb_context c, mb_model m, const char* const* params, const
 
 /* ------------------------------------------------------------------ results */
 mb_status mb_result_free(mb_result r);
-/* dims: windows, bins (2^k), non-internal count k, state words W, node count N */
+/* dims: windows, bins (2^k; 0 for a sparse result), non-internal count k, state words W, node count N.
+ * With 21 to 112 non-internal nodes (the reference's limit is 20, src/main.cpp:142-146) the result
+ * is sparse: window probabilities and final states exist only for the states that occurred, through
+ * mb_result_sparse_*; the dense getters (window probabilities, raw window sums, final counts) fail. */
 mb_status mb_result_dims(mb_result r, int* windows, int* bins, int* noninternal, int* state_words, int* nodes);
 mb_status mb_result_transitions(mb_result r, unsigned long long* transitions);
 /* Trajectory count, time constants and non-internal node indices ([k], may be NULL) of a result. */
@@ -339,6 +344,14 @@ mb_status mb_result_window_entropy(mb_result r, double* th);
 mb_status mb_result_window_raw(mb_result r, long long* occupancy, unsigned* counts, long long* entropy,
                                int* occupancy_exponent, int* entropy_exponent);
 mb_status mb_result_final_counts(mb_result r, unsigned* counts);
+/* Sparse results: entry counts and the number of bin additions lost to a full table (0 means exact). */
+mb_status mb_result_sparse_size(mb_result r, long long* window_entries, long long* final_entries,
+                                unsigned* bin_overflow);
+/* Window entries sorted by window then non-internal index (bit i = i-th non-internal node, at most 112
+ * nodes, two uint64 per index: bits 0-63, then 64-127): raw sums (fixed point as in
+ * mb_result_window_raw) and probabilities; any output may be NULL. Final states: the same indices. */
+mb_status mb_result_sparse_windows(mb_result r, int* windows, uint64_t* states, long long* raw, double* probs);
+mb_status mb_result_sparse_final(mb_result r, uint64_t* states, unsigned* counts);
 mb_status mb_result_num_fixed(mb_result r, int* n, unsigned* overflow);
 mb_status mb_result_fixed(mb_result r, int i, uint32_t* state_words, unsigned* count);
 

@@ -613,6 +613,7 @@ mb_status mb_run_config_default(mb_model m, mb_run_config* cfg)
 		c.blocks_per_sm = 0;
 		c.fixed_capacity_log2 = 0;
 		c.stats_trajectories = 0;
+		c.bin_capacity_log2 = 0;
 		*cfg = c;
 	});
 }
@@ -631,6 +632,7 @@ mb::run_config to_config(mb_module mod, const mb_run_config* cfg)
 	c.blocks_per_sm = cfg->blocks_per_sm;
 	c.fixed_capacity_log2 = cfg->fixed_capacity_log2;
 	c.stats_trajectories = cfg->stats_trajectories;
+	c.bin_capacity_log2 = cfg->bin_capacity_log2;
 	return c;
 }
 } // namespace
@@ -731,6 +733,7 @@ mb_status mb_run_module(mb_module mod, const mb_run_config* cfg, const mb_run_pa
 		c.blocks_per_sm = cfg->blocks_per_sm;
 		c.fixed_capacity_log2 = cfg->fixed_capacity_log2;
 		c.stats_trajectories = cfg->stats_trajectories;
+		c.bin_capacity_log2 = cfg->bin_capacity_log2;
 		auto r = std::make_unique<mb_result_s>();
 		r->res = mb::run(*mod->mod, c);
 		*out = r.release();
@@ -945,6 +948,7 @@ mb_status mb_result_window_probs(mb_result r, double* probs)
 		need(r && probs, "null argument");
 		const mb::result& x = *r->res;
 		need(x.sections & MB_STATS_WINDOWS, "the result has no window statistics");
+		need(!x.wide, "sparse result (more than 20 non-internal nodes): use mb_result_sparse_windows");
 		for (int w = 0; w < x.n_windows; w++)
 			for (unsigned b = 0; b < x.n_bins; b++)
 				probs[(size_t)w * x.n_bins + b] = x.n_traj > 0 ? x.window_prob(w, b) : 0.0;
@@ -986,7 +990,63 @@ mb_status mb_result_final_counts(mb_result r, unsigned* counts)
 	return guard([&] {
 		need(r && counts, "null argument");
 		need(r->res->sections & MB_STATS_FINAL, "the result has no final-state statistics");
+		need(!r->res->wide, "sparse result (more than 20 non-internal nodes): use mb_result_sparse_final");
 		std::memcpy(counts, r->res->final_cnt.data(), r->res->final_cnt.size() * sizeof(unsigned));
+	});
+}
+
+mb_status mb_result_sparse_size(mb_result r, long long* window_entries, long long* final_entries,
+								unsigned* bin_overflow)
+{
+	return guard([&] {
+		need(r, "null result");
+		const mb::result& x = *r->res;
+		if (window_entries)
+			*window_entries = (long long)x.sp_w.size();
+		if (final_entries)
+			*final_entries = (long long)x.fin_idx.size();
+		if (bin_overflow)
+			*bin_overflow = x.bin_overflow;
+	});
+}
+
+mb_status mb_result_sparse_windows(mb_result r, int* windows, uint64_t* states, long long* raw, double* probs)
+{
+	return guard([&] {
+		need(r, "null result");
+		const mb::result& x = *r->res;
+		for (size_t i = 0; i < x.sp_w.size(); i++)
+		{
+			if (windows)
+				windows[i] = x.sp_w[i];
+			if (states)
+			{
+				states[2 * i] = (uint64_t)x.sp_idx[i];
+				states[2 * i + 1] = (uint64_t)(x.sp_idx[i] >> 64);
+			}
+			if (raw)
+				raw[i] = x.sp_val[i];
+			if (probs)
+				probs[i] = x.sparse_prob(i);
+		}
+	});
+}
+
+mb_status mb_result_sparse_final(mb_result r, uint64_t* states, unsigned* counts)
+{
+	return guard([&] {
+		need(r, "null result");
+		const mb::result& x = *r->res;
+		for (size_t i = 0; i < x.fin_idx.size(); i++)
+		{
+			if (states)
+			{
+				states[2 * i] = (uint64_t)x.fin_idx[i];
+				states[2 * i + 1] = (uint64_t)(x.fin_idx[i] >> 64);
+			}
+			if (counts)
+				counts[i] = x.fin_cnt[i];
+		}
 	});
 }
 

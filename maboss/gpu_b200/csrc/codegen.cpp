@@ -722,7 +722,28 @@ std::string generate_code(const model_t& m)
 	ss << "    return entropy;" << std::endl << "}" << std::endl << std::endl;
 	ss << "} // namespace" << std::endl << std::endl;
 
-	// ---- get_non_internal_index (generator.cpp:207-235)
+	// ---- get_non_internal_index (generator.cpp:207-235); the reference stops at 20 non-internal
+	// nodes (main.cpp:142-146), this engine goes on to 112 with a 128-bit index and sparse window bins
+	if (L.noninternal_nodes.size() > 112)
+		throw model_error("more than 112 non-internal nodes (" + std::to_string(L.noninternal_nodes.size()) + ")");
+	if (L.noninternal_nodes.size() > 20)
+	{
+		ss << "#define MBG_WIDE_INDEX 1" << std::endl;
+		ss << "__device__ unsigned __int128 get_non_internal_index(const state_word_t* __restrict__ state)"
+		   << std::endl;
+		ss << "{" << std::endl << "    return" << std::endl << "\t\t\t";
+		int k = 0;
+		const int kc = (int)L.noninternal_nodes.size();
+		for (int i : L.noninternal_nodes)
+		{
+			ss << "((unsigned __int128)((state[" << i / 32 << "] >> " << i % 32 << ") & 1u) << " << k++ << ")";
+			if (k != kc)
+				ss << " | ";
+		}
+		ss << ";" << std::endl << "}" << std::endl << std::endl;
+	}
+	else
+	{
 	ss << "__device__ uint32_t get_non_internal_index(const state_word_t* __restrict__ state)" << std::endl;
 	ss << "{" << std::endl;
 	if (L.noninternal_nodes.empty() || L.noninternal_nodes.size() > 32)
@@ -747,6 +768,7 @@ std::string generate_code(const model_t& m)
 		ss << ";" << std::endl;
 	}
 	ss << "}" << std::endl << std::endl;
+	}
 
 	// ---- engine helpers (not part of the reference's generated text)
 	ss << "// ---- B200 engine helpers" << std::endl;

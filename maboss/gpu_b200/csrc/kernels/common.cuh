@@ -15,12 +15,76 @@ __device__ __forceinline__ unsigned long long mb_mix64(unsigned long long x)
 
 // ---------------------------------------------------------------- window accumulation
 
+// The non-internal index: 32 bits for at most 20 non-internal nodes (dense bins, the reference's
+// limit), 128 bits beyond (sparse bins, at most 112 nodes; the generated code defines MBG_WIDE_INDEX).
+#ifdef MBG_WIDE_INDEX
+typedef unsigned __int128 mb_idx_t;
+#else
+typedef uint32_t mb_idx_t;
+#endif
+
+// Adds v to the sparse bin (w, idx): key = (index bits 0-63, index bits 64-111 | (w + 1) << 48);
+// open addressing with bounded linear probing; a bin that finds no slot is counted in bin_overflow
+// and lost (never waited on).
+__device__ inline void mb_bin_add(const mb_stats_params& p, int w, unsigned long long lo, unsigned long long hi,
+								  long long v)
+{
+	const mb_key128 key = { lo, (hi & 0xffffffffffffull) | ((unsigned long long)(w + 1) << 48) };
+	const unsigned long long hsh = mb_mix64(key.lo ^ mb_mix64(key.hi));
+	for (unsigned probe = 0; probe < 64; probe++)
+	{
+		const unsigned slot = (unsigned)(hsh + probe) & p.bin_mask;
+		mb_key128 cur = p.bin_keys[slot];
+		if (cur.lo == 0ull && cur.hi == 0ull)
+		{
+			const mb_key128 empty = { 0ull, 0ull };
+			cur = atomicCAS(p.bin_keys + slot, empty, key);
+			if (cur.lo == 0ull && cur.hi == 0ull)
+				cur = key;
+		}
+		if (cur.lo == key.lo && cur.hi == key.hi)
+		{
+			atomicAdd(reinterpret_cast<unsigned long long*>(p.bin_vals + slot), (unsigned long long)v);
+			return;
+		}
+	}
+	atomicAdd(p.bin_overflow, 1u);
+}
+
+// Window sum of the continuous occupancy, the discrete count, and the final-state count.
+__device__ __forceinline__ void mb_occ_add(const mb_stats_params& p, int w, mb_idx_t idx, long long q)
+{
+#ifdef MBG_WIDE_INDEX
+	mb_bin_add(p, w, (unsigned long long)idx, (unsigned long long)(idx >> 64), q);
+#else
+	atomicAdd(reinterpret_cast<unsigned long long*>(p.win_occ + (size_t)w * p.n_bins + idx), (unsigned long long)q);
+#endif
+}
+
+__device__ __forceinline__ void mb_cnt_add(const mb_stats_params& p, int w, mb_idx_t idx)
+{
+#ifdef MBG_WIDE_INDEX
+	mb_bin_add(p, w, (unsigned long long)idx, (unsigned long long)(idx >> 64), 1);
+#else
+	atomicAdd(p.win_cnt + (size_t)w * p.n_bins + idx, 1u);
+#endif
+}
+
+__device__ __forceinline__ void mb_final_add(const mb_stats_params& p, mb_idx_t idx)
+{
+#ifdef MBG_WIDE_INDEX
+	mb_bin_add(p, p.n_windows, (unsigned long long)idx, (unsigned long long)(idx >> 64), 1);
+#else
+	atomicAdd(p.final_cnt + idx, 1u);
+#endif
+}
+
 // Per-thread run-length accumulator: consecutive slices that fall into the same
 // (window, non-internal state) bin are summed in a register before one atomic.
 struct mb_win_acc
 {
 	int ow;
-	uint32_t oi;
+	mb_idx_t oi;
 	long long oq;
 	int hw;
 	long long hq;
@@ -44,8 +108,7 @@ __device__ __forceinline__ void mb_add_h(long long* hsink, int w, long long v)
 __device__ __forceinline__ void mb_acc_flush(mb_win_acc& a, const mb_stats_params& p, long long* hsink)
 {
 	if (a.ow >= 0 && a.oq != 0)
-		atomicAdd(reinterpret_cast<unsigned long long*>(p.win_occ + (size_t)a.ow * p.n_bins + a.oi),
-				  (unsigned long long)a.oq);
+		mb_occ_add(p, a.ow, a.oi, a.oq);
 	if (a.hw >= 0)
 		mb_add_h(hsink, a.hw, a.hq);
 	mb_acc_init(a);
@@ -54,7 +117,7 @@ __device__ __forceinline__ void mb_acc_flush(mb_win_acc& a, const mb_stats_param
 // Continuous time: the state `idx` occupies (t0, t1]; split it over windows exactly like
 // window_average_small.cu:66-92 and add each slice (and h * slice) to its window.
 __device__ __forceinline__ void mb_record_cont(mb_win_acc& a, const mb_stats_params& p, long long* hsink,
-											   uint32_t idx, float t0, float t1, float h)
+											   mb_idx_t idx, float t0, float t1, float h)
 {
 	float sb = t0;
 	int w = (int)floorf(sb / p.win_tick);
@@ -71,8 +134,7 @@ __device__ __forceinline__ void mb_record_cont(mb_win_acc& a, const mb_stats_par
 			else
 			{
 				if (a.ow >= 0 && a.oq != 0)
-					atomicAdd(reinterpret_cast<unsigned long long*>(p.win_occ + (size_t)a.ow * p.n_bins + a.oi),
-							  (unsigned long long)a.oq);
+					mb_occ_add(p, a.ow, a.oi, a.oq);
 				a.ow = w;
 				a.oi = idx;
 				a.oq = q;
@@ -94,13 +156,13 @@ __device__ __forceinline__ void mb_record_cont(mb_win_acc& a, const mb_stats_par
 }
 
 // Discrete time: count the state at window lround(t0 / tick) (window_average_small.cu:117-130).
-__device__ __forceinline__ void mb_record_disc(const mb_stats_params& p, long long* hsink, uint32_t idx, float t0,
+__device__ __forceinline__ void mb_record_disc(const mb_stats_params& p, long long* hsink, mb_idx_t idx, float t0,
 											   float h)
 {
 	const int w = (int)lroundf(t0 / p.win_tick);
 	if (w >= 0 && w < p.n_windows)
 	{
-		atomicAdd(p.win_cnt + (size_t)w * p.n_bins + idx, 1u);
+		mb_cnt_add(p, w, idx);
 		mb_add_h(hsink, w, __double2ll_rn((double)h * p.fx_h));
 	}
 }

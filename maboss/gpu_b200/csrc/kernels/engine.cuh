@@ -107,7 +107,7 @@ __device__ __forceinline__ void mb_record(mb_win_acc& a, const mb_stats_params& 
 {
 	if (t1 == 0.f) // zero-time slots are empty (window_average_small.cu:68)
 		return;
-	const uint32_t idx = get_non_internal_index(st);
+	const mb_idx_t idx = get_non_internal_index(st);
 	if (discrete_time)
 		mb_record_disc(p, hsink, idx, t0, h);
 	else
@@ -172,7 +172,7 @@ __device__ __forceinline__ void mb_trajectory(const mb_fused_params& P, RNG& rng
 		const float r = curand_uniform(&rng) * total;
 		mb_flip(st, mbg_select_flip(st, r));
 	}
-	atomicAdd(P.st.final_cnt + get_non_internal_index(st), 1u);
+	mb_final_add(P.st, get_non_internal_index(st));
 	if (fixed)
 		mb_fixed_insert(P.st, st);
 }
@@ -247,6 +247,20 @@ __device__ __forceinline__ void mb_fused_body(const mb_fused_params& P)
 // reference; not bit-exact (different random streams and rate rounding below 2^-shift).
 constexpr int MB_WPG = state_words <= 2 ? 1 : (state_words <= 8 ? 2 : 8);
 constexpr int MB_GROUPS = (state_words + MB_WPG - 1) / MB_WPG;
+
+// OR of a non-internal index contribution over the warp (128-bit indices as four 32-bit parts).
+__device__ __forceinline__ mb_idx_t mb_or_all(mb_idx_t v)
+{
+#ifdef MBG_WIDE_INDEX
+	mb_idx_t r = 0;
+#pragma unroll
+	for (int q = 0; q < 4; q++)
+		r |= (mb_idx_t)__reduce_or_sync(0xffffffffu, (unsigned)(v >> (32 * q))) << (32 * q);
+	return r;
+#else
+	return __reduce_or_sync(0xffffffffu, v);
+#endif
+}
 
 struct mb_incr_view
 {
@@ -328,7 +342,7 @@ __device__ __forceinline__ float mb_incr_entropy(const mb_incr_view& v)
 // the non-internal state.
 __device__ __forceinline__ void mb_incr_start(const mb_fused_params& P, const mb_incr_view& v0, int col,
 											  unsigned long long t, unsigned long long (&gs)[MB_GROUPS],
-											  unsigned long long& total, uint32_t& idx)
+											  unsigned long long& total, mb_idx_t& idx)
 {
 	const int lane = threadIdx.x & 31;
 	mb_incr_view v = v0;
@@ -361,19 +375,20 @@ __device__ __forceinline__ void mb_incr_start(const mb_fused_params& P, const mb
 		const uint32_t sw = v.S(w);
 		const bool on = (sw >> lane) & 1u;
 		bool unstable = false;
-		uint32_t q = 0, nibit = 0;
+		uint32_t q = 0;
+		mb_idx_t nibit = 0;
 		if (i < state_size)
 		{
 			const int r = __ldg(mbg_inc_self + i);
 			const uint4 hdr = __ldg(mbg_inc_rec_hdr + r);
 			unstable = on != mb_incr_logic(v, r, hdr, __ldg(mbg_inc_rec_in + r));
 			q = unstable ? (on ? hdr.z : hdr.y) : 0u;
-			const int pos = (int)((hdr.x >> 21) & 31u) - 1;
-			nibit = (pos >= 0 && on) ? (1u << pos) : 0u;
+			const int pos = (int)((hdr.x >> 21) & 127u) - 1;
+			nibit = (pos >= 0 && on) ? ((mb_idx_t)1 << pos) : (mb_idx_t)0;
 		}
 		const uint32_t um = __ballot_sync(0xffffffffu, unstable);
 		const uint32_t qw = __reduce_add_sync(0xffffffffu, q);
-		idx |= __reduce_or_sync(0xffffffffu, nibit);
+		idx |= mb_or_all(nibit);
 		if (lane == 0)
 		{
 			v.U(w) = um;
@@ -423,7 +438,7 @@ __device__ __forceinline__ float mb_exact_word_sum(float run, uint32_t um, uint3
 // Unstable masks of the states held by the lanes in `lanes`, computed by the whole warp (all 32 lanes
 // call it): one node per lane, one state word at a time. Returns the calling lane's non-internal
 // index when the lane is in `lanes`, else `idx`.
-__device__ __forceinline__ uint32_t mb_exact_masks(const mb_incr_view& v, unsigned lanes, uint32_t idx)
+__device__ __forceinline__ mb_idx_t mb_exact_masks(const mb_incr_view& v, unsigned lanes, mb_idx_t idx)
 {
 	const int lane = threadIdx.x & 31;
 	while (lanes)
@@ -433,23 +448,23 @@ __device__ __forceinline__ uint32_t mb_exact_masks(const mb_incr_view& v, unsign
 		mb_incr_view c = v;
 		c.st = v.st - (lane - src);
 		c.un = v.un - (lane - src);
-		uint32_t ix = 0;
+		mb_idx_t ix = 0;
 		for (int w = 0; w < state_words; w++)
 		{
 			const int i = 32 * w + lane;
 			const bool on = (c.S(w) >> lane) & 1u;
 			bool unstable = false;
-			uint32_t nibit = 0;
+			mb_idx_t nibit = 0;
 			if (i < state_size)
 			{
 				const int r = __ldg(mbg_inc_self + i);
 				const uint4 hdr = __ldg(mbg_inc_rec_hdr + r);
 				unstable = on != mb_incr_logic(c, r, hdr, __ldg(mbg_inc_rec_in + r));
-				const int pos = (int)((hdr.x >> 21) & 31u) - 1;
-				nibit = (pos >= 0 && on) ? (1u << pos) : 0u;
+				const int pos = (int)((hdr.x >> 21) & 127u) - 1;
+				nibit = (pos >= 0 && on) ? ((mb_idx_t)1 << pos) : (mb_idx_t)0;
 			}
 			const uint32_t um = __ballot_sync(0xffffffffu, unstable);
-			ix |= __reduce_or_sync(0xffffffffu, nibit);
+			ix |= mb_or_all(nibit);
 			if (lane == 0)
 				c.U(w) = um;
 		}
@@ -529,14 +544,14 @@ __device__ __forceinline__ int mb_exact_select(const mb_incr_view& v, float r)
 // Flips node j, re-evaluates it and the nodes whose logic reads it, updates the non-internal index;
 // returns the lowest state word whose rates changed, and sets ni_changed when the rate of a
 // non-internal node may have changed (the transition entropy depends on nothing else).
-__device__ __forceinline__ int mb_exact_flip(const mb_incr_view& v, int j, uint32_t& idx, bool& ni_changed)
+__device__ __forceinline__ int mb_exact_flip(const mb_incr_view& v, int j, mb_idx_t& idx, bool& ni_changed)
 {
 	v.S(j >> 5) ^= 1u << (j & 31);
 	int lo = j >> 5;
 	const uint4 nj = __ldg(mbg_inc_node + j);
 	const int pj = (int)(nj.w >> 16) - 1;
 	if (pj >= 0)
-		idx ^= 1u << pj;
+		idx ^= (mb_idx_t)1 << pj;
 	ni_changed |= pj >= 0;
 	const int d0 = (int)nj.z, d1 = d0 + (int)(nj.w & 0xffffu);
 	for (int d = d0; d < d1; d++)
@@ -551,7 +566,7 @@ __device__ __forceinline__ int mb_exact_flip(const mb_incr_view& v, int j, uint3
 		{
 			v.U(k >> 5) = uw ^ bk;
 			lo = min(lo, k >> 5);
-			ni_changed |= ((hdr.x >> 21) & 31u) != 0u;
+			ni_changed |= ((hdr.x >> 21) & 127u) != 0u;
 		}
 	}
 	return lo;
@@ -597,7 +612,7 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 	mb_win_acc acc;
 	mb_acc_init(acc);
 	bool working = true, running = false;
-	uint32_t idx = 0;
+	mb_idx_t idx = 0;
 	float time = 0.f;
 	int slot = 1;
 	int lo = 0;				// lowest state word changed since the word-end sums were computed
@@ -655,7 +670,7 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 				// an infinite total rate gives zero waiting times forever: stop this trajectory
 				atomicAdd(P.errors, 1u);
 				running = false;
-				atomicAdd(P.st.final_cnt + idx, 1u);
+				mb_final_add(P.st, idx);
 			}
 			else if (total == 0.f)
 				tn = max_time;
@@ -689,7 +704,7 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 			if (time >= max_time)
 			{
 				running = false;
-				atomicAdd(P.st.final_cnt + idx, 1u);
+				mb_final_add(P.st, idx);
 				if (total == 0.f)
 				{
 					state_word_t st[state_words];
@@ -759,7 +774,7 @@ extern "C" __global__ void __launch_bounds__(128, 4) mb_fused_fast(mb_fused_para
 	bool running = false; // the lane holds a trajectory
 	unsigned long long gs[MB_GROUPS];
 	unsigned long long total = 0;
-	uint32_t idx = 0;
+	mb_idx_t idx = 0;
 	float time = 0.f, h = 0.f;
 	curandStatePhilox4_32_10_t rng;
 
@@ -786,7 +801,7 @@ extern "C" __global__ void __launch_bounds__(128, 4) mb_fused_fast(mb_fused_para
 			const unsigned long long ts = __shfl_sync(0xffffffffu, t, src);
 			unsigned long long gsx[MB_GROUPS];
 			unsigned long long tot;
-			uint32_t ix;
+			mb_idx_t ix;
 			mb_incr_start(P, v, (threadIdx.x & ~31) + src, ts, gsx, tot, ix);
 			if (lane == src)
 			{
@@ -840,7 +855,7 @@ extern "C" __global__ void __launch_bounds__(128, 4) mb_fused_fast(mb_fused_para
 			{
 				// end of the trajectory: final state, fixed point
 				running = false;
-				atomicAdd(P.st.final_cnt + idx, 1u);
+				mb_final_add(P.st, idx);
 				if (total == 0)
 				{
 					state_word_t st[state_words];
@@ -899,7 +914,7 @@ extern "C" __global__ void __launch_bounds__(128, 4) mb_fused_fast(mb_fused_para
 				v.S(j >> 5) ^= 1u << (j & 31);
 				const int pj = (int)(nj.w >> 16) - 1;
 				if (pj >= 0)
-					idx ^= 1u << pj;
+					idx ^= (mb_idx_t)1 << pj;
 				bool ni_changed = pj >= 0;
 				const int d0 = (int)nj.z, d1 = d0 + (int)(nj.w & 0xffffu);
 				// the dependents of one flip are distinct nodes: their records are evaluated
@@ -925,7 +940,7 @@ extern "C" __global__ void __launch_bounds__(128, 4) mb_fused_fast(mb_fused_para
 						total += (unsigned long long)dq;
 					}
 					if (qn != qo || unstable != was_unstable)
-						ni_changed |= ((hdr.x >> 21) & 31u) != 0u;
+						ni_changed |= ((hdr.x >> 21) & 127u) != 0u;
 				};
 				for (int d = d0; d < d1; d += 2)
 				{
@@ -1016,7 +1031,7 @@ extern "C" __global__ void __launch_bounds__(128)
 	for (int w = 0; w < state_words; w++)
 		v.S(w) = active ? last_states[(size_t)w * stride + id] : 0u;
 	__syncwarp();
-	uint32_t idx = mb_exact_masks(v, __ballot_sync(0xffffffffu, active), 0u);
+	mb_idx_t idx = mb_exact_masks(v, __ballot_sync(0xffffffffu, active), 0u);
 	unsigned long long trans = 0;
 	if (active)
 	{
@@ -1216,7 +1231,7 @@ extern "C" __global__ void __launch_bounds__(256)
 
 // Final states of FINISHED / FIXED_POINT trajectories (final_states.cu:9-21).
 extern "C" __global__ void mb_final_epoch(int n, int stride, const uint32_t* __restrict__ last_states,
-										   const uint8_t* __restrict__ statuses, unsigned* __restrict__ final_cnt)
+										   const uint8_t* __restrict__ statuses, mb_stats_params p)
 {
 	const int id = blockIdx.x * blockDim.x + threadIdx.x;
 	if (id >= n)
@@ -1228,8 +1243,24 @@ extern "C" __global__ void mb_final_epoch(int n, int stride, const uint32_t* __r
 #pragma unroll
 		for (int w = 0; w < state_words; w++)
 			st[w] = last_states[(size_t)w * stride + id];
-		atomicAdd(final_cnt + get_non_internal_index(st), 1u);
+		mb_final_add(p, get_non_internal_index(st));
 	}
+}
+
+// Compaction of the occupied sparse bins into (key, value) records.
+extern "C" __global__ void mb_bins_extract(unsigned cap, const mb_key128* __restrict__ keys,
+										   const long long* __restrict__ vals, unsigned* __restrict__ out_n,
+										   mb_key128* __restrict__ out_keys, long long* __restrict__ out_vals)
+{
+	const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= cap)
+		return;
+	const mb_key128 k = keys[i];
+	if (k.lo == 0ull && k.hi == 0ull)
+		return;
+	const unsigned o = atomicAdd(out_n, 1u);
+	out_keys[o] = k;
+	out_vals[o] = vals[i];
 }
 
 // Fixed points of one epoch (replaces the CUB select/sort/run-length pipeline of

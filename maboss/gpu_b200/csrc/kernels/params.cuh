@@ -25,6 +25,12 @@ struct mb_stats_params
 	unsigned* fp_states;  // [cap * W]
 	unsigned fp_mask;	  // cap - 1 (cap is a power of two)
 	unsigned* fp_overflow;
+	// more than 20 non-internal nodes: window sums (continuous occupancy or discrete counts) and, at
+	// window T, final-state counts in a hash table keyed by (window + 1, 64-bit non-internal index)
+	mb_key128* bin_keys;  // [cap] ({0, 0} = empty)
+	long long* bin_vals;  // [cap]
+	unsigned bin_mask;	  // cap - 1
+	unsigned* bin_overflow;
 };
 
 struct mb_fused_params

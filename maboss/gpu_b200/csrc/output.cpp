@@ -24,34 +24,51 @@ std::string state_name(const std::vector<std::string>& names, const unsigned* wo
 	return s.empty() ? "<nil>" : s;
 }
 
-std::vector<unsigned> noninternal_index_to_state(const std::vector<int>& noninternal, int n_nodes, unsigned idx)
+std::vector<unsigned> noninternal_index_to_state(const std::vector<int>& noninternal, int n_nodes,
+												 unsigned __int128 idx)
 {
 	std::vector<unsigned> w((n_nodes + 31) / 32, 0u);
 	for (size_t k = 0; k < noninternal.size(); k++)
-		if (idx & (1u << k))
+		if ((unsigned)(idx >> k) & 1u)
 			w[noninternal[k] / 32] |= 1u << (noninternal[k] % 32);
 	return w;
 }
 
 namespace {
 
-// Probability as the reference prints it (a float).
-float prob_f(const result& r, int w, unsigned b) { return (float)r.window_prob(w, b); }
-
-float window_entropy(const result& r, int w)
+// The non-zero probabilities of window w (as the reference prints them: floats), in increasing order
+// of the non-internal index, from the dense histogram or the sparse bins.
+std::vector<std::pair<unsigned __int128, float>> window_entries(const result& r, int w)
 {
-	float entropy = 0.f;
+	std::vector<std::pair<unsigned __int128, float>> out;
+	if (r.wide)
+	{
+		for (size_t i = r.sp_begin[w]; i < r.sp_begin[w + 1]; i++)
+		{
+			const float p = (float)r.sparse_prob(i);
+			if (p != 0.f)
+				out.push_back({ r.sp_idx[i], p });
+		}
+		return out;
+	}
 	for (unsigned b = 0; b < r.n_bins; b++)
 	{
-		const float p = prob_f(r, w, b);
-		if (p == 0.f)
-			continue;
-		entropy += -std::log2(p) * p;
+		const float p = (float)r.window_prob(w, b);
+		if (p != 0.f)
+			out.push_back({ b, p });
 	}
+	return out;
+}
+
+float window_entropy(const std::vector<std::pair<unsigned __int128, float>>& entries)
+{
+	float entropy = 0.f;
+	for (auto& e : entries)
+		entropy += -std::log2(e.second) * e.second;
 	return entropy;
 }
 
-std::string idx_name(const result& r, const std::vector<std::string>& names, unsigned b)
+std::string idx_name(const result& r, const std::vector<std::string>& names, unsigned __int128 b)
 {
 	auto st = noninternal_index_to_state(r.noninternal_nodes, r.state_size, b);
 	return state_name(names, st.data(), r.state_size);
@@ -62,31 +79,25 @@ std::string idx_name(const result& r, const std::vector<std::string>& names, uns
 std::string format_probtraj_csv(const result& r, const std::vector<std::string>& names)
 {
 	std::ostringstream ofs;
-	int max_states = 0;
+	std::vector<std::vector<std::pair<unsigned __int128, float>>> entries(r.n_windows);
+	size_t max_states = 0;
 	for (int w = 0; w < r.n_windows; w++)
 	{
-		int c = 0;
-		for (unsigned b = 0; b < r.n_bins; b++)
-			c += prob_f(r, w, b) != 0.f ? 1 : 0;
-		max_states = std::max(max_states, c);
+		entries[w] = window_entries(r, w);
+		max_states = std::max(max_states, entries[w].size());
 	}
 	ofs << "Time\tTH\tErrorTH\tH\tHD=0";
-	for (int i = 0; i < max_states; i++)
+	for (size_t i = 0; i < max_states; i++)
 		ofs << "\tState\tProba\tErrorProba";
 	ofs << std::endl;
 	for (int w = 0; w < r.n_windows; w++)
 	{
 		const float th = (float)r.window_th(w);
-		const float entropy = window_entropy(r, w);
+		const float entropy = window_entropy(entries[w]);
 		ofs << (float)w * r.time_tick << "\t";
 		ofs << th << "\t" << 0.f << "\t" << entropy << "\t" << 0.f;
-		for (unsigned b = 0; b < r.n_bins; b++)
-		{
-			const float p = prob_f(r, w, b);
-			if (p == 0.f)
-				continue;
-			ofs << "\t" << idx_name(r, names, b) << "\t" << p << "\t" << 0.f;
-		}
+		for (auto& e : entries[w])
+			ofs << "\t" << idx_name(r, names, e.first) << "\t" << e.second << "\t" << 0.f;
 		ofs << std::endl;
 	}
 	return ofs.str();
@@ -117,6 +128,9 @@ std::string format_final_visualize(const result& r, const std::vector<std::strin
 {
 	std::ostringstream os;
 	os << "final points:" << std::endl;
+	if (r.wide)
+		for (size_t i = 0; i < r.fin_idx.size(); i++)
+			os << (float)r.fin_cnt[i] / (float)r.n_traj << " " << idx_name(r, names, r.fin_idx[i]) << std::endl;
 	for (unsigned b = 0; b < r.n_bins && b < r.final_cnt.size(); b++)
 		if (r.final_cnt[b] != 0)
 			os << (float)r.final_cnt[b] / (float)r.n_traj << " " << idx_name(r, names, b) << std::endl;
@@ -145,16 +159,12 @@ std::string format_windows_visualize(const result& r, const std::vector<std::str
 		return os.str();
 	for (int w = 0; w < r.n_windows; w++)
 	{
+		const auto entries = window_entries(r, w);
 		os << "window (" << (float)w * r.time_tick << ", " << (float)(w + 1) * r.time_tick << "]" << std::endl;
-		os << "entropy: " << window_entropy(r, w) << std::endl;
+		os << "entropy: " << window_entropy(entries) << std::endl;
 		os << "transition entropy: " << (float)r.window_th(w) << std::endl;
-		for (unsigned b = 0; b < r.n_bins; b++)
-		{
-			const float p = prob_f(r, w, b);
-			if (p == 0.f)
-				continue;
-			os << p << " " << idx_name(r, names, b) << std::endl;
-		}
+		for (auto& e : entries)
+			os << e.second << " " << idx_name(r, names, e.first) << std::endl;
 	}
 	return os.str();
 }

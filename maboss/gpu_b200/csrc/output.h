@@ -12,7 +12,8 @@ namespace mb {
 std::string state_name(const std::vector<std::string>& names, const unsigned* words, int n_nodes);
 
 // window_average_small_stats::non_internal_idx_to_state (window_average_small.cpp:109-124).
-std::vector<unsigned> noninternal_index_to_state(const std::vector<int>& noninternal, int n_nodes, unsigned idx);
+std::vector<unsigned> noninternal_index_to_state(const std::vector<int>& noninternal, int n_nodes,
+												 unsigned __int128 idx);
 
 // <prefix>_probtraj.csv (window_average_small.cpp:181-250).
 std::string format_probtraj_csv(const result& r, const std::vector<std::string>& names);

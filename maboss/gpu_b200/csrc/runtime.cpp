@@ -208,7 +208,7 @@ std::vector<char> compile_cubin(const std::string& generated_code, std::string& 
 	if (N <= 0 || W != (N + 31) / 32)
 		throw engine_error(MB_ERR_COMPILE, "generated code does not define state_size/state_words");
 	const std::string inc = "-I" + cuda_include_dir();
-	const char* opts[] = { "-arch=sm_100a", "-std=c++17", "-lineinfo", "-DNDEBUG", inc.c_str() };
+	const char* opts[] = { "-arch=sm_100a", "-std=c++17", "-lineinfo", "-DNDEBUG", "--device-int128", inc.c_str() };
 	const size_t key = std::hash<std::string>()(source + inc);
 	{
 		std::lock_guard<std::mutex> lk(cache_mu);
@@ -295,6 +295,7 @@ void module::ensure(int family)
 		get(compact_scan, "mb_compact_scan");
 		get(compact_scatter, "mb_compact_scatter");
 		get(fixed_extract, "mb_fixed_extract");
+		get(bins_extract, "mb_bins_extract");
 	}
 }
 
@@ -365,6 +366,13 @@ double result::window_prob(int w, unsigned bin) const
 	return ((double)win_occ[i] / fx) / ((double)n_traj * (double)time_tick);
 }
 
+double result::sparse_prob(size_t i) const
+{
+	if (discrete_time)
+		return (double)sp_val[i] / (double)n_traj;
+	return ((double)sp_val[i] / fx) / ((double)n_traj * (double)time_tick);
+}
+
 double result::window_th(int w) const
 {
 	double v = ((double)win_h[w] / fx_h) / (double)n_traj;
@@ -374,7 +382,8 @@ double result::window_th(int w) const
 // ---------------------------------------------------------------- statistics state
 
 void stats_state::init(module& m, float tick, float tmax, bool discrete, const std::vector<int>& noninternal,
-					   long long n, int fixed_capacity_log2, cudaStream_t s, unsigned secs, long long scale_traj)
+					   long long n, int fixed_capacity_log2, cudaStream_t s, unsigned secs, long long scale_traj,
+					   int bin_capacity_log2)
 {
 	mod = &m;
 	if (secs == 0 || (secs & ~7u))
@@ -385,9 +394,9 @@ void stats_state::init(module& m, float tick, float tmax, bool discrete, const s
 	if ((secs & 3u) && m.noninternal_count >= 0 && m.noninternal_count != k)
 		throw engine_error(MB_ERR_INVALID, "the module was generated for " + std::to_string(m.noninternal_count) +
 											   " non-internal nodes, the statistics got " + std::to_string(k));
-	if (k > 20)
-		throw engine_error(MB_ERR_LIMIT, "more than 20 non-internal nodes (" + std::to_string(k) +
-											 ") is not supported by the dense window histogram");
+	if (k > 112)
+		throw engine_error(MB_ERR_LIMIT, "more than 112 non-internal nodes (" + std::to_string(k) + ")");
+	wide = k > 20 && (secs & 3u);
 	for (int i : noninternal)
 		if (i < 0 || i >= m.state_size)
 			throw engine_error(MB_ERR_INVALID, "non-internal node index out of range");
@@ -400,7 +409,9 @@ void stats_state::init(module& m, float tick, float tmax, bool discrete, const s
 	if (T > (double)(1 << 24))
 		throw engine_error(MB_ERR_LIMIT, "too many windows (max_time / time_tick)");
 	n_windows = (int)T;
-	n_bins = 1u << k;
+	if (wide && n_windows > 65533)
+		throw engine_error(MB_ERR_LIMIT, "sparse window bins support at most 65533 windows");
+	n_bins = wide ? 0u : 1u << std::min(k, 20);
 	discrete_time = discrete;
 	time_tick = tick;
 	max_time = tmax;
@@ -411,7 +422,25 @@ void stats_state::init(module& m, float tick, float tmax, bool discrete, const s
 	h_in_smem = n_windows * sizeof(long long) <= 48 * 1024 ? 1 : 0;
 
 	const size_t cells = (size_t)n_windows * n_bins;
-	if (sections & 1u)
+	if (wide)
+	{
+		// one table for the window bins and (at window T) the final states; automatic size: four
+		// slots per trajectory and window (a chaotic network makes ~1.5 distinct bins per trajectory
+		// and window and shares almost none across trajectories), 2^16 to 2^28 slots
+		const long long want = std::min<long long>(std::max(n, 1LL) * (n_windows + 1), 1LL << 26);
+		bin_cap = bin_capacity_log2 > 0 ? (1u << std::min(bin_capacity_log2, 30))
+										: std::max(1u << 16, (unsigned)std::min<unsigned long long>(next_pow2(4 * want), 1ull << 28));
+		bin_keys.alloc((size_t)bin_cap * sizeof(mb_key128));
+		bin_vals.alloc((size_t)bin_cap * sizeof(long long));
+		MB_CUDA(cudaMemsetAsync(bin_keys.p, 0, bin_keys.bytes, s));
+		MB_CUDA(cudaMemsetAsync(bin_vals.p, 0, bin_vals.bytes, s));
+	}
+	if ((sections & 1u) && wide)
+	{
+		h.alloc(n_windows * sizeof(long long));
+		MB_CUDA(cudaMemsetAsync(h.p, 0, h.bytes, s));
+	}
+	else if (sections & 1u)
 	{
 		if (discrete)
 		{
@@ -426,7 +455,7 @@ void stats_state::init(module& m, float tick, float tmax, bool discrete, const s
 		h.alloc(n_windows * sizeof(long long));
 		MB_CUDA(cudaMemsetAsync(h.p, 0, h.bytes, s));
 	}
-	if (sections & 2u)
+	if ((sections & 2u) && !wide)
 	{
 		fin.alloc(n_bins * sizeof(unsigned));
 		MB_CUDA(cudaMemsetAsync(fin.p, 0, fin.bytes, s));
@@ -461,12 +490,16 @@ void stats_state::init(module& m, float tick, float tmax, bool discrete, const s
 	p.fp_counts = fp_counts.as<unsigned>();
 	p.fp_states = fp_states.as<unsigned>();
 	p.fp_mask = fp_cap ? fp_cap - 1 : 0;
+	p.bin_keys = bin_keys.as<mb_key128>();
+	p.bin_vals = bin_vals.as<long long>();
+	p.bin_mask = bin_cap ? bin_cap - 1 : 0;
 	p.fp_overflow = fp_overflow_ctr();
+	p.bin_overflow = bin_overflow_ctr();
 }
 
 void stats_state::zero(cudaStream_t s)
 {
-	for (dbuf* b : { &occ, &cnt, &h, &fin, &fp_keys, &fp_counts, &counters })
+	for (dbuf* b : { &occ, &cnt, &h, &fin, &fp_keys, &fp_counts, &counters, &bin_keys, &bin_vals })
 		if (b->p)
 			MB_CUDA(cudaMemsetAsync(b->p, 0, b->bytes, s));
 }
@@ -499,8 +532,8 @@ void stats_state::final_batch(cudaStream_t s, int n, int stride, const unsigned*
 		throw engine_error(MB_ERR_INVALID, "these statistics were created without the final-state section");
 	if (n <= 0)
 		return;
-	unsigned* fc = p.final_cnt;
-	void* a[] = { &n, &stride, &last_states, &statuses, &fc };
+	mb_stats_params sp = p;
+	void* a[] = { &n, &stride, &last_states, &statuses, &sp };
 	launch(mod->final_epoch, (n + 255) / 256, 256, 0, s, a);
 }
 
@@ -533,8 +566,73 @@ std::unique_ptr<result> stats_state::finalize(long long n, cudaStream_t s)
 	r.fx = fx;
 	r.fx_h = fx_h;
 	r.sections = sections;
+	r.wide = wide;
 	const size_t cells = (size_t)n_windows * n_bins;
-	if ((sections & 1u) && discrete_time)
+	if (wide)
+	{
+		// compact the occupied bins on the device, then sort them (and merge any key that two
+		// concurrent first insertions stored twice) on the host
+		if (out_bin_keys.bytes != (size_t)bin_cap * sizeof(mb_key128))
+		{
+			out_bin_keys.alloc((size_t)bin_cap * sizeof(mb_key128));
+			out_bin_vals.alloc((size_t)bin_cap * sizeof(long long));
+		}
+		MB_CUDA(cudaMemsetAsync(bin_extract_ctr(), 0, sizeof(unsigned), s));
+		unsigned cap = bin_cap;
+		mb_key128* keys = p.bin_keys;
+		long long* vals = p.bin_vals;
+		unsigned* out_n = bin_extract_ctr();
+		mb_key128* ok = out_bin_keys.as<mb_key128>();
+		long long* ov = out_bin_vals.as<long long>();
+		void* args[] = { &cap, &keys, &vals, &out_n, &ok, &ov };
+		launch(m.bins_extract, (cap + 255) / 256, 256, 0, s, args);
+		unsigned nb = 0, ovf = 0;
+		MB_CUDA(cudaMemcpyAsync(&nb, bin_extract_ctr(), sizeof nb, cudaMemcpyDeviceToHost, s));
+		MB_CUDA(cudaMemcpyAsync(&ovf, bin_overflow_ctr(), sizeof ovf, cudaMemcpyDeviceToHost, s));
+		MB_CUDA(cudaStreamSynchronize(s));
+		std::vector<mb_key128> bk(nb);
+		std::vector<long long> bv(nb);
+		if (nb)
+		{
+			MB_CUDA(cudaMemcpy(bk.data(), ok, nb * sizeof(mb_key128), cudaMemcpyDeviceToHost));
+			MB_CUDA(cudaMemcpy(bv.data(), ov, nb * sizeof(long long), cudaMemcpyDeviceToHost));
+		}
+		std::map<std::pair<int, unsigned __int128>, long long> bins;
+		for (unsigned i = 0; i < nb; i++)
+		{
+			const int w = (int)(bk[i].hi >> 48) - 1;
+			const unsigned __int128 idx = ((unsigned __int128)(bk[i].hi & 0xffffffffffffull) << 64) | bk[i].lo;
+			bins[{ w, idx }] += bv[i];
+		}
+		r.sp_begin.assign(n_windows + 1, 0);
+		for (auto& [key, v] : bins)
+		{
+			if (key.first < n_windows)
+			{
+				r.sp_w.push_back(key.first);
+				r.sp_idx.push_back(key.second);
+				r.sp_val.push_back(v);
+			}
+			else
+			{
+				r.fin_idx.push_back(key.second);
+				r.fin_cnt.push_back((unsigned)v);
+			}
+		}
+		for (int w = 0, e = 0; w <= n_windows; w++)
+		{
+			while (e < (int)r.sp_w.size() && r.sp_w[e] < w)
+				e++;
+			r.sp_begin[w] = e;
+		}
+		r.bin_overflow = ovf;
+	}
+	if ((sections & 1u) && wide)
+	{
+		r.win_h.resize(n_windows);
+		MB_CUDA(cudaMemcpyAsync(r.win_h.data(), h.p, n_windows * sizeof(long long), cudaMemcpyDeviceToHost, s));
+	}
+	else if ((sections & 1u) && discrete_time)
 	{
 		r.win_cnt.resize(cells);
 		MB_CUDA(cudaMemcpyAsync(r.win_cnt.data(), cnt.p, cells * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
@@ -549,7 +647,7 @@ std::unique_ptr<result> stats_state::finalize(long long n, cudaStream_t s)
 		r.win_h.resize(n_windows);
 		MB_CUDA(cudaMemcpyAsync(r.win_h.data(), h.p, n_windows * sizeof(long long), cudaMemcpyDeviceToHost, s));
 	}
-	if (sections & 2u)
+	if ((sections & 2u) && !wide)
 	{
 		r.final_cnt.resize(n_bins);
 		MB_CUDA(cudaMemcpyAsync(r.final_cnt.data(), fin.p, n_bins * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
@@ -642,10 +740,21 @@ std::unique_ptr<result> merge_results(const std::vector<const result*>& parts)
 	r.win_cnt.assign(a.win_cnt.size(), 0);
 	r.win_h.assign(a.win_h.size(), 0);
 	r.final_cnt.assign(a.final_cnt.size(), 0);
+	r.wide = a.wide;
+	r.bin_overflow = 0;
 	std::map<std::vector<unsigned>, unsigned long long> fixed;
+	std::map<std::pair<int, unsigned __int128>, long long> bins;
+	std::map<unsigned __int128, unsigned long long> finals;
 	for (const result* p : parts)
 	{
 		const result& b = *p;
+		if (b.wide != a.wide)
+			throw engine_error(MB_ERR_INVALID, "merge: the results are not shards of the same run");
+		for (size_t i = 0; i < b.sp_w.size(); i++)
+			bins[{ b.sp_w[i], b.sp_idx[i] }] += b.sp_val[i];
+		for (size_t i = 0; i < b.fin_idx.size(); i++)
+			finals[b.fin_idx[i]] += b.fin_cnt[i];
+		r.bin_overflow += b.bin_overflow;
 		if (b.state_size != a.state_size || b.n_windows != a.n_windows || b.n_bins != a.n_bins ||
 			b.discrete_time != a.discrete_time || b.time_tick != a.time_tick || b.max_time != a.max_time ||
 			b.noninternal_nodes != a.noninternal_nodes || b.sections != a.sections)
@@ -679,6 +788,27 @@ std::unique_ptr<result> merge_results(const std::vector<const result*>& parts)
 		cn.push_back((unsigned)count);
 	}
 	set_fixed_sorted(r, st, cn);
+	if (r.wide)
+	{
+		for (auto& [key, v] : bins)
+		{
+			r.sp_w.push_back(key.first);
+			r.sp_idx.push_back(key.second);
+			r.sp_val.push_back(v);
+		}
+		for (auto& [idx, c] : finals)
+		{
+			r.fin_idx.push_back(idx);
+			r.fin_cnt.push_back((unsigned)c);
+		}
+		r.sp_begin.assign(r.n_windows + 1, 0);
+		for (int w = 0, e = 0; w <= r.n_windows; w++)
+		{
+			while (e < (int)r.sp_w.size() && r.sp_w[e] < w)
+				e++;
+			r.sp_begin[w] = e;
+		}
+	}
 	return out;
 }
 
@@ -903,7 +1033,7 @@ runner::runner(module& m, const run_config& c) : mod(&m), cfg(c)
 	if (c.stats_trajectories < 0 || (c.stats_trajectories > 0 && c.stats_trajectories < c.sample_count))
 		throw engine_error(MB_ERR_INVALID, "stats_trajectories must be 0 or at least sample_count");
 	st.init(m, c.time_tick, c.max_time, c.discrete_time, c.noninternal_nodes, c.sample_count, c.fixed_capacity_log2, s,
-			7u, c.stats_trajectories);
+			7u, c.stats_trajectories, c.bin_capacity_log2);
 	st.set_istate(c.istate, s);
 	if (c.mode == MB_MODE_FUSED_EXACT && c.sample_count > 0 && c.sample_count <= max_rng_states)
 		rng.alloc((size_t)c.sample_count * sizeof(curandState));
@@ -1010,7 +1140,8 @@ bool same_run(const run_config& a, const run_config& b)
 		   a.max_time == b.max_time && a.time_tick == b.time_tick && a.discrete_time == b.discrete_time &&
 		   a.istate == b.istate && a.noninternal_nodes == b.noninternal_nodes && a.traj_len == b.traj_len &&
 		   a.batch_limit == b.batch_limit && a.block == b.block && a.blocks_per_sm == b.blocks_per_sm &&
-		   a.fixed_capacity_log2 == b.fixed_capacity_log2 && a.stats_trajectories == b.stats_trajectories;
+		   a.fixed_capacity_log2 == b.fixed_capacity_log2 && a.stats_trajectories == b.stats_trajectories &&
+		   a.bin_capacity_log2 == b.bin_capacity_log2;
 }
 
 std::unique_ptr<result> run(module& m, const run_config& c)

@@ -94,6 +94,7 @@ struct module
 	CUfunction init_random = nullptr, init_state = nullptr, sim_epoch = nullptr, sim_epoch_dense = nullptr;
 	CUfunction window_epoch = nullptr, final_epoch = nullptr, fixed_epoch = nullptr;
 	CUfunction compact_count = nullptr, compact_scan = nullptr, compact_scatter = nullptr, fixed_extract = nullptr;
+	CUfunction bins_extract = nullptr;
 
 	void ensure(int family);		// compile + load a family if needed (thread-safe)
 	void ensure_any();				// at least one family (the shared statistics kernels)
@@ -139,6 +140,7 @@ struct run_config
 	int blocks_per_sm = 0;			 // 0 = occupancy calculator
 	int fixed_capacity_log2 = 0;	 // 0 = automatic
 	long long stats_trajectories = 0; // trajectory count the fixed-point scales are chosen for (0 = sample_count)
+	int bin_capacity_log2 = 0;		  // sparse bins (more than 20 non-internal nodes): table size, 0 = automatic
 };
 
 run_config config_from_layout(const model_layout& L, int mode);
@@ -161,6 +163,17 @@ struct result
 	unsigned fixed_overflow = 0;
 	unsigned rate_errors = 0; // trajectories stopped on a non-finite total rate
 	unsigned sections = 7;	  // statistics present: 1 windows, 2 final states, 4 fixed points
+	// more than 20 non-internal nodes: sparse window bins (sorted by window, then index; sp_begin[w]
+	// is the first entry of window w) and sparse final states (sorted by index); n_bins is 0
+	bool wide = false;
+	std::vector<int> sp_w;
+	std::vector<unsigned __int128> sp_idx;
+	std::vector<long long> sp_val; // occupancy in fixed point (continuous) or count (discrete)
+	std::vector<size_t> sp_begin;  // [n_windows + 1]
+	std::vector<unsigned __int128> fin_idx;
+	std::vector<unsigned> fin_cnt;
+	unsigned bin_overflow = 0; // bin additions that found no slot in the table (lost)
+	double sparse_prob(size_t i) const; // probability of window entry i
 	unsigned long long transitions = 0;
 	float kernel_ms = 0; // device time of the simulation kernels
 	float total_ms = 0;	 // device time of the whole run (setup + kernels + result copies)
@@ -189,6 +202,9 @@ struct stats_state
 	module* mod = nullptr;
 	dbuf occ, cnt, h, fin, fp_keys, fp_counts, fp_states, counters, istate;
 	dbuf out_counts, out_states; // compacted fixed points (finalize)
+	dbuf bin_keys, bin_vals, out_bin_keys, out_bin_vals; // sparse bins (more than 20 non-internal nodes)
+	unsigned bin_cap = 0;
+	bool wide = false;
 	unsigned fp_cap = 0;
 	int n_windows = 0;
 	unsigned n_bins = 0;
@@ -202,7 +218,8 @@ struct stats_state
 
 	void init(module& m, float time_tick, float max_time, bool discrete, const std::vector<int>& noninternal,
 			  long long n_traj, int fixed_capacity_log2, cudaStream_t s, unsigned sections = 7,
-			  long long scale_traj = 0); // scale_traj: trajectories the fixed-point scales are chosen for (0 = n_traj)
+			  long long scale_traj = 0, // trajectories the fixed-point scales are chosen for (0 = n_traj)
+			  int bin_capacity_log2 = 0);
 	void zero(cudaStream_t s); // clear every accumulator (asynchronous)
 	void set_istate(const std::vector<float>& istate, cudaStream_t s);
 	size_t h_smem() const { return h_in_smem ? (size_t)n_windows * sizeof(long long) : 0; }
@@ -217,6 +234,8 @@ struct stats_state
 	unsigned* fp_overflow_ctr() const { return counters.as<unsigned>() + 4; }
 	unsigned* extract_ctr() const { return counters.as<unsigned>() + 5; }
 	unsigned* error_ctr() const { return counters.as<unsigned>() + 6; }
+	unsigned* bin_overflow_ctr() const { return counters.as<unsigned>() + 7; }
+	unsigned* bin_extract_ctr() const { return counters.as<unsigned>() + 8; }
 	// copy everything back (synchronises the stream)
 	std::unique_ptr<result> finalize(long long n_traj, cudaStream_t s);
 };

@@ -25,6 +25,7 @@ class RunConfig(C.Structure):
         ("blocks_per_sm", C.c_int),
         ("fixed_capacity_log2", C.c_int),
         ("stats_trajectories", C.c_longlong),
+        ("bin_capacity_log2", C.c_int),
     ]
 
 
@@ -184,7 +185,8 @@ class Module:
 
     def config(self, mode: str = "exact", sample_count: int | None = None, seed: int | None = None,
                first_traj: int = 0, traj_len: int = 100, batch_limit: int = 1_000_000, block: int = 256,
-               blocks_per_sm: int = 0, fixed_capacity_log2: int = 0, stats_trajectories: int = 0) -> RunConfig:
+               blocks_per_sm: int = 0, fixed_capacity_log2: int = 0, stats_trajectories: int = 0,
+               bin_capacity_log2: int = 0) -> RunConfig:
         cfg = RunConfig()
         check(lib().mb_run_config_default(self.model._h, C.byref(cfg)))
         cfg.mode = MODES[mode]
@@ -199,6 +201,7 @@ class Module:
         cfg.blocks_per_sm = blocks_per_sm
         cfg.fixed_capacity_log2 = fixed_capacity_log2
         cfg.stats_trajectories = stats_trajectories
+        cfg.bin_capacity_log2 = bin_capacity_log2
         return cfg
 
     def autotune(self, mode: str = "fast", sample_count: int | None = None, **kw) -> dict:
@@ -526,6 +529,29 @@ class Result:
         h_out = C.c_void_p()
         check(lib().mb_result_create(C.byref(d), C.byref(h_out)))
         return cls(h_out)
+
+    @property
+    def is_sparse(self) -> bool:
+        """More than 20 non-internal nodes: windows and final states as sparse entries."""
+        return self.dims.bins == 0 and self.dims.noninternal > 20
+
+    def sparse(self) -> dict:
+        """mb_result_sparse_*: window entries (window, state, raw sum, probability) sorted by window then
+        state, final states and counts, and the number of bin additions lost to a full table. States are
+        non-internal indices as (bits 0-63, bits 64-127) uint64 pairs."""
+        nw, nf, ovf = C.c_longlong(), C.c_longlong(), C.c_uint()
+        check(lib().mb_result_sparse_size(self._h, C.byref(nw), C.byref(nf), C.byref(ovf)))
+        w = np.zeros(max(1, nw.value), np.int32)
+        st = np.zeros((max(1, nw.value), 2), np.uint64)
+        raw = np.zeros(max(1, nw.value), np.int64)
+        pr = np.zeros(max(1, nw.value), np.float64)
+        check(lib().mb_result_sparse_windows(self._h, w.ctypes.data, st.ctypes.data, raw.ctypes.data, pr.ctypes.data))
+        fs = np.zeros((max(1, nf.value), 2), np.uint64)
+        fc = np.zeros(max(1, nf.value), np.uint32)
+        check(lib().mb_result_sparse_final(self._h, fs.ctypes.data, fc.ctypes.data))
+        n, m = nw.value, nf.value
+        return dict(windows=w[:n], states=st[:n], raw=raw[:n], probs=pr[:n], final_states=fs[:m],
+                    final_counts=fc[:m], overflow=ovf.value)
 
     def write_csv(self, model: Model, prefix: str) -> None:
         check(lib().mb_result_write_csv(self._h, model._h, prefix.encode()))

@@ -729,11 +729,11 @@ struct compiled
 		return (float)r.get();
 	}
 
-	uint32_t ni_index(const uint32_t* s) const
+	unsigned __int128 ni_index(const uint32_t* s) const
 	{
-		uint32_t idx = 0;
+		unsigned __int128 idx = 0;
 		for (size_t k = 0; k < ni.size(); k++)
-			idx |= ((s[ni[k] / 32] >> (ni[k] % 32)) & 1u) << k;
+			idx |= (unsigned __int128)((s[ni[k] / 32] >> (ni[k] % 32)) & 1u) << k;
 		return idx;
 	}
 };
@@ -903,6 +903,11 @@ struct sinks
 	std::vector<unsigned> cnt, fin;
 	std::map<std::vector<uint32_t>, unsigned, state_less> fixed;
 	unsigned long long transitions = 0;
+	// sparse bins (more than 20 non-internal nodes, or forced): (window, index) -> occupancy or count,
+	// and index -> final count, merged from the threads' maps at the end of a run
+	bool sparse = false;
+	std::map<std::pair<int, unsigned __int128>, long long> sp;
+	std::map<unsigned __int128, unsigned long long> sp_fin;
 };
 
 template <typename T>
@@ -914,23 +919,61 @@ void atomic_add(T* p, T v)
 struct run_acc
 {
 	int ow = -1;
-	uint32_t oi = 0;
+	unsigned __int128 oi = 0;
 	long long oq = 0;
 	int hw = -1;
 	long long hq = 0;
+	std::map<std::pair<int, unsigned __int128>, long long> sp; // this thread's sparse bins
+	std::map<unsigned __int128, unsigned long long> sp_fin;
+	void add_occ(sinks& s, int w, unsigned __int128 idx, long long q)
+	{
+		if (s.sparse)
+			sp[{ w, idx }] += q;
+		else
+			atomic_add(&s.occ[(size_t)w * s.S + idx], q);
+	}
+	void add_cnt(sinks& s, int w, unsigned __int128 idx)
+	{
+		if (s.sparse)
+			sp[{ w, idx }] += 1;
+		else
+			atomic_add(&s.cnt[(size_t)w * s.S + idx], 1u);
+	}
+	void add_fin(sinks& s, unsigned __int128 idx)
+	{
+		if (s.sparse)
+			sp_fin[idx] += 1;
+		else
+			atomic_add(&s.fin[idx], 1u);
+	}
 	void flush(sinks& s)
 	{
 		if (ow >= 0 && oq)
-			atomic_add(&s.occ[(size_t)ow * s.S + oi], oq);
+			add_occ(s, ow, oi, oq);
 		if (hw >= 0 && hq)
 			atomic_add(&s.h[hw], hq);
 		ow = hw = -1;
 		oq = hq = 0;
 	}
+	// the thread's sparse bins into the run's (after flush)
+	void merge(sinks& s)
+	{
+		if (!s.sparse)
+			return;
+#pragma omp critical(oracle_sparse)
+		{
+			for (auto& kv : sp)
+				s.sp[kv.first] += kv.second;
+			for (auto& kv : sp_fin)
+				s.sp_fin[kv.first] += kv.second;
+		}
+		sp.clear();
+		sp_fin.clear();
+	}
 };
 
 // window_average_small.cu:66-92 (continuous) and :117-130 (discrete)
-void record(const compiled& c, sinks& s, run_acc& a, uint32_t idx, float t0, float t1, float h)
+void record(const compiled& c, sinks& s, run_acc& a, unsigned __int128 idx, float t0, float t1, float h)
 {
 	if (t1 == 0.f)
 		return;
@@ -939,7 +982,7 @@ void record(const compiled& c, sinks& s, run_acc& a, uint32_t idx, float t0, flo
 		const int w = (int)lroundf(t0 / c.tick_f);
 		if (w >= 0 && w < s.T)
 		{
-			atomic_add(&s.cnt[(size_t)w * s.S + idx], 1u);
+			a.add_cnt(s, w, idx);
 			long long q = llrint((double)h * s.fxh);
 			if (q)
 				atomic_add(&s.h[w], q);
@@ -961,7 +1004,7 @@ void record(const compiled& c, sinks& s, run_acc& a, uint32_t idx, float t0, flo
 			else
 			{
 				if (a.ow >= 0 && a.oq)
-					atomic_add(&s.occ[(size_t)a.ow * s.S + a.oi], a.oq);
+					a.add_occ(s, a.ow, a.oi, a.oq);
 				a.ow = w;
 				a.oi = idx;
 				a.oq = q;
@@ -1120,7 +1163,7 @@ void trajectory_integer(const compiled& c, sinks& s, unsigned long long seed, un
 			trace->emplace_back(j, time);
 		st[j / 32] ^= 1u << (j % 32);
 	}
-	atomic_add(&s.fin[c.ni_index(st.data())], 1u);
+	acc.add_fin(s, c.ni_index(st.data()));
 	if (fixed)
 	{
 #pragma omp critical(oracle_fixed)
@@ -1201,7 +1244,7 @@ void trajectory(const compiled& c, sinks& s, RNG& rng, bool exact, int traj_len,
 			trace->emplace_back(idx, time);
 		st[idx / 32] ^= 1u << (idx % 32);
 	}
-	atomic_add(&s.fin[c.ni_index(st.data())], 1u);
+	acc.add_fin(s, c.ni_index(st.data()));
 	if (fixed)
 	{
 #pragma omp critical(oracle_fixed)
@@ -1307,24 +1350,28 @@ int oracle_model_noninternal(const oracle_model* m, int* out)
 float oracle_model_rate(const oracle_model* m, int i, const uint32_t* s) { return m->c->rate(i, s); }
 
 // Run n trajectories [first, first + n). Fixed-point exponents must be those of the GPU run.
-oracle_result* oracle_run(const oracle_model* m, int mode, long long n, unsigned long long seed,
-						  unsigned long long first, int traj_len, int occ_exp, int ent_exp, int threads)
+// flags: 1 = sparse bins even with at most 20 non-internal nodes (to pin the sparse path against
+// the dense one); more than 20 non-internal nodes (at most 112) always use sparse bins.
+oracle_result* oracle_run_ex(const oracle_model* m, int mode, long long n, unsigned long long seed,
+							 unsigned long long first, int traj_len, int occ_exp, int ent_exp, int threads, int flags)
 {
 	const compiled& c = *m->c;
-	if (c.ni.size() > 20)
+	if (c.ni.size() > 112)
 		return nullptr;
 	auto r = new oracle_result;
 	sinks& s = r->s;
 	s.T = c.T;
-	s.S = 1u << c.ni.size();
+	s.sparse = c.ni.size() > 20 || (flags & 1);
+	s.S = s.sparse ? 0u : 1u << c.ni.size();
 	s.fx = std::ldexp(1.0, occ_exp);
 	s.fxh = std::ldexp(1.0, ent_exp);
-	if (c.discrete)
+	if (!s.sparse && c.discrete)
 		s.cnt.assign((size_t)s.T * s.S, 0u);
-	else
+	else if (!s.sparse)
 		s.occ.assign((size_t)s.T * s.S, 0);
 	s.h.assign(s.T, 0);
-	s.fin.assign(s.S, 0u);
+	if (!s.sparse)
+		s.fin.assign(s.S, 0u);
 #ifdef _OPENMP
 	const double t0 = omp_get_wtime();
 	if (threads > 0)
@@ -1353,6 +1400,7 @@ oracle_result* oracle_run(const oracle_model* m, int mode, long long n, unsigned
 			}
 		}
 		acc.flush(s);
+		acc.merge(s);
 	}
 	s.transitions = trans;
 #ifdef _OPENMP
@@ -1366,7 +1414,46 @@ oracle_result* oracle_run(const oracle_model* m, int mode, long long n, unsigned
 	return r;
 }
 
+oracle_result* oracle_run(const oracle_model* m, int mode, long long n, unsigned long long seed,
+						  unsigned long long first, int traj_len, int occ_exp, int ent_exp, int threads)
+{
+	return oracle_run_ex(m, mode, n, seed, first, traj_len, occ_exp, ent_exp, threads, 0);
+}
+
 void oracle_result_free(oracle_result* r) { delete r; }
+
+// Sparse bins of a run: entry counts, then (window, index, value) sorted by window and index, and the
+// final states (index, count) sorted by index.
+int oracle_result_sparse_size(const oracle_result* r, long long* window_entries, long long* final_entries)
+{
+	*window_entries = (long long)r->s.sp.size();
+	*final_entries = (long long)r->s.sp_fin.size();
+	return r->s.sparse ? 1 : 0;
+}
+
+int oracle_result_sparse(const oracle_result* r, int* windows, uint64_t* idx, long long* vals, uint64_t* fin_idx,
+						 unsigned long long* fin_cnt)
+{
+	// indices as (bits 0-63, bits 64-127) pairs
+	size_t i = 0;
+	for (auto& kv : r->s.sp)
+	{
+		windows[i] = kv.first.first;
+		idx[2 * i] = (uint64_t)kv.first.second;
+		idx[2 * i + 1] = (uint64_t)(kv.first.second >> 64);
+		vals[i] = kv.second;
+		i++;
+	}
+	i = 0;
+	for (auto& kv : r->s.sp_fin)
+	{
+		fin_idx[2 * i] = (uint64_t)kv.first;
+		fin_idx[2 * i + 1] = (uint64_t)(kv.first >> 64);
+		fin_cnt[i] = kv.second;
+		i++;
+	}
+	return 0;
+}
 
 int oracle_result_get(const oracle_result* r, long long* occ, unsigned* cnt, long long* h, unsigned* fin,
 					  unsigned long long* transitions, double* seconds)
@@ -1406,7 +1493,8 @@ int oracle_trace(const oracle_model* m, int mode, unsigned long long seed, unsig
 	const compiled& c = *m->c;
 	sinks s;
 	s.T = c.T;
-	s.S = 1u << std::min<size_t>(c.ni.size(), 20);
+	s.sparse = c.ni.size() > 20;
+	s.S = s.sparse ? 0u : 1u << c.ni.size();
 	s.occ.assign((size_t)s.T * s.S, 0);
 	s.cnt.assign((size_t)s.T * s.S, 0);
 	s.h.assign(s.T, 0);

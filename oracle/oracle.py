@@ -40,6 +40,11 @@ def lib() -> C.CDLL:
         L.oracle_run.restype = C.c_void_p
         L.oracle_run.argtypes = [C.c_void_p, C.c_int, C.c_longlong, C.c_ulonglong, C.c_ulonglong, C.c_int,
                                  C.c_int, C.c_int, C.c_int]
+        L.oracle_run_ex.restype = C.c_void_p
+        L.oracle_run_ex.argtypes = [C.c_void_p, C.c_int, C.c_longlong, C.c_ulonglong, C.c_ulonglong, C.c_int,
+                                    C.c_int, C.c_int, C.c_int, C.c_int]
+        L.oracle_result_sparse_size.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        L.oracle_result_sparse.argtypes = [C.c_void_p] + [C.c_void_p] * 5
         L.oracle_result_free.argtypes = [C.c_void_p]
         L.oracle_result_get.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.POINTER(C.c_ulonglong), C.POINTER(C.c_double)]
@@ -109,19 +114,35 @@ class OracleModel:
 
     def run(self, n: int | None = None, mode: int = 0, seed: int | None = None, first: int = 0,
             traj_len: int = 100, occ_exp: int | None = None, ent_exp: int | None = None,
-            threads: int = 0) -> dict:
-        """Simulate trajectories [first, first+n) on the CPU. mode 0 = exact, 1 = fast."""
+            threads: int = 0, sparse: bool = False) -> dict:
+        """Simulate trajectories [first, first+n) on the CPU. mode 0 = exact, 1 = fast. With more than 20
+        non-internal nodes (or sparse=True) the windows and final states come back as sparse entries
+        under the key "sparse" (the dense arrays are then empty; states as (bits 0-63, bits 64-127) pairs)."""
         n = self.sample_count if n is None else n
         seed = self.seed if seed is None else seed
         if occ_exp is None:
             occ_exp = occupancy_exponent(n, self.tick, self.discrete)
         if ent_exp is None:
             ent_exp = entropy_exponent(n, self.tick, self.discrete)
-        r = lib().oracle_run(self._h, mode, n, seed, first, traj_len, occ_exp, ent_exp, threads)
+        r = lib().oracle_run_ex(self._h, mode, n, seed, first, traj_len, occ_exp, ent_exp, threads,
+                                1 if sparse else 0)
         if not r:
-            raise ValueError("oracle: unsupported model (more than 20 non-internal nodes)")
+            raise ValueError("oracle: unsupported model (more than 112 non-internal nodes)")
         try:
-            S = 1 << self.k
+            nw, nf = C.c_longlong(), C.c_longlong()
+            is_sparse = lib().oracle_result_sparse_size(r, C.byref(nw), C.byref(nf)) == 1
+            sp = None
+            if is_sparse:
+                w = np.zeros(max(1, nw.value), np.int32)
+                ix = np.zeros((max(1, nw.value), 2), np.uint64)
+                val = np.zeros(max(1, nw.value), np.int64)
+                fi = np.zeros((max(1, nf.value), 2), np.uint64)
+                fc = np.zeros(max(1, nf.value), np.uint64)
+                lib().oracle_result_sparse(r, w.ctypes.data, ix.ctypes.data, val.ctypes.data, fi.ctypes.data,
+                                           fc.ctypes.data)
+                sp = dict(windows=w[:nw.value], states=ix[:nw.value], raw=val[:nw.value],
+                          final_states=fi[:nf.value], final_counts=fc[:nf.value])
+            S = 0 if is_sparse else 1 << self.k
             T = self.windows
             occ = np.zeros(T * S, np.int64)
             cnt = np.zeros(T * S, np.uint32)
@@ -130,18 +151,21 @@ class OracleModel:
             tr, secs = C.c_ulonglong(), C.c_double()
             lib().oracle_result_get(r, occ.ctypes.data, cnt.ctypes.data, h.ctypes.data, fin.ctypes.data,
                                     C.byref(tr), C.byref(secs))
-            nf = lib().oracle_result_num_fixed(r)
-            fs = np.zeros(max(1, nf) * self.words, np.uint32)
-            fc = np.zeros(max(1, nf), np.uint32)
-            lib().oracle_result_fixed(r, fs.ctypes.data, fc.ctypes.data)
+            nfx = lib().oracle_result_num_fixed(r)
+            fs = np.zeros(max(1, nfx) * self.words, np.uint32)
+            fcx = np.zeros(max(1, nfx), np.uint32)
+            lib().oracle_result_fixed(r, fs.ctypes.data, fcx.ctypes.data)
         finally:
             lib().oracle_result_free(r)
         out = dict(n=n, windows=T, bins=S, discrete=self.discrete, tick=self.tick,
                    occ=occ.reshape(T, S), cnt=cnt.reshape(T, S), h=h, final=fin,
-                   fixed_states=fs[: nf * self.words].reshape(nf, self.words), fixed_counts=fc[:nf],
-                   transitions=tr.value, seconds=secs.value, occ_exp=occ_exp, ent_exp=ent_exp)
+                   fixed_states=fs[: nfx * self.words].reshape(nfx, self.words), fixed_counts=fcx[:nfx],
+                   transitions=tr.value, seconds=secs.value, occ_exp=occ_exp, ent_exp=ent_exp, sparse=sp)
         out["probs"] = window_probs(out)
         out["th"] = window_th(out)
+        if sp is not None:
+            raw = sp["raw"].astype(np.float64)
+            sp["probs"] = raw / n if self.discrete else (raw / 2.0 ** occ_exp) / (n * float(np.float32(self.tick)))
         return out
 
     def trace(self, traj: int, mode: int = 0, seed: int | None = None, traj_len: int = 100, cap: int = 1 << 16):
