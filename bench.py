@@ -43,6 +43,9 @@ EXTRA_WORKLOADS = {
 WORKLOADS = {
     # name: (generator, kwargs, description)
     "c1": ("c1", {}, "10-node random network, 1e5 trajectories, max_time 5, tick 0.2"),
+    "c2": ("c2", {}, "100-node network, 20 % internal nodes (77 non-internal: sparse window bins), 1e6 trajectories, "
+                   "max_time 100, tick 1"),
+    "c2disc": ("c2", dict(discrete=True), "the same in discrete time"),
     "c2b": ("c2", dict(noninternal=20), "100-node network, 20 non-internal nodes, 1e6 trajectories, max_time 100"),
     "c3": ("c3", {}, "1000-node power-law network, 10 non-internal nodes, 1e6 trajectories, max_time 50, tick 0.5"),
     "c4": ("c4", {}, "50-node network with 40 rate parameters, 8 outputs, 1e6 trajectories"),
@@ -374,7 +377,7 @@ def run_ours(args) -> None:
         else:
             res = mod.run(mode=args.mode, sample_count=n, **launch_kw)
             e2e_trans += res.transitions
-        probs = res.window_probs  # host copy of the result
+        probs = res.sparse()["probs"] if res.is_sparse else res.window_probs  # host copy of the result
     barrier()
     e2e_s = time.perf_counter() - t
     e2e_time = torch.tensor([e2e_s], dtype=torch.float64, device=local)
@@ -384,7 +387,11 @@ def run_ours(args) -> None:
         dist.all_reduce(e2e_total, op=dist.ReduceOp.SUM)
     d = res.dims
     h2d = model.num_nodes * 4
-    d2h = d.windows * d.bins * 8 + d.windows * 8 + d.bins * 4 + len(res.fixed) * (4 * d.state_words + 4) + 64
+    if res.is_sparse:  # compacted bins: 16-byte key + 8-byte value each
+        sp = res.sparse()
+        d2h = (len(sp["raw"]) + len(sp["final_counts"])) * 24 + d.windows * 8 + len(res.fixed) * (4 * d.state_words + 4) + 64
+    else:
+        d2h = d.windows * d.bins * 8 + d.windows * 8 + d.bins * 4 + len(res.fixed) * (4 * d.state_words + 4) + 64
 
     if world > 1:
         dist.destroy_process_group()

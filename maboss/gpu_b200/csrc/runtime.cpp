@@ -590,34 +590,48 @@ std::unique_ptr<result> stats_state::finalize(long long n, cudaStream_t s)
 		MB_CUDA(cudaMemcpyAsync(&nb, bin_extract_ctr(), sizeof nb, cudaMemcpyDeviceToHost, s));
 		MB_CUDA(cudaMemcpyAsync(&ovf, bin_overflow_ctr(), sizeof ovf, cudaMemcpyDeviceToHost, s));
 		MB_CUDA(cudaStreamSynchronize(s));
+		// sorted on the device
 		std::vector<mb_key128> bk(nb);
 		std::vector<long long> bv(nb);
 		if (nb)
 		{
-			MB_CUDA(cudaMemcpy(bk.data(), ok, nb * sizeof(mb_key128), cudaMemcpyDeviceToHost));
-			MB_CUDA(cudaMemcpy(bv.data(), ov, nb * sizeof(long long), cudaMemcpyDeviceToHost));
+			dbuf sk((size_t)nb * sizeof(mb_key128)), sv((size_t)nb * sizeof(long long));
+			sort_bins(ok, ov, nb, sk.as<mb_key128>(), sv.as<long long>(), s);
+			MB_CUDA(cudaMemcpy(bk.data(), sk.p, nb * sizeof(mb_key128), cudaMemcpyDeviceToHost));
+			MB_CUDA(cudaMemcpy(bv.data(), sv.p, nb * sizeof(long long), cudaMemcpyDeviceToHost));
 		}
-		std::map<std::pair<int, unsigned __int128>, long long> bins;
+		struct bin
+		{
+			int w;
+			unsigned __int128 idx;
+			long long v;
+		};
+		std::vector<bin> bins(nb);
 		for (unsigned i = 0; i < nb; i++)
-		{
-			const int w = (int)(bk[i].hi >> 48) - 1;
-			const unsigned __int128 idx = ((unsigned __int128)(bk[i].hi & 0xffffffffffffull) << 64) | bk[i].lo;
-			bins[{ w, idx }] += bv[i];
-		}
+			bins[i] = { (int)(bk[i].hi >> 48) - 1,
+						((unsigned __int128)(bk[i].hi & 0xffffffffffffull) << 64) | bk[i].lo, bv[i] };
 		r.sp_begin.assign(n_windows + 1, 0);
-		for (auto& [key, v] : bins)
+		r.sp_w.reserve(nb);
+		r.sp_idx.reserve(nb);
+		r.sp_val.reserve(nb);
+		for (size_t i = 0; i < bins.size();)
 		{
-			if (key.first < n_windows)
+			size_t j = i;
+			long long v = 0;
+			for (; j < bins.size() && bins[j].w == bins[i].w && bins[j].idx == bins[i].idx; j++)
+				v += bins[j].v;
+			if (bins[i].w < n_windows)
 			{
-				r.sp_w.push_back(key.first);
-				r.sp_idx.push_back(key.second);
+				r.sp_w.push_back(bins[i].w);
+				r.sp_idx.push_back(bins[i].idx);
 				r.sp_val.push_back(v);
 			}
 			else
 			{
-				r.fin_idx.push_back(key.second);
+				r.fin_idx.push_back(bins[i].idx);
 				r.fin_cnt.push_back((unsigned)v);
 			}
+			i = j;
 		}
 		for (int w = 0, e = 0; w <= n_windows; w++)
 		{

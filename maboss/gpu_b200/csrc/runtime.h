@@ -115,6 +115,11 @@ void simulate_epoch(module& m, bool dense, cudaStream_t s, int n, int stride, in
 					float* last_times, void* rands, unsigned* traj_states, float* traj_times, float* traj_h,
 					unsigned char* statuses, unsigned long long* transitions);
 
+// Sorts n sparse-bin records by their 128-bit keys (window, then non-internal index) on the device
+// (sort.cu); synchronises the stream.
+void sort_bins(const mb_key128* keys, const long long* vals, unsigned n, mb_key128* out_keys, long long* out_vals,
+			   cudaStream_t s);
+
 // Stable partition of the CONTINUE trajectories of an epoch batch into another buffer set
 // (last_states SoA [word * stride + i], last_times, random states); the number kept is written to
 // the device word *kept. `scratch` holds partition_scratch_bytes(n) bytes.
