@@ -9,6 +9,8 @@
 //     --device D       CUDA device ordinal (default 0)
 //     --emit-code      print the generated CUDA source and exit (no GPU needed)
 //     --stats          print transitions and epochs to stderr
+//     --max-noninternal K  accept up to K non-internal nodes (default 20 as the reference; at most
+//                      112: above 20 the window statistics are sparse bins)
 //   MABOSS_DIAGS=1 prints the timer_stats scopes to stderr.
 #include <algorithm>
 #include <iostream>
@@ -86,8 +88,8 @@ void do_visualization(stats_composite& stats_runner, int sample_count, const std
 
 void usage()
 {
-	std::cout << "Usage: MaBoSS.GPU [--mode exact|fast|epoch] [--device D] [--emit-code] [--stats] [-o prefix] "
-				 "bnd_file cfg_file"
+	std::cout << "Usage: MaBoSS.GPU [--mode exact|fast|epoch] [--device D] [--emit-code] [--stats] "
+				 "[--max-noninternal K] [-o prefix] bnd_file cfg_file"
 			  << std::endl;
 }
 
@@ -97,7 +99,7 @@ int main(int argc, char** argv)
 {
 	std::vector<std::string> args(argv + 1, argv + argc);
 	std::string output_prefix, mode_name = "exact";
-	int device = 0;
+	int device = 0, max_noninternal = 20;
 	bool emit = false, print_stats = false;
 	std::vector<std::string> files;
 	for (size_t i = 0; i < args.size(); i++)
@@ -109,6 +111,8 @@ int main(int argc, char** argv)
 			mode_name = args[++i];
 		else if (a == "--device" && i + 1 < args.size())
 			device = std::stoi(args[++i]);
+		else if (a == "--max-noninternal" && i + 1 < args.size())
+			max_noninternal = std::stoi(args[++i]);
 		else if (a == "--emit-code")
 			emit = true;
 		else if (a == "--stats")
@@ -157,9 +161,10 @@ int main(int argc, char** argv)
 			node_names.push_back(node.name);
 
 		// src/main.cpp:142-146
-		if (noninternals_count > 20)
+		if (noninternals_count > std::min(max_noninternal, 112))
 		{
-			std::cerr << "This executable supports a maximum of 20 non-internal nodes." << std::endl;
+			std::cerr << "This executable supports a maximum of " << std::min(max_noninternal, 112)
+					  << " non-internal nodes." << std::endl;
 			return 1;
 		}
 

@@ -68,6 +68,9 @@ def test_cli_usage_and_limits(tmp_path):
     (tmp_path / "m.cfg").write_text("max_time = 1;\n")
     p = subprocess.run([CLI, str(tmp_path / "m.bnd"), str(tmp_path / "m.cfg")], capture_output=True, text=True)
     assert p.returncode == 1 and "maximum of 20 non-internal nodes" in p.stderr
+    code = subprocess.run([CLI, "--max-noninternal", "64", "--emit-code", str(tmp_path / "m.bnd"),
+                           str(tmp_path / "m.cfg")], capture_output=True, text=True)
+    assert code.returncode == 0 and "MBG_WIDE_INDEX" in code.stdout
 
 
 def test_cli_emits_the_generated_code():
