@@ -255,8 +255,7 @@ void emit_incremental_tables(std::ostream& ss, const model_layout& L)
 	};
 	ss << "#define MBG_INCREMENTAL 1" << std::endl;
 	ss << "constexpr int mbg_inc_rate_shift = " << t.rate_shift << ";" << std::endl;
-	emit_array(ss, "uint4", "mbg_inc_node", u4(t.node));
-	// (q_up, q_down) of every node alone: the flip selection scans these (8 bytes per node stay in L1)
+	// the node records split in two 8-byte tables: (q_up, q_down) of every node alone: the flip selection scans these (8 bytes per node stay in L1)
 	std::vector<unsigned> q2;
 	for (size_t i = 0; i + 3 < t.node.size(); i += 4)
 	{
@@ -264,6 +263,15 @@ void emit_incremental_tables(std::ostream& ss, const model_layout& L)
 		q2.push_back(t.node[i + 1]);
 	}
 	emit_array(ss, "unsigned", "mbg_inc_q", q2);
+	// (first dependent record, dependents | (ni_pos + 1) << 16) of every node alone: a flip reads
+	// these 8 bytes (L1-resident) instead of the 16-byte node record
+	std::vector<unsigned> dep2;
+	for (size_t i = 0; i + 3 < t.node.size(); i += 4)
+	{
+		dep2.push_back(t.node[i + 2]);
+		dep2.push_back(t.node[i + 3]);
+	}
+	emit_array(ss, "unsigned", "mbg_inc_dep", dep2);
 	emit_array(ss, "uint4", "mbg_inc_rec_hdr", u4(t.hdr));
 	emit_array(ss, "uint4", "mbg_inc_rec_in", u4(t.in1));
 	emit_array(ss, "uint4", "mbg_inc_rec_in2", u4(t.in2));

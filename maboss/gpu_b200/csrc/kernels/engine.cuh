@@ -548,12 +548,12 @@ __device__ __forceinline__ int mb_exact_flip(const mb_incr_view& v, int j, mb_id
 {
 	v.S(j >> 5) ^= 1u << (j & 31);
 	int lo = j >> 5;
-	const uint4 nj = __ldg(mbg_inc_node + j);
-	const int pj = (int)(nj.w >> 16) - 1;
+	const uint2 nj = __ldg(reinterpret_cast<const uint2*>(mbg_inc_dep) + j);
+	const int pj = (int)(nj.y >> 16) - 1;
 	if (pj >= 0)
 		idx ^= (mb_idx_t)1 << pj;
 	ni_changed |= pj >= 0;
-	const int d0 = (int)nj.z, d1 = d0 + (int)(nj.w & 0xffffu);
+	const int d0 = (int)nj.x, d1 = d0 + (int)(nj.y & 0xffffu);
 	for (int d = d0; d < d1; d++)
 	{
 		const uint4 hdr = __ldg(mbg_inc_rec_hdr + d);
@@ -908,15 +908,15 @@ extern "C" __global__ void __launch_bounds__(128, 4) mb_fused_fast(mb_fused_para
 					cum += q;
 					um &= um - 1u;
 				}
-				const uint4 nj = __ldg(mbg_inc_node + j);
+				const uint2 nj = __ldg(reinterpret_cast<const uint2*>(mbg_inc_dep) + j);
 
 				// flip j and re-evaluate it and the nodes whose logic reads it
 				v.S(j >> 5) ^= 1u << (j & 31);
-				const int pj = (int)(nj.w >> 16) - 1;
+				const int pj = (int)(nj.y >> 16) - 1;
 				if (pj >= 0)
 					idx ^= (mb_idx_t)1 << pj;
 				bool ni_changed = pj >= 0;
-				const int d0 = (int)nj.z, d1 = d0 + (int)(nj.w & 0xffffu);
+				const int d0 = (int)nj.x, d1 = d0 + (int)(nj.y & 0xffffu);
 				// the dependents of one flip are distinct nodes: their records are evaluated
 				// independently, two at a time so that both records' loads are in flight together
 				auto dependent = [&](int d, const uint4& hdr, const uint4& in) {
