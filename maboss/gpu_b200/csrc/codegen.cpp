@@ -229,14 +229,17 @@ void emit_array(std::ostream& os, const char* type, const char* name, const std:
 	os << "};" << std::endl;
 }
 
-// Tables of the incremental fast-mode kernel (kernels/engine.cuh, MBG_INCREMENTAL), built by
-// build_incremental_tables:
+// Tables of the incremental kernels (kernels/engine.cuh, MBG_INCREMENTAL), built by
+// build_incremental_tables (the batched kernel uploads node/hdr/in1/in2 at run time):
 //   node[i]    = {q_up, q_down, first dependent record, dependents | (ni_pos + 1) << 16}
 //   hdr[r]     = {k | m << 16 | (ni_pos(k) + 1) << 21, q_up(k), q_down(k), truth table or offset}
 //   in1[r]     = inputs 0..7 of k's logic as 16-bit node indices, in2[r] = inputs 8..15
 //   self[i]    = the record of node i's own logic
-// The truth table of k is inline when it has at most 5 inputs (32 patterns), else an offset into
-// tt. Records keep everything one dependent re-evaluation needs in two 16-byte loads.
+// The NVRTC kernels read the same content in L1-sized pieces: mbg_inc_q (q_up, q_down) and
+// mbg_inc_dep (first record, dependents | ni) of every node in 8 bytes each, and one 16-byte record
+//   crec[r]    = {k | m << 16 | (ni_pos(k) + 1) << 21, truth table or offset, inputs 0-1, inputs 2-3}
+// with inputs 4..11 in cext[r], read only for logics of more than 4 inputs. The truth table of k is
+// inline when it has at most 5 inputs (32 patterns), else an offset into tt.
 void emit_incremental_tables(std::ostream& ss, const model_layout& L)
 {
 	ss << std::endl << "// ---- incremental engine tables" << std::endl;
@@ -272,9 +275,9 @@ void emit_incremental_tables(std::ostream& ss, const model_layout& L)
 		dep2.push_back(t.node[i + 3]);
 	}
 	emit_array(ss, "unsigned", "mbg_inc_dep", dep2);
-	emit_array(ss, "uint4", "mbg_inc_rec_hdr", u4(t.hdr));
-	emit_array(ss, "uint4", "mbg_inc_rec_in", u4(t.in1));
-	emit_array(ss, "uint4", "mbg_inc_rec_in2", u4(t.in2));
+	// 16-byte dependent records (the node's rates come from mbg_inc_q); inputs 4-11 apart
+	emit_array(ss, "uint4", "mbg_inc_crec", u4(t.crec));
+	emit_array(ss, "uint4", "mbg_inc_cext", u4(t.cext));
 	emit_array(ss, "unsigned", "mbg_inc_tt", t.tt);
 	emit_array(ss, "int", "mbg_inc_self", t.self);
 	// float rates (up, down) of every node as the generated rate functions return them (exact mode)
@@ -637,6 +640,9 @@ incremental_tables build_incremental_tables(const model_layout& L, const std::ve
 				in[x] = (unsigned)L.in_idx[a0 + x];
 			push4(t.in1, in[0] | in[1] << 16, in[2] | in[3] << 16, in[4] | in[5] << 16, in[6] | in[7] << 16);
 			push4(t.in2, in[8] | in[9] << 16, in[10] | in[11] << 16, in[12] | in[13] << 16, in[14] | in[15] << 16);
+			push4(t.crec, (unsigned)k | ((unsigned)m << 16) | ((unsigned)(ni_pos[k] + 1) << 21), ttw,
+				  in[0] | in[1] << 16, in[2] | in[3] << 16);
+			push4(t.cext, in[4] | in[5] << 16, in[6] | in[7] << 16, in[8] | in[9] << 16, in[10] | in[11] << 16);
 		}
 	}
 	if (t.tt.empty())

@@ -72,6 +72,9 @@ struct incremental_tables
 	int rate_shift = 0;
 	bool ok = false; // rates representable (every positive rate >= 2^10 units)
 	std::vector<unsigned> node, hdr, in1, in2; // uint4 records, 4 words each
+	// compact dependent records (the NVRTC kernels): {k | m << 16 | (ni_pos(k) + 1) << 21, truth
+	// table or offset, inputs 0-1, inputs 2-3}, and inputs 4-11 of records with more than 4 inputs
+	std::vector<unsigned> crec, cext;
 	std::vector<unsigned> tt;
 	std::vector<int> self;
 	std::vector<unsigned> q; // (q_up, q_down) per node

@@ -274,13 +274,13 @@ struct mb_incr_view
 };
 
 // Logic value of the node of dependent record `hdr`/`in` in the state held by view `v`.
-__device__ __forceinline__ bool mb_incr_logic(const mb_incr_view& v, int r, const uint4& hdr, const uint4& in)
+__device__ __forceinline__ bool mb_incr_logic(const mb_incr_view& v, int r, const uint4& rec)
 {
-	const int m = (hdr.x >> 16) & 31;
-	const unsigned ins[4] = { in.x, in.y, in.z, in.w };
+	const int m = (rec.x >> 16) & 31;
+	const unsigned ins[2] = { rec.z, rec.w };
 	unsigned p = 0;
 #pragma unroll
-	for (int t = 0; t < 8; t++)
+	for (int t = 0; t < 4; t++)
 	{
 		if (t < m)
 		{
@@ -288,21 +288,21 @@ __device__ __forceinline__ bool mb_incr_logic(const mb_incr_view& v, int r, cons
 			p |= ((v.S(node >> 5) >> (node & 31)) & 1u) << t;
 		}
 	}
-	if (m > 8)
+	if (m > 4)
 	{
-		const uint4 in2 = __ldg(mbg_inc_rec_in2 + r);
-		const unsigned ins2[4] = { in2.x, in2.y, in2.z, in2.w };
+		const uint4 ext = __ldg(mbg_inc_cext + r);
+		const unsigned ins2[4] = { ext.x, ext.y, ext.z, ext.w };
 #pragma unroll
-		for (int t = 8; t < 16; t++)
+		for (int t = 4; t < 12; t++)
 		{
 			if (t < m)
 			{
-				const unsigned node = (ins2[(t - 8) >> 1] >> ((t & 1) * 16)) & 0xffffu;
+				const unsigned node = (ins2[(t - 4) >> 1] >> ((t & 1) * 16)) & 0xffffu;
 				p |= ((v.S(node >> 5) >> (node & 31)) & 1u) << t;
 			}
 		}
 	}
-	const unsigned ttw = m <= 5 ? hdr.w : __ldg(mbg_inc_tt + hdr.w + (p >> 5));
+	const unsigned ttw = m <= 5 ? rec.y : __ldg(mbg_inc_tt + rec.y + (p >> 5));
 	return (ttw >> (p & 31)) & 1u;
 }
 
@@ -380,10 +380,11 @@ __device__ __forceinline__ void mb_incr_start(const mb_fused_params& P, const mb
 		if (i < state_size)
 		{
 			const int r = __ldg(mbg_inc_self + i);
-			const uint4 hdr = __ldg(mbg_inc_rec_hdr + r);
-			unstable = on != mb_incr_logic(v, r, hdr, __ldg(mbg_inc_rec_in + r));
-			q = unstable ? (on ? hdr.z : hdr.y) : 0u;
-			const int pos = (int)((hdr.x >> 21) & 127u) - 1;
+			const uint4 rec = __ldg(mbg_inc_crec + r);
+			unstable = on != mb_incr_logic(v, r, rec);
+			const uint2 qi = __ldg(reinterpret_cast<const uint2*>(mbg_inc_q) + i);
+			q = unstable ? (on ? qi.y : qi.x) : 0u;
+			const int pos = (int)((rec.x >> 21) & 127u) - 1;
 			nibit = (pos >= 0 && on) ? ((mb_idx_t)1 << pos) : (mb_idx_t)0;
 		}
 		const uint32_t um = __ballot_sync(0xffffffffu, unstable);
@@ -458,8 +459,8 @@ __device__ __forceinline__ mb_idx_t mb_exact_masks(const mb_incr_view& v, unsign
 			if (i < state_size)
 			{
 				const int r = __ldg(mbg_inc_self + i);
-				const uint4 hdr = __ldg(mbg_inc_rec_hdr + r);
-				unstable = on != mb_incr_logic(c, r, hdr, __ldg(mbg_inc_rec_in + r));
+				const uint4 hdr = __ldg(mbg_inc_crec + r);
+				unstable = on != mb_incr_logic(c, r, hdr);
 				const int pos = (int)((hdr.x >> 21) & 127u) - 1;
 				nibit = (pos >= 0 && on) ? ((mb_idx_t)1 << pos) : (mb_idx_t)0;
 			}
@@ -556,11 +557,11 @@ __device__ __forceinline__ int mb_exact_flip(const mb_incr_view& v, int j, mb_id
 	const int d0 = (int)nj.x, d1 = d0 + (int)(nj.y & 0xffffu);
 	for (int d = d0; d < d1; d++)
 	{
-		const uint4 hdr = __ldg(mbg_inc_rec_hdr + d);
+		const uint4 hdr = __ldg(mbg_inc_crec + d);
 		const int k = (int)(hdr.x & 0xffffu);
 		const uint32_t bk = 1u << (k & 31);
 		const bool on = (v.S(k >> 5) & bk) != 0;
-		const bool unstable = on != mb_incr_logic(v, d, hdr, __ldg(mbg_inc_rec_in + d));
+		const bool unstable = on != mb_incr_logic(v, d, hdr);
 		const uint32_t uw = v.U(k >> 5);
 		if (unstable != ((uw & bk) != 0))
 		{
@@ -919,17 +920,18 @@ extern "C" __global__ void __launch_bounds__(128, 4) mb_fused_fast(mb_fused_para
 				const int d0 = (int)nj.x, d1 = d0 + (int)(nj.y & 0xffffu);
 				// the dependents of one flip are distinct nodes: their records are evaluated
 				// independently, two at a time so that both records' loads are in flight together
-				auto dependent = [&](int d, const uint4& hdr, const uint4& in) {
-					const int k = (int)(hdr.x & 0xffffu);
+				auto dependent = [&](int d, const uint4& rec) {
+					const int k = (int)(rec.x & 0xffffu);
+					const uint2 qk = __ldg(q2 + k);
 					const int wk = k >> 5;
 					const uint32_t bk = 1u << (k & 31);
 					const bool on = (v.S(wk) & bk) != 0;
 					const bool was_on = (k == j) ? !on : on;
 					const uint32_t uw = v.U(wk);
 					const bool was_unstable = (uw & bk) != 0;
-					const bool unstable = on != mb_incr_logic(v, d, hdr, in);
-					const uint32_t qo = was_unstable ? (was_on ? hdr.z : hdr.y) : 0u;
-					const uint32_t qn = unstable ? (on ? hdr.z : hdr.y) : 0u;
+					const bool unstable = on != mb_incr_logic(v, d, rec);
+					const uint32_t qo = was_unstable ? (was_on ? qk.y : qk.x) : 0u;
+					const uint32_t qn = unstable ? (on ? qk.y : qk.x) : 0u;
 					if (unstable != was_unstable)
 						v.U(wk) = uw ^ bk;
 					if (qn != qo)
@@ -940,18 +942,16 @@ extern "C" __global__ void __launch_bounds__(128, 4) mb_fused_fast(mb_fused_para
 						total += (unsigned long long)dq;
 					}
 					if (qn != qo || unstable != was_unstable)
-						ni_changed |= ((hdr.x >> 21) & 127u) != 0u;
+						ni_changed |= ((rec.x >> 21) & 127u) != 0u;
 				};
 				for (int d = d0; d < d1; d += 2)
 				{
 					const bool two = d + 1 < d1;
-					const uint4 hdr0 = __ldg(mbg_inc_rec_hdr + d);
-					const uint4 in0 = __ldg(mbg_inc_rec_in + d);
-					const uint4 hdr1 = two ? __ldg(mbg_inc_rec_hdr + d + 1) : make_uint4(0u, 0u, 0u, 0u);
-					const uint4 in1 = two ? __ldg(mbg_inc_rec_in + d + 1) : make_uint4(0u, 0u, 0u, 0u);
-					dependent(d, hdr0, in0);
+					const uint4 rec0 = __ldg(mbg_inc_crec + d);
+					const uint4 rec1 = two ? __ldg(mbg_inc_crec + d + 1) : make_uint4(0u, 0u, 0u, 0u);
+					dependent(d, rec0);
 					if (two)
-						dependent(d + 1, hdr1, in1);
+						dependent(d + 1, rec1);
 				}
 				if (ni_changed)
 					h = mb_incr_entropy(v);
