@@ -77,10 +77,15 @@ int batch_engine::add_model(const model_t& m)
 	MB_CUDA(cudaSetDevice(ctx->device));
 	cudaStream_t s = ctx->stream;
 	const incremental_tables t = build_incremental_tables(L, L.up, L.down);
-	upload(net->node, t.node, s);
-	upload(net->hdr, t.hdr, s);
-	upload(net->in1, t.in1, s);
-	upload(net->in2, t.in2, s);
+	std::vector<unsigned> dep;
+	for (size_t i = 0; i + 3 < t.node.size(); i += 4)
+	{
+		dep.push_back(t.node[i + 2]);
+		dep.push_back(t.node[i + 3]);
+	}
+	upload(net->dep, dep, s);
+	upload(net->rec, t.crec, s);
+	upload(net->ext, t.cext, s);
 	upload(net->tt, t.tt, s);
 	upload(net->self, t.self, s);
 	upload(net->ni_node, L.noninternal_nodes, s);
@@ -175,10 +180,9 @@ batch_engine::prepared& batch_engine::prepare(bool grad)
 		d.discrete = L.discrete_time ? 1 : 0;
 		d.max_time = print6(L.max_time); // the generated code's 6-digit constants
 		d.tick = print6(L.time_tick);
-		d.node = N.node.as<uint4>();
-		d.hdr = N.hdr.as<uint4>();
-		d.in1 = N.in1.as<uint4>();
-		d.in2 = N.in2.as<uint4>();
+		d.dep = N.dep.as<uint2>();
+		d.rec = N.rec.as<uint4>();
+		d.ext = N.ext.as<uint4>();
 		d.tt = N.tt.as<unsigned>();
 		d.self = N.self.as<int>();
 		d.ni_node = N.ni_node.as<int>();
@@ -264,7 +268,7 @@ batch_engine::prepared& batch_engine::prepare(bool grad)
 	B.next = ps->counters.as<unsigned long long>();
 	B.errors = ps->counters.as<unsigned>() + 4;
 	ps->fn = grad ? (const void*)mb_batched_grad : (const void*)mb_batched_fast;
-	ps->smem_per_thread = (3 * (size_t)max_W + (grad ? 4 * (size_t)P : 0)) * 4;
+	ps->smem_per_thread = (3 * (size_t)max_W + (grad ? 5 * (size_t)P : 0)) * 4;
 	MB_CUDA(cudaStreamSynchronize(s));
 	slot = std::move(ps);
 	return *slot;

@@ -45,7 +45,7 @@ public:
 	{
 		model_t model;
 		model_layout L;
-		dbuf node, hdr, in1, in2, tt, self, ni_node;
+		dbuf dep, rec, ext, tt, self, ni_node;
 	};
 	struct variant
 	{

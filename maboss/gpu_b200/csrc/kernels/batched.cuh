@@ -22,10 +22,9 @@ struct mb_net
 {
 	int N, W, k, discrete;
 	float max_time, tick; // simulation constants (as the generated code of the network has them)
-	const uint4* node;	  // {-, -, first record, dependents | (ni_pos + 1) << 16}
-	const uint4* hdr;	  // {k | m << 16 | (ni_pos + 1) << 21, -, -, truth table or offset}
-	const uint4* in1;
-	const uint4* in2;
+	const uint2* dep;	  // per node: {first record, dependents | (ni_pos + 1) << 16}
+	const uint4* rec;	  // {k | m << 16 | (ni_pos + 1) << 21, truth table or offset, inputs 0-1, inputs 2-3}
+	const uint4* ext;	  // inputs 4-11 of records with more than 4 inputs
 	const unsigned* tt;
 	const int* self;
 	const int* ni_node; // [k]
@@ -71,10 +70,12 @@ struct mbb_lane
 	uint32_t* st;
 	uint32_t* un;
 	uint32_t* ws;
-	float* gS;	// [P] score at gT
-	float* gD;	// [P] d a0 / d theta
-	float* gT;	// [P] time of the last change of gD
+	// per gradient parameter p (continuous time: the score is S_p(t) = A_p - D_p t between changes)
+	float* gS;	// [P] A_p (continuous) or the score S_p (discrete)
+	float* gD;	// [P] D_p = d a0 / d theta_p of the current state
+	float* gT;	// [P] continuous: C1 at p's last change (C1 = sum over slices of c * length)
 	float* gG;	// [P] accumulated vector-Jacobian product of the trajectory
+	float* gC;	// [P] continuous: C2 at p's last change (C2 = sum over slices of c * length * midpoint)
 	int stride;
 	__device__ __forceinline__ uint32_t& S(int w) const { return st[w * stride]; }
 	__device__ __forceinline__ uint32_t& U(int w) const { return un[w * stride]; }
@@ -83,16 +84,16 @@ struct mbb_lane
 	__device__ __forceinline__ float& GD(int p) const { return gD[p * stride]; }
 	__device__ __forceinline__ float& GT(int p) const { return gT[p * stride]; }
 	__device__ __forceinline__ float& GG(int p) const { return gG[p * stride]; }
+	__device__ __forceinline__ float& GC(int p) const { return gC[p * stride]; }
 };
 
-__device__ __forceinline__ bool mbb_logic(const mb_net& net, const mbb_lane& v, int r, const uint4& hdr,
-										  const uint4& in)
+__device__ __forceinline__ bool mbb_logic(const mb_net& net, const mbb_lane& v, int r, const uint4& rec)
 {
-	const int m = (hdr.x >> 16) & 31;
-	const unsigned ins[4] = { in.x, in.y, in.z, in.w };
+	const int m = (rec.x >> 16) & 31;
+	const unsigned ins[2] = { rec.z, rec.w };
 	unsigned p = 0;
 #pragma unroll
-	for (int t = 0; t < 8; t++)
+	for (int t = 0; t < 4; t++)
 	{
 		if (t < m)
 		{
@@ -100,21 +101,21 @@ __device__ __forceinline__ bool mbb_logic(const mb_net& net, const mbb_lane& v, 
 			p |= ((v.S(node >> 5) >> (node & 31)) & 1u) << t;
 		}
 	}
-	if (m > 8)
+	if (m > 4)
 	{
-		const uint4 in2 = __ldg(net.in2 + r);
-		const unsigned ins2[4] = { in2.x, in2.y, in2.z, in2.w };
+		const uint4 ext = __ldg(net.ext + r);
+		const unsigned ins2[4] = { ext.x, ext.y, ext.z, ext.w };
 #pragma unroll
-		for (int t = 8; t < 16; t++)
+		for (int t = 4; t < 12; t++)
 		{
 			if (t < m)
 			{
-				const unsigned node = (ins2[(t - 8) >> 1] >> ((t & 1) * 16)) & 0xffffu;
+				const unsigned node = (ins2[(t - 4) >> 1] >> ((t & 1) * 16)) & 0xffffu;
 				p |= ((v.S(node >> 5) >> (node & 31)) & 1u) << t;
 			}
 		}
 	}
-	const unsigned ttw = m <= 5 ? hdr.w : __ldg(net.tt + hdr.w + (p >> 5));
+	const unsigned ttw = m <= 5 ? rec.y : __ldg(net.tt + rec.y + (p >> 5));
 	return (ttw >> (p & 31)) & 1u;
 }
 
@@ -147,44 +148,59 @@ __device__ __forceinline__ float mbb_entropy(const mb_net& net, const mb_variant
 }
 
 // d a_0 changes by `sign` times node k's rate derivatives in direction `dir` at time `now`
+// Continuous time, lazily: the slices recorded since parameter p last changed contribute
+// sum c * int (A_p - D_p t) dt = A_p (C1 - C1_p) - D_p (C2 - C2_p); this adds them and moves p's
+// checkpoints to the current sums, so a slice costs O(1) instead of O(P).
+__device__ __forceinline__ void mbb_grad_flush(const mbb_lane& v, int p, double C1, double C2)
+{
+	v.GG(p) += (float)((double)v.GS(p) * (C1 - (double)v.GT(p)) - (double)v.GD(p) * (C2 - (double)v.GC(p)));
+	v.GT(p) = (float)C1;
+	v.GC(p) = (float)C2;
+}
+
+// D_p of the parameters of node k's rate in direction dir changes by sign * d rate / d theta_p at
+// time `now`; continuous time keeps S_p(now) (A_p absorbs the change).
 __device__ __forceinline__ void mbb_grad_active(const mb_variant& var, const mbb_lane& v, int k, int dir, float sign,
-												float now, bool discrete)
+												float now, bool discrete, double C1, double C2)
 {
 	const int a = __ldg(var.g_ptr + 2 * k + dir), b = __ldg(var.g_ptr + 2 * k + dir + 1);
 	for (int e = a; e < b; e++)
 	{
 		const int p = __ldg(var.g_p + e);
+		const float dd = sign * __ldg(var.g_d + e);
 		if (!discrete)
 		{
-			v.GS(p) -= v.GD(p) * (now - v.GT(p));
-			v.GT(p) = now;
+			mbb_grad_flush(v, p, C1, C2);
+			v.GS(p) += dd * now;
 		}
-		v.GD(p) += sign * __ldg(var.g_d + e);
+		v.GD(p) += dd;
 	}
 }
 
-// the slice [u, w1] of window `w` in state `idx` contributes c * int S dt (continuous) or c * S (discrete)
+// the slice [u, w1] of window `w` in state `idx` contributes c * int S dt (continuous: into the
+// trajectory's running sums C1, C2) or c * S (discrete)
 __device__ __forceinline__ void mbb_grad_slice(const mb_variant& var, const mbb_lane& v, int P, int w, unsigned idx,
-											   float u, float w1, bool discrete)
+											   float u, float w1, bool discrete, double& C1, double& C2)
 {
 	const double c = var.cot[(size_t)w * var.st.n_bins + idx];
 	if (c == 0.0)
 		return;
-	const float cf = (float)c;
 	if (discrete)
 	{
+		const float cf = (float)c;
 		for (int p = 0; p < P; p++)
 			v.GG(p) += cf * v.GS(p);
 		return;
 	}
-	const float len = w1 - u, mid = 0.5f * (u + w1);
-	for (int p = 0; p < P; p++)
-		v.GG(p) += cf * len * (v.GS(p) - v.GD(p) * (mid - v.GT(p)));
+	const double len = (double)w1 - (double)u;
+	C1 += c * len;
+	C2 += c * len * 0.5 * ((double)u + (double)w1);
 }
 
 template <bool GRAD>
 __device__ __forceinline__ void mbb_record(const mb_variant& var, const mbb_lane& v, int P, mb_win_acc& acc,
-										   unsigned idx, float t0, float t1, float h, bool discrete, float tick)
+										   unsigned idx, float t0, float t1, float h, bool discrete, float tick,
+										   double& C1, double& C2)
 {
 	if (t1 == 0.f)
 		return;
@@ -195,7 +211,7 @@ __device__ __forceinline__ void mbb_record(const mb_variant& var, const mbb_lane
 		{
 			const int w = (int)lroundf(t0 / tick);
 			if (w >= 0 && w < var.st.n_windows)
-				mbb_grad_slice(var, v, P, w, idx, t0, t1, true);
+				mbb_grad_slice(var, v, P, w, idx, t0, t1, true, C1, C2);
 		}
 		return;
 	}
@@ -210,7 +226,7 @@ __device__ __forceinline__ void mbb_record(const mb_variant& var, const mbb_lane
 			const float we = (float)(w + 1) * tick;
 			const float se = fminf(t1, we);
 			if (w >= 0 && w < var.st.n_windows)
-				mbb_grad_slice(var, v, P, w, idx, sb, se, false);
+				mbb_grad_slice(var, v, P, w, idx, sb, se, false, C1, C2);
 			w++;
 			sb = se;
 		}
@@ -233,6 +249,8 @@ __device__ void mbb_body(const mb_batch_params& B)
 	v.gD = gbase + (size_t)P * bs + threadIdx.x;
 	v.gT = gbase + (size_t)2 * P * bs + threadIdx.x;
 	v.gG = gbase + (size_t)3 * P * bs + threadIdx.x;
+	v.gC = gbase + (size_t)4 * P * bs + threadIdx.x;
+	double C1 = 0.0, C2 = 0.0; // continuous-time gradient running sums of the lane's trajectory
 
 	mb_win_acc acc;
 	mb_acc_init(acc);
@@ -319,11 +337,11 @@ __device__ void mbb_body(const mb_batch_params& B)
 				if (i < net.N)
 				{
 					const int r = __ldg(net.self + i);
-					const uint4 hdr = __ldg(net.hdr + r);
-					unstable = on != mbb_logic(net, c, r, hdr, __ldg(net.in1 + r));
+					const uint4 rec = __ldg(net.rec + r);
+					unstable = on != mbb_logic(net, c, r, rec);
 					const uint2 qq = __ldg(var.q + i);
 					q = unstable ? (on ? qq.y : qq.x) : 0u;
-					const int pos = (int)((hdr.x >> 21) & 31u) - 1;
+					const int pos = (int)((rec.x >> 21) & 31u) - 1;
 					nibit = (pos >= 0 && on) ? (1u << pos) : 0u;
 				}
 				const uint32_t um = __ballot_sync(0xffffffffu, unstable);
@@ -365,12 +383,14 @@ __device__ void mbb_body(const mb_batch_params& B)
 			}
 			if (GRAD)
 			{
+				C1 = C2 = 0.0;
 				for (int p = 0; p < P; p++)
 				{
 					v.GS(p) = 0.f;
 					v.GD(p) = 0.f;
 					v.GT(p) = 0.f;
 					v.GG(p) = 0.f;
+					v.GC(p) = 0.f;
 				}
 				// d a0 / d theta of the initial state: every unstable node's active-direction derivatives
 				for (int w = 0; w < net.W; w++)
@@ -381,7 +401,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 					{
 						const int b = __ffs(um) - 1;
 						um &= um - 1u;
-						mbb_grad_active(var, v, 32 * w + b, (sw >> b) & 1u, 1.f, 0.f, net.discrete);
+						mbb_grad_active(var, v, 32 * w + b, (sw >> b) & 1u, 1.f, 0.f, net.discrete, C1, C2);
 					}
 				}
 			}
@@ -412,7 +432,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 				tn = fminf(tn, max_time);
 			}
 			trans += (tn != 0.f) ? 1ull : 0ull;
-			mbb_record<GRAD>(var, v, P, acc, idx, time, tn, total == 0 ? 0.f : h, discrete, var.st.win_tick);
+			mbb_record<GRAD>(var, v, P, acc, idx, time, tn, total == 0 ? 0.f : h, discrete, var.st.win_tick, C1, C2);
 			time = tn;
 			if (time >= max_time)
 			{
@@ -428,7 +448,11 @@ __device__ void mbb_body(const mb_batch_params& B)
 				}
 				if (GRAD)
 					for (int p = 0; p < P; p++)
+					{
+						if (!discrete)
+							mbb_grad_flush(v, p, C1, C2);
 						atomicAdd(var.grad + p, (double)v.GG(p));
+					}
 				atomicAdd(var.transitions, trans);
 				trans = 0;
 			}
@@ -480,7 +504,12 @@ __device__ void mbb_body(const mb_batch_params& B)
 					const float rj = __ldg(var.rate + 2 * j + jdir);
 					const int a = __ldg(var.g_ptr + 2 * j + jdir), b = __ldg(var.g_ptr + 2 * j + jdir + 1);
 					for (int e = a; e < b; e++)
-						v.GS(__ldg(var.g_p + e)) += __ldg(var.g_d + e) / rj;
+					{
+						const int p = __ldg(var.g_p + e);
+						if (!discrete)
+							mbb_grad_flush(v, p, C1, C2);
+						v.GS(p) += __ldg(var.g_d + e) / rj;
+					}
 					if (discrete)
 					{
 						const float a0 = (float)total * (1.0f / (float)(1u << var.rate_shift));
@@ -491,24 +520,23 @@ __device__ void mbb_body(const mb_batch_params& B)
 
 				// flip j and re-evaluate it and the nodes whose logic reads it
 				v.S(j >> 5) ^= 1u << (j & 31);
-				const uint4 nj = __ldg(net.node + j);
-				const int pj = (int)(nj.w >> 16) - 1;
+				const uint2 nj = __ldg(net.dep + j);
+				const int pj = (int)(nj.y >> 16) - 1;
 				if (pj >= 0)
 					idx ^= 1u << pj;
 				bool ni_changed = pj >= 0;
-				const int d0 = (int)nj.z, d1 = d0 + (int)(nj.w & 0xffffu);
+				const int d0 = (int)nj.x, d1 = d0 + (int)(nj.y & 0xffffu);
 				for (int d = d0; d < d1; d++)
 				{
-					const uint4 hdr = __ldg(net.hdr + d);
-					const uint4 in = __ldg(net.in1 + d);
-					const int k = (int)(hdr.x & 0xffffu);
+					const uint4 rec = __ldg(net.rec + d);
+					const int k = (int)(rec.x & 0xffffu);
 					const int wk = k >> 5;
 					const uint32_t bk = 1u << (k & 31);
 					const bool on = (v.S(wk) & bk) != 0;
 					const bool was_on = (k == j) ? !on : on;
 					const uint32_t uw = v.U(wk);
 					const bool was_unstable = (uw & bk) != 0;
-					const bool unstable = on != mbb_logic(net, v, d, hdr, in);
+					const bool unstable = on != mbb_logic(net, v, d, rec);
 					const uint2 qq = __ldg(var.q + k);
 					const uint32_t qo = was_unstable ? (was_on ? qq.y : qq.x) : 0u;
 					const uint32_t qn = unstable ? (on ? qq.y : qq.x) : 0u;
@@ -524,12 +552,12 @@ __device__ void mbb_body(const mb_batch_params& B)
 					if (GRAD && (unstable != was_unstable || on != was_on))
 					{
 						if (was_unstable)
-							mbb_grad_active(var, v, k, was_on ? 1 : 0, -1.f, time, discrete);
+							mbb_grad_active(var, v, k, was_on ? 1 : 0, -1.f, time, discrete, C1, C2);
 						if (unstable)
-							mbb_grad_active(var, v, k, on ? 1 : 0, 1.f, time, discrete);
+							mbb_grad_active(var, v, k, on ? 1 : 0, 1.f, time, discrete, C1, C2);
 					}
 					if (qn != qo || unstable != was_unstable)
-						ni_changed |= ((hdr.x >> 21) & 31u) != 0u;
+						ni_changed |= ((rec.x >> 21) & 31u) != 0u;
 				}
 				if (ni_changed)
 					h = mbb_entropy(net, var, v);
