@@ -268,7 +268,7 @@ batch_engine::prepared& batch_engine::prepare(bool grad)
 	B.next = ps->counters.as<unsigned long long>();
 	B.errors = ps->counters.as<unsigned>() + 4;
 	ps->fn = grad ? (const void*)mb_batched_grad : (const void*)mb_batched_fast;
-	ps->smem_per_thread = (3 * (size_t)max_W + (grad ? 5 * (size_t)P : 0)) * 4;
+	ps->smem_per_thread = (3 * (size_t)max_W + (grad ? 2 * (size_t)P : 0)) * 4;
 	MB_CUDA(cudaStreamSynchronize(s));
 	slot = std::move(ps);
 	return *slot;
@@ -307,6 +307,12 @@ void batch_engine::set_shape(prepared& ps, int block, int per_sm)
 	ps.smem = smem;
 	ps.grid = (unsigned)std::max<unsigned long long>(
 		1ull, std::min<unsigned long long>(needed, (unsigned long long)per_sm * ctx->sm_count));
+	// gradient runs: the lanes' global scratch (accumulated products and checkpoints, 3 P floats each)
+	ps.B->gstride = ps.grid * (unsigned)block;
+	const size_t gbytes = ps.grad ? (size_t)3 * ps.B->P * ps.B->gstride * sizeof(float) : 0;
+	if (ps.gscratch.bytes < gbytes)
+		ps.gscratch.alloc(gbytes);
+	ps.B->gmem = ps.gscratch.as<float>();
 	if (ps.exec)
 	{
 		cudaGraphExecDestroy(ps.exec);

@@ -106,7 +106,7 @@ private:
 		size_t smem_per_thread = 0, smem = 0;
 		int block = 0, per_sm = 0;
 		unsigned grid = 0;
-		dbuf counters;
+		dbuf counters, gscratch;
 		void* host = nullptr; // pinned
 		std::vector<host_off_t> host_off;
 		cudaEvent_t e0 = nullptr, e1 = nullptr;

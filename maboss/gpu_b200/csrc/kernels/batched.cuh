@@ -61,6 +61,8 @@ struct mb_batch_params
 	unsigned long long seed;
 	unsigned long long* next;
 	unsigned* errors;
+	float* gmem;		  // gradient runs: per-lane global scratch [3 P][gstride] (accumulated product,
+	unsigned gstride;	  // checkpoints C1, C2), gstride = the launch's thread count
 };
 
 constexpr int MBB_GROUPS = 16; // register group sums; words per group = ceil(W / 16)
@@ -70,21 +72,23 @@ struct mbb_lane
 	uint32_t* st;
 	uint32_t* un;
 	uint32_t* ws;
-	// per gradient parameter p (continuous time: the score is S_p(t) = A_p - D_p t between changes)
+	// per gradient parameter p (continuous time: the score is S_p(t) = A_p - D_p t between changes);
+	// A_p and D_p, read at every change, in shared memory; the rest in the lane's global scratch
 	float* gS;	// [P] A_p (continuous) or the score S_p (discrete)
 	float* gD;	// [P] D_p = d a0 / d theta_p of the current state
 	float* gT;	// [P] continuous: C1 at p's last change (C1 = sum over slices of c * length)
 	float* gG;	// [P] accumulated vector-Jacobian product of the trajectory
 	float* gC;	// [P] continuous: C2 at p's last change (C2 = sum over slices of c * length * midpoint)
-	int stride;
+	int stride;	 // shared-memory rows (block size)
+	unsigned gstride; // global-scratch rows (threads of the launch)
 	__device__ __forceinline__ uint32_t& S(int w) const { return st[w * stride]; }
 	__device__ __forceinline__ uint32_t& U(int w) const { return un[w * stride]; }
 	__device__ __forceinline__ uint32_t& Q(int w) const { return ws[w * stride]; }
 	__device__ __forceinline__ float& GS(int p) const { return gS[p * stride]; }
 	__device__ __forceinline__ float& GD(int p) const { return gD[p * stride]; }
-	__device__ __forceinline__ float& GT(int p) const { return gT[p * stride]; }
-	__device__ __forceinline__ float& GG(int p) const { return gG[p * stride]; }
-	__device__ __forceinline__ float& GC(int p) const { return gC[p * stride]; }
+	__device__ __forceinline__ float& GT(int p) const { return gT[(size_t)p * gstride]; }
+	__device__ __forceinline__ float& GG(int p) const { return gG[(size_t)p * gstride]; }
+	__device__ __forceinline__ float& GC(int p) const { return gC[(size_t)p * gstride]; }
 };
 
 __device__ __forceinline__ bool mbb_logic(const mb_net& net, const mbb_lane& v, int r, const uint4& rec)
@@ -247,9 +251,11 @@ __device__ void mbb_body(const mb_batch_params& B)
 	float* gbase = reinterpret_cast<float*>(mbb_smem + (size_t)3 * MW * bs);
 	v.gS = gbase + threadIdx.x;
 	v.gD = gbase + (size_t)P * bs + threadIdx.x;
-	v.gT = gbase + (size_t)2 * P * bs + threadIdx.x;
-	v.gG = gbase + (size_t)3 * P * bs + threadIdx.x;
-	v.gC = gbase + (size_t)4 * P * bs + threadIdx.x;
+	const unsigned gtid = blockIdx.x * bs + threadIdx.x;
+	v.gstride = B.gstride;
+	v.gG = B.gmem + gtid;
+	v.gT = B.gmem + (size_t)P * B.gstride + gtid;
+	v.gC = B.gmem + (size_t)2 * P * B.gstride + gtid;
 	double C1 = 0.0, C2 = 0.0; // continuous-time gradient running sums of the lane's trajectory
 
 	mb_win_acc acc;
@@ -570,4 +576,4 @@ __device__ void mbb_body(const mb_batch_params& B)
 }
 
 extern "C" __global__ void __launch_bounds__(128, 5) mb_batched_fast(mb_batch_params B) { mbb_body<false>(B); }
-extern "C" __global__ void __launch_bounds__(128) mb_batched_grad(mb_batch_params B) { mbb_body<true>(B); }
+extern "C" __global__ void __launch_bounds__(128, 4) mb_batched_grad(mb_batch_params B) { mbb_body<true>(B); }
