@@ -307,12 +307,12 @@ void batch_engine::set_shape(prepared& ps, int block, int per_sm)
 	ps.smem = smem;
 	ps.grid = (unsigned)std::max<unsigned long long>(
 		1ull, std::min<unsigned long long>(needed, (unsigned long long)per_sm * ctx->sm_count));
-	// gradient runs: the lanes' global scratch (accumulated products and checkpoints, 3 P floats each)
+	// gradient runs: the lanes' global scratch (partial products R_p, P doubles each)
 	ps.B->gstride = ps.grid * (unsigned)block;
-	const size_t gbytes = ps.grad ? (size_t)3 * ps.B->P * ps.B->gstride * sizeof(float) : 0;
+	const size_t gbytes = ps.grad ? (size_t)ps.B->P * ps.B->gstride * sizeof(double) : 0;
 	if (ps.gscratch.bytes < gbytes)
 		ps.gscratch.alloc(gbytes);
-	ps.B->gmem = ps.gscratch.as<float>();
+	ps.B->gmem = ps.gscratch.as<double>();
 	if (ps.exec)
 	{
 		cudaGraphExecDestroy(ps.exec);

@@ -61,8 +61,8 @@ struct mb_batch_params
 	unsigned long long seed;
 	unsigned long long* next;
 	unsigned* errors;
-	float* gmem;		  // gradient runs: per-lane global scratch [3 P][gstride] (accumulated product,
-	unsigned gstride;	  // checkpoints C1, C2), gstride = the launch's thread count
+	double* gmem;		  // gradient runs: per-lane global scratch [P][gstride] of partial products R_p,
+	unsigned gstride;	  // gstride = the launch's thread count
 };
 
 constexpr int MBB_GROUPS = 16; // register group sums; words per group = ceil(W / 16)
@@ -73,22 +73,19 @@ struct mbb_lane
 	uint32_t* un;
 	uint32_t* ws;
 	// per gradient parameter p (continuous time: the score is S_p(t) = A_p - D_p t between changes);
-	// A_p and D_p, read at every change, in shared memory; the rest in the lane's global scratch
-	float* gS;	// [P] A_p (continuous) or the score S_p (discrete)
-	float* gD;	// [P] D_p = d a0 / d theta_p of the current state
-	float* gT;	// [P] continuous: C1 at p's last change (C1 = sum over slices of c * length)
-	float* gG;	// [P] accumulated vector-Jacobian product of the trajectory
-	float* gC;	// [P] continuous: C2 at p's last change (C2 = sum over slices of c * length * midpoint)
-	int stride;	 // shared-memory rows (block size)
+	// A_p and D_p in shared memory, R_p in the lane's global scratch
+	float* gS;	 // [P] A_p (continuous) or the score S_p (discrete)
+	float* gD;	 // [P] D_p = d a0 / d theta_p of the current state
+	double* gR;	 // [P] continuous: sum over p's changes of dD * C2 - dA * C1; discrete: sum of c * S_p;
+				 // accumulates the lane's trajectories of one variant
+	int stride;		  // shared-memory rows (block size)
 	unsigned gstride; // global-scratch rows (threads of the launch)
 	__device__ __forceinline__ uint32_t& S(int w) const { return st[w * stride]; }
 	__device__ __forceinline__ uint32_t& U(int w) const { return un[w * stride]; }
 	__device__ __forceinline__ uint32_t& Q(int w) const { return ws[w * stride]; }
 	__device__ __forceinline__ float& GS(int p) const { return gS[p * stride]; }
 	__device__ __forceinline__ float& GD(int p) const { return gD[p * stride]; }
-	__device__ __forceinline__ float& GT(int p) const { return gT[(size_t)p * gstride]; }
-	__device__ __forceinline__ float& GG(int p) const { return gG[(size_t)p * gstride]; }
-	__device__ __forceinline__ float& GC(int p) const { return gC[(size_t)p * gstride]; }
+	__device__ __forceinline__ double& GR(int p) const { return gR[(size_t)p * gstride]; }
 };
 
 __device__ __forceinline__ bool mbb_logic(const mb_net& net, const mbb_lane& v, int r, const uint4& rec)
@@ -151,16 +148,10 @@ __device__ __forceinline__ float mbb_entropy(const mb_net& net, const mb_variant
 	return h > 0.f ? h : 0.f;
 }
 
-// d a_0 changes by `sign` times node k's rate derivatives in direction `dir` at time `now`
-// Continuous time, lazily: the slices recorded since parameter p last changed contribute
-// sum c * int (A_p - D_p t) dt = A_p (C1 - C1_p) - D_p (C2 - C2_p); this adds them and moves p's
-// checkpoints to the current sums, so a slice costs O(1) instead of O(P).
-__device__ __forceinline__ void mbb_grad_flush(const mbb_lane& v, int p, double C1, double C2)
-{
-	v.GG(p) += (float)((double)v.GS(p) * (C1 - (double)v.GT(p)) - (double)v.GD(p) * (C2 - (double)v.GC(p)));
-	v.GT(p) = (float)C1;
-	v.GC(p) = (float)C2;
-}
+// Continuous time, summed by parts: with the running sums C1 = sum c * length and
+// C2 = sum c * length * midpoint over the trajectory's slices, and A_p, D_p piecewise constant,
+//   sum over slices of c * int (A_p - D_p t) dt = A_p C1 - D_p C2 - sum over p's changes (dA C1 - dD C2),
+// each change's term taken at the sums of its time; a change costs one update of R_p and a slice O(1).
 
 // D_p of the parameters of node k's rate in direction dir changes by sign * d rate / d theta_p at
 // time `now`; continuous time keeps S_p(now) (A_p absorbs the change).
@@ -174,10 +165,36 @@ __device__ __forceinline__ void mbb_grad_active(const mb_variant& var, const mbb
 		const float dd = sign * __ldg(var.g_d + e);
 		if (!discrete)
 		{
-			mbb_grad_flush(v, p, C1, C2);
-			v.GS(p) += dd * now;
+			const float dA = dd * now;
+			v.GR(p) += (double)dd * C2 - (double)dA * C1;
+			v.GS(p) += dA;
 		}
 		v.GD(p) += dd;
+	}
+}
+
+// the lane's trajectory ends: its products join R_p (which then holds the sum over the lane's
+// trajectories) and the score restarts
+__device__ __forceinline__ void mbb_grad_end(const mbb_lane& v, int P, bool discrete, double C1, double C2)
+{
+	for (int p = 0; p < P; p++)
+	{
+		if (!discrete)
+			v.GR(p) += (double)v.GS(p) * C1 - (double)v.GD(p) * C2;
+		v.GS(p) = 0.f;
+		v.GD(p) = 0.f;
+	}
+}
+
+// R_p of the lane's trajectories of variant `var` into the variant's gradient
+__device__ __forceinline__ void mbb_grad_emit(const mb_variant& var, const mbb_lane& v, int P)
+{
+	for (int p = 0; p < P; p++)
+	{
+		const double g = v.GR(p);
+		if (g != 0.0)
+			atomicAdd(var.grad + p, g);
+		v.GR(p) = 0.0;
 	}
 }
 
@@ -193,7 +210,7 @@ __device__ __forceinline__ void mbb_grad_slice(const mb_variant& var, const mbb_
 	{
 		const float cf = (float)c;
 		for (int p = 0; p < P; p++)
-			v.GG(p) += cf * v.GS(p);
+			v.GR(p) += (double)(cf * v.GS(p));
 		return;
 	}
 	const double len = (double)w1 - (double)u;
@@ -251,12 +268,15 @@ __device__ void mbb_body(const mb_batch_params& B)
 	float* gbase = reinterpret_cast<float*>(mbb_smem + (size_t)3 * MW * bs);
 	v.gS = gbase + threadIdx.x;
 	v.gD = gbase + (size_t)P * bs + threadIdx.x;
-	const unsigned gtid = blockIdx.x * bs + threadIdx.x;
 	v.gstride = B.gstride;
-	v.gG = B.gmem + gtid;
-	v.gT = B.gmem + (size_t)P * B.gstride + gtid;
-	v.gC = B.gmem + (size_t)2 * P * B.gstride + gtid;
+	v.gR = GRAD ? B.gmem + blockIdx.x * bs + threadIdx.x : nullptr;
 	double C1 = 0.0, C2 = 0.0; // continuous-time gradient running sums of the lane's trajectory
+	for (int p = 0; p < P; p++)
+	{
+		v.GS(p) = 0.f;
+		v.GD(p) = 0.f;
+		v.GR(p) = 0.0;
+	}
 
 	mb_win_acc acc;
 	mb_acc_init(acc);
@@ -384,20 +404,16 @@ __device__ void mbb_body(const mb_batch_params& B)
 			if (acc_var != vi)
 			{
 				if (acc_var >= 0)
+				{
 					mb_acc_flush(acc, B.vars[acc_var].st, B.vars[acc_var].st.win_h);
+					if (GRAD)
+						mbb_grad_emit(B.vars[acc_var], v, P);
+				}
 				acc_var = vi;
 			}
 			if (GRAD)
 			{
 				C1 = C2 = 0.0;
-				for (int p = 0; p < P; p++)
-				{
-					v.GS(p) = 0.f;
-					v.GD(p) = 0.f;
-					v.GT(p) = 0.f;
-					v.GG(p) = 0.f;
-					v.GC(p) = 0.f;
-				}
 				// d a0 / d theta of the initial state: every unstable node's active-direction derivatives
 				for (int w = 0; w < net.W; w++)
 				{
@@ -453,12 +469,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 					mb_fixed_insert_rt(var.st, st, W);
 				}
 				if (GRAD)
-					for (int p = 0; p < P; p++)
-					{
-						if (!discrete)
-							mbb_grad_flush(v, p, C1, C2);
-						atomicAdd(var.grad + p, (double)v.GG(p));
-					}
+					mbb_grad_end(v, P, discrete, C1, C2);
 				atomicAdd(var.transitions, trans);
 				trans = 0;
 			}
@@ -512,9 +523,10 @@ __device__ void mbb_body(const mb_batch_params& B)
 					for (int e = a; e < b; e++)
 					{
 						const int p = __ldg(var.g_p + e);
+						const float dA = __ldg(var.g_d + e) / rj;
 						if (!discrete)
-							mbb_grad_flush(v, p, C1, C2);
-						v.GS(p) += __ldg(var.g_d + e) / rj;
+							v.GR(p) -= (double)dA * C1;
+						v.GS(p) += dA;
 					}
 					if (discrete)
 					{
@@ -572,7 +584,11 @@ __device__ void mbb_body(const mb_batch_params& B)
 		__syncwarp();
 	}
 	if (acc_var >= 0)
+	{
 		mb_acc_flush(acc, B.vars[acc_var].st, B.vars[acc_var].st.win_h);
+		if (GRAD)
+			mbb_grad_emit(B.vars[acc_var], v, P);
+	}
 }
 
 extern "C" __global__ void __launch_bounds__(128, 5) mb_batched_fast(mb_batch_params B) { mbb_body<false>(B); }

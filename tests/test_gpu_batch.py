@@ -102,13 +102,17 @@ def test_gradient_of_two_state_chain_matches_analytic(gpu):
     assert np.all(np.abs(mean - exact) < 4 * sem + 0.01 * np.abs(exact)), (mean, exact, sem)
 
 
-def test_gradient_matches_common_random_number_finite_differences(gpu):
+@pytest.mark.parametrize("discrete", [False, True], ids=["continuous", "discrete"])
+def test_gradient_matches_common_random_number_finite_differences(gpu, discrete):
     """C4-style network: score-function gradients of sum_w P_w(output node 0 on) against central
     finite differences with common random numbers (variants with the same random streams in one
     batched launch). Both are Monte-Carlo estimates: over 4 seeds, the means must agree within 4
     combined standard errors plus 2% of |FD|. The step is 1% of each parameter: with 1e3-fold
-    smaller steps the finite-difference noise at this sample size exceeds most of the gradients."""
+    smaller steps the finite-difference noise at this sample size exceeds most of the gradients.
+    Discrete time: one transition per tick, chosen with probability rate / a0."""
     bnd, cfg = synth.c4()
+    if discrete:
+        cfg += "\ndiscrete_time = 1;\n"
     model = mb.Model(bnd, cfg)
     names = [f"$u_{i}" for i in range(4)] + [f"$d_{i}" for i in range(4)]
     theta = {k: model.variable(k) for k in names}
