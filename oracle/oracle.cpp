@@ -17,6 +17,10 @@
 //
 // Modes: 0 = exact (reference semantics incl. the 100-slot epoch boundary), 1 = fast (Philox
 // streams, no epoch boundary, entropy via sum r*log2 r), mirroring the engine's two fused modes.
+//
+// Gradient: gradient_integer states the score-function gradient that the engine's batched gradient
+// kernel computes (the reference has no gradient) directly along the fast-mode trajectories; it is
+// pinned against exact derivatives of small chains solved in closed form (tests/test_oracle_gradient.py).
 #include <curand_kernel.h>
 
 #include <algorithm>
@@ -1171,6 +1175,134 @@ void trajectory_integer(const compiled& c, sinks& s, unsigned long long seed, un
 	}
 }
 
+// Score-function (likelihood-ratio) gradient of sum_w,b cot[w][b] * (window statistic) along the
+// trajectories of trajectory_integer (same Philox streams, integer rates, flips), stated directly:
+// the score of parameter p at time t is S_p(t) = J_p(t) - I_p(t), J_p the sum over the jumps so far
+// of (d rate_j / d theta_p) / rate_j and I_p the integral of d a0 / d theta_p, recomputed from all
+// unstable nodes at every step; every window slice adds cot * integral of S_p over the slice
+// (continuous time) or cot * S_p (discrete time, whose score is sum over jumps of
+// d log rate_j - d log a0). The engine's batched gradient kernel keeps the same quantities
+// incrementally; this checks it. dR is a CSR over entry 2i (node i's up rate) and 2i + 1 (its down
+// rate) of (parameter, d rate / d parameter); grad receives the sum over trajectories (unscaled).
+void gradient_integer(const compiled& c, unsigned long long seed, unsigned long long traj, const double* cot,
+					  int P, const int* gptr, const int* gp, const float* gd, std::vector<double>& G)
+{
+	curandStatePhilox4_32_10_t rng;
+	curand_init(seed, traj, 0ull, &rng);
+	std::vector<uint32_t> st(c.W, 0u);
+	for (int i = 0; i < c.N; i++)
+		if (curand_uniform(&rng) <= c.m.nodes[i].istate)
+			st[i / 32] |= 1u << (i % 32);
+	const float inv_scale = 1.0f / (float)(1u << c.shift);
+	curand_init(seed, traj, (unsigned long long)((c.N + 3) & ~3), &rng);
+	const size_t S = (size_t)1 << c.ni.size();
+	std::vector<unsigned> q(c.N);
+	std::vector<double> J(P, 0.0), I(P, 0.0), D(P, 0.0);
+	float time = 0.f;
+	for (;;)
+	{
+		const uint4 rb = curand4(&rng);
+		unsigned long long total = 0;
+		std::fill(D.begin(), D.end(), 0.0);
+		for (int i = 0; i < c.N; i++)
+		{
+			const bool on = (st[i / 32] >> (i % 32)) & 1u;
+			unsigned p = 0;
+			const std::vector<int>& in = c.tt_in[i];
+			for (size_t k = 0; k < in.size(); k++)
+				p |= ((st[in[k] / 32] >> (in[k] % 32)) & 1u) << k;
+			const bool lg = (c.tt[i][p >> 6] >> (p & 63)) & 1u;
+			q[i] = 0;
+			if (on != lg)
+			{
+				q[i] = on ? c.q_down[i] : c.q_up[i];
+				const int e = 2 * i + (on ? 1 : 0);
+				for (int k = gptr[e]; k < gptr[e + 1]; k++)
+					D[gp[k]] += gd[k];
+			}
+			total += q[i];
+		}
+		float tn;
+		if (total == 0)
+			tn = c.max_time_sim;
+		else
+		{
+			if (c.discrete)
+			{
+				tn = time + c.tick_sim;
+				tn = c.max_time_sim - c.tick_sim < tn ? c.max_time_sim : tn;
+			}
+			else
+			{
+				const float total_f = (float)total * inv_scale;
+				const float u = (float)((rb.x >> 8) + 1u) * 5.9604644775390625e-8f;
+				tn = time + -logf(u) / total_f;
+			}
+			tn = std::fmin(tn, c.max_time_sim);
+		}
+		const size_t idx = (size_t)c.ni_index(st.data());
+		if (tn != 0.f)
+		{
+			if (c.discrete)
+			{
+				const int w = (int)lroundf(time / c.tick_f);
+				if (w >= 0 && w < c.T)
+					for (int p = 0; p < P; p++)
+						G[p] += cot[(size_t)w * S + idx] * (J[p] - I[p]);
+			}
+			else
+			{
+				// the window slices of record(), each integrated exactly: S_p is linear on the step
+				float sb = time;
+				int w = (int)floorf(sb / c.tick_f);
+				for (int guard = 0; tn > sb && guard <= c.T + 2; guard++)
+				{
+					const float se = std::fmin(tn, (float)(w + 1) * c.tick_f);
+					if (w >= 0 && w < c.T)
+					{
+						const double cw = cot[(size_t)w * S + idx];
+						const double len = (double)se - (double)sb, mid = 0.5 * ((double)sb + (double)se);
+						for (int p = 0; p < P; p++)
+							G[p] += cw * len * (J[p] - I[p] - D[p] * (mid - (double)time));
+					}
+					w++;
+					sb = se;
+				}
+				for (int p = 0; p < P; p++)
+					I[p] += D[p] * ((double)tn - (double)time);
+			}
+		}
+		time = tn;
+		if (time >= c.max_time_sim)
+			break;
+		const unsigned long long r64 = ((unsigned long long)rb.y << 32) | rb.z;
+		const unsigned long long r = (unsigned long long)(((unsigned __int128)r64 * total) >> 64);
+		unsigned long long cum = 0;
+		int j = -1;
+		for (int i = 0; i < c.N; i++)
+		{
+			cum += q[i];
+			if (r < cum)
+			{
+				j = i;
+				break;
+			}
+		}
+		const bool on_j = (st[j / 32] >> (j % 32)) & 1u;
+		const double rj = on_j ? c.down[j] : c.up[j];
+		const int e = 2 * j + (on_j ? 1 : 0);
+		for (int k = gptr[e]; k < gptr[e + 1]; k++)
+			J[gp[k]] += (double)gd[k] / rj;
+		if (c.discrete)
+		{
+			const double a0 = (double)((float)total * inv_scale);
+			for (int p = 0; p < P; p++)
+				I[p] += D[p] / a0;
+		}
+		st[j / 32] ^= 1u << (j % 32);
+	}
+}
+
 template <typename RNG>
 void trajectory(const compiled& c, sinks& s, RNG& rng, bool exact, int traj_len, run_acc& acc,
 				unsigned long long& trans, std::vector<std::pair<int, float>>* trace)
@@ -1487,6 +1619,30 @@ int oracle_result_fixed(const oracle_result* r, uint32_t* states, unsigned* coun
 
 // Trace of one trajectory: flip indices (-1 = end, -2 = epoch boundary) and the time before
 // each event. Returns the number of events (may exceed cap; only cap are written).
+// gradient_integer summed over trajectories first .. first + n - 1 (integer-rate models only;
+// returns -1 otherwise). grad[P] receives the unscaled sum.
+int oracle_gradient(const oracle_model* m, unsigned long long seed, unsigned long long first, long long n,
+					const double* cot, int P, const int* gptr, const int* gp, const float* gd, double* grad)
+{
+	const compiled& c = *m->c;
+	if (!c.integer_rates || c.ni.size() > 20)
+		return -1;
+	std::vector<double> total(P, 0.0);
+#pragma omp parallel
+	{
+		std::vector<double> G(P, 0.0);
+#pragma omp for schedule(dynamic, 16)
+		for (long long t = 0; t < n; t++)
+			gradient_integer(c, seed, first + (unsigned long long)t, cot, P, gptr, gp, gd, G);
+#pragma omp critical(oracle_gradient)
+		for (int p = 0; p < P; p++)
+			total[p] += G[p];
+	}
+	for (int p = 0; p < P; p++)
+		grad[p] = total[p];
+	return 0;
+}
+
 int oracle_trace(const oracle_model* m, int mode, unsigned long long seed, unsigned long long traj, int traj_len,
 				 int* flips, float* times, int cap)
 {

@@ -54,6 +54,9 @@ def lib() -> C.CDLL:
         L.oracle_model_set_variables.argtypes = [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int]
         L.oracle_trace.argtypes = [C.c_void_p, C.c_int, C.c_ulonglong, C.c_ulonglong, C.c_int,
                                    C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int]
+        L.oracle_gradient.restype = C.c_int
+        L.oracle_gradient.argtypes = [C.c_void_p, C.c_ulonglong, C.c_ulonglong, C.c_longlong, C.c_void_p, C.c_int,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _LIB = L
     return _LIB
 
@@ -167,6 +170,31 @@ class OracleModel:
             raw = sp["raw"].astype(np.float64)
             sp["probs"] = raw / n if self.discrete else (raw / 2.0 ** occ_exp) / (n * float(np.float32(self.tick)))
         return out
+
+    def gradient(self, n: int, cotangent: np.ndarray, derivatives: list[list[tuple[int, float]]],
+                 n_params: int, seed: int | None = None, first: int = 0) -> np.ndarray:
+        """Score-function gradient of sum(cotangent * window probabilities) over the fast-mode
+        (integer-rate) trajectories first .. first + n - 1, by the direct definition
+        (oracle.cpp: gradient_integer). derivatives[2 i] / [2 i + 1] list the (parameter, d rate /
+        d parameter) pairs of node i's up / down rate. Scaled like the probabilities."""
+        seed = self.seed if seed is None else seed
+        cot = np.ascontiguousarray(cotangent, dtype=np.float64).ravel()
+        assert cot.size == self.windows << self.k and len(derivatives) == 2 * self.nodes
+        gptr = np.zeros(2 * self.nodes + 1, np.int32)
+        gp, gd = [], []
+        for e, lst in enumerate(derivatives):
+            for p, d in lst:
+                gp.append(p)
+                gd.append(d)
+            gptr[e + 1] = len(gp)
+        gp = np.ascontiguousarray(gp if gp else [0], dtype=np.int32)
+        gd = np.ascontiguousarray(gd if gd else [0.0], dtype=np.float32)
+        out = np.zeros(max(1, n_params), np.float64)
+        if lib().oracle_gradient(self._h, seed, first, n, cot.ctypes.data, n_params, gptr.ctypes.data,
+                                 gp.ctypes.data, gd.ctypes.data, out.ctypes.data) != 0:
+            raise ValueError("the gradient needs integer rates and at most 20 non-internal nodes")
+        scale = 1.0 / (n * (1.0 if self.discrete else float(np.float32(self.tick))))
+        return out[:n_params] * scale
 
     def trace(self, traj: int, mode: int = 0, seed: int | None = None, traj_len: int = 100, cap: int = 1 << 16):
         seed = self.seed if seed is None else seed
