@@ -85,7 +85,7 @@ struct mbb_lane
 	__device__ __forceinline__ uint32_t& Q(int w) const { return ws[w * stride]; }
 	__device__ __forceinline__ float& GS(int p) const { return gS[p * stride]; }
 	__device__ __forceinline__ float& GD(int p) const { return gD[p * stride]; }
-	__device__ __forceinline__ double& GR(int p) const { return gR[(size_t)p * gstride]; }
+	__device__ __forceinline__ double* GR(int p) const { return gR + (size_t)p * gstride; }
 };
 
 __device__ __forceinline__ bool mbb_logic(const mb_net& net, const mbb_lane& v, int r, const uint4& rec)
@@ -148,6 +148,14 @@ __device__ __forceinline__ float mbb_entropy(const mb_net& net, const mb_variant
 	return h > 0.f ? h : 0.f;
 }
 
+// R_p lives in the lane's own global scratch: it is only ever added to, with a reduction that
+// does not return the old value (red), so the lane does not wait for an L2 round trip per change;
+// the lane reads it back once, with an atomic exchange (ordered after its own reductions).
+__device__ __forceinline__ void mbb_red_add(double* a, double v)
+{
+	asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(a), "d"(v) : "memory");
+}
+
 // Continuous time, summed by parts: with the running sums C1 = sum c * length and
 // C2 = sum c * length * midpoint over the trajectory's slices, and A_p, D_p piecewise constant,
 //   sum over slices of c * int (A_p - D_p t) dt = A_p C1 - D_p C2 - sum over p's changes (dA C1 - dD C2),
@@ -166,7 +174,7 @@ __device__ __forceinline__ void mbb_grad_active(const mb_variant& var, const mbb
 		if (!discrete)
 		{
 			const float dA = dd * now;
-			v.GR(p) += (double)dd * C2 - (double)dA * C1;
+			mbb_red_add(v.GR(p), (double)dd * C2 - (double)dA * C1);
 			v.GS(p) += dA;
 		}
 		v.GD(p) += dd;
@@ -180,7 +188,7 @@ __device__ __forceinline__ void mbb_grad_end(const mbb_lane& v, int P, bool disc
 	for (int p = 0; p < P; p++)
 	{
 		if (!discrete)
-			v.GR(p) += (double)v.GS(p) * C1 - (double)v.GD(p) * C2;
+			mbb_red_add(v.GR(p), (double)v.GS(p) * C1 - (double)v.GD(p) * C2);
 		v.GS(p) = 0.f;
 		v.GD(p) = 0.f;
 	}
@@ -191,10 +199,10 @@ __device__ __forceinline__ void mbb_grad_emit(const mb_variant& var, const mbb_l
 {
 	for (int p = 0; p < P; p++)
 	{
-		const double g = v.GR(p);
+		const double g = __longlong_as_double(
+			(long long)atomicExch(reinterpret_cast<unsigned long long*>(v.GR(p)), 0ull));
 		if (g != 0.0)
 			atomicAdd(var.grad + p, g);
-		v.GR(p) = 0.0;
 	}
 }
 
@@ -203,14 +211,14 @@ __device__ __forceinline__ void mbb_grad_emit(const mb_variant& var, const mbb_l
 __device__ __forceinline__ void mbb_grad_slice(const mb_variant& var, const mbb_lane& v, int P, int w, unsigned idx,
 											   float u, float w1, bool discrete, double& C1, double& C2)
 {
-	const double c = var.cot[(size_t)w * var.st.n_bins + idx];
+	const double c = __ldg(var.cot + (size_t)w * var.st.n_bins + idx);
 	if (c == 0.0)
 		return;
 	if (discrete)
 	{
 		const float cf = (float)c;
 		for (int p = 0; p < P; p++)
-			v.GR(p) += (double)(cf * v.GS(p));
+			mbb_red_add(v.GR(p), (double)(cf * v.GS(p)));
 		return;
 	}
 	const double len = (double)w1 - (double)u;
@@ -275,7 +283,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 	{
 		v.GS(p) = 0.f;
 		v.GD(p) = 0.f;
-		v.GR(p) = 0.0;
+		*v.GR(p) = 0.0;
 	}
 
 	mb_win_acc acc;
@@ -525,7 +533,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 						const int p = __ldg(var.g_p + e);
 						const float dA = __ldg(var.g_d + e) / rj;
 						if (!discrete)
-							v.GR(p) -= (double)dA * C1;
+							mbb_red_add(v.GR(p), -(double)dA * C1);
 						v.GS(p) += dA;
 					}
 					if (discrete)
