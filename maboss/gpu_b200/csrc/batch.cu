@@ -202,14 +202,21 @@ batch_engine::prepared& batch_engine::prepare(bool grad)
 		std::vector<uint2> q2(L.state_size);
 		for (int n = 0; n < L.state_size; n++)
 			q2[n] = make_uint2(V.q[2 * n], V.q[2 * n + 1]);
-		std::vector<float> rate(2 * L.state_size);
+		std::vector<float> rate(2 * L.state_size), rlog(2 * L.state_size);
 		for (int n = 0; n < L.state_size; n++)
 		{
 			rate[2 * n] = V.rates.up[n];
 			rate[2 * n + 1] = V.rates.down[n];
 		}
+		// r log2 r of the entropy, as the generated tables of the NVRTC kernels compute it
+		for (int e = 0; e < 2 * L.state_size; e++)
+		{
+			const double r = rate[e];
+			rlog[e] = r > 0 ? (float)(r * std::log2(r)) : 0.f;
+		}
 		upload(V.d_q, q2, s);
 		upload(V.d_rate, rate, s);
+		upload(V.d_rlog, rlog, s);
 		upload(V.d_istate, L.istate, s);
 		upload(V.d_gptr, V.rates.grad_ptr, s);
 		upload(V.d_gp, V.rates.grad_p, s);
@@ -224,6 +231,7 @@ batch_engine::prepared& batch_engine::prepare(bool grad)
 		d.rate_shift = V.rate_shift;
 		d.q = V.d_q.as<uint2>();
 		d.rate = V.d_rate.as<float>();
+		d.rlog = V.d_rlog.as<float>();
 		d.istate = V.d_istate.as<float>();
 		d.begin = begin;
 		d.first_traj = V.first_traj;

@@ -57,7 +57,7 @@ public:
 		int rate_shift = 0;
 		std::vector<unsigned> q;
 		plain_stats st;
-		dbuf d_q, d_rate, d_istate, d_gptr, d_gp, d_gd, d_counters, d_grad, d_cot, out_states, out_counts;
+		dbuf d_q, d_rate, d_rlog, d_istate, d_gptr, d_gp, d_gd, d_counters, d_grad, d_cot, out_states, out_counts;
 		std::unique_ptr<result> res;
 		std::vector<double> grad; // d (sum_ws cot[w][s] P_w(s)) / d parameter
 	};

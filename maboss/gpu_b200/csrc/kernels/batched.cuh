@@ -36,6 +36,7 @@ struct mb_variant
 	int rate_shift;
 	const uint2* q;		  // [N] (q_up, q_down) integer rates
 	const float* rate;	  // [2N] (up, down) float rates
+	const float* rlog;	  // [2N] r * log2(r) of those rates (fp64 log2 rounded to fp32, as the NVRTC tables)
 	const float* istate;  // [N]
 	unsigned long long begin; // first global work index of this variant
 	unsigned long long first_traj; // random stream of the variant's trajectory 0
@@ -136,10 +137,9 @@ __device__ __forceinline__ float mbb_entropy(const mb_net& net, const mb_variant
 		const uint32_t bit = 1u << (i & 31);
 		if (v.U(i >> 5) & bit)
 		{
-			const bool up = (v.S(i >> 5) & bit) != 0;
-			const float r = __ldg(var.rate + 2 * i + (up ? 1 : 0));
-			t += r;
-			tl += r > 0.f ? r * log2f(r) : 0.f;
+			const int e = 2 * i + ((v.S(i >> 5) & bit) ? 1 : 0);
+			t += __ldg(var.rate + e);
+			tl += __ldg(var.rlog + e);
 		}
 	}
 	if (!(t > 0.f))
@@ -485,17 +485,19 @@ __device__ void mbb_body(const mb_batch_params& B)
 			{
 				const unsigned long long r = __umul64hi(((unsigned long long)rb.y << 32) | rb.z, total);
 				const int wpg = (net.W + MBB_GROUPS - 1) / MBB_GROUPS;
+				const int ng = (net.W + wpg - 1) / wpg; // groups of this network
 				unsigned long long cum = 0;
-				int g = -1;
+				int g = 0;
+				// the first group whose running sum exceeds r (the group sums add up to total, so
+				// the last group is reached only when it is that group)
 #pragma unroll
 				for (int i = 0; i < MBB_GROUPS; i++)
 				{
-					const bool hit = g < 0 && r < cum + gs[i];
-					g = hit ? i : g;
-					cum += (g < 0) ? gs[i] : 0ull;
+					g = i;
+					if (i + 1 >= ng || r < cum + gs[i])
+						break;
+					cum += gs[i];
 				}
-				if (g < 0)
-					g = 0; // unreachable: the group sums add up to total
 				int word = g * wpg;
 				for (int i = 0; i < wpg; i++)
 				{
