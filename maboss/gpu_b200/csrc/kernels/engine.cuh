@@ -884,17 +884,31 @@ extern "C" __global__ void __launch_bounds__(128, 5) mb_fused_fast(mb_fused_para
 				}
 				if (g < 0)
 					g = MB_GROUPS - 1; // unreachable: the group sums add up to total
+				// the group's word sums are loaded together (independent shared-memory loads), then
+				// walked in registers: +2.3 % on the 1000-node network over a load-compare loop
 				int word = g * MB_WPG;
-				for (int i = 0; i < MB_WPG; i++)
 				{
-					const int w = g * MB_WPG + i;
-					if (w >= state_words)
-						break;
-					word = w;
-					const uint32_t q = v.Q(w);
-					if (r < cum + q)
-						break;
-					cum += q;
+					uint32_t qv[MB_WPG];
+#pragma unroll
+					for (int i = 0; i < MB_WPG; i++)
+					{
+						const int w = g * MB_WPG + i;
+						qv[i] = w < state_words ? v.Q(w) : 0u;
+					}
+					bool done = false;
+#pragma unroll
+					for (int i = 0; i < MB_WPG; i++)
+					{
+						const int w = g * MB_WPG + i;
+						if (!done && w < state_words)
+						{
+							word = w;
+							if (r < cum + qv[i])
+								done = true;
+							else
+								cum += qv[i];
+						}
+					}
 				}
 				const uint32_t sw = v.S(word);
 				uint32_t um = v.U(word);
