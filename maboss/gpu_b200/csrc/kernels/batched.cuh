@@ -66,7 +66,10 @@ struct mb_batch_params
 	unsigned gstride;	  // gstride = the launch's thread count
 };
 
-constexpr int MBB_GROUPS = 16; // register group sums; words per group = ceil(W / 16)
+// register group sums; words per group = ceil(W / 8). Measured on C5 (256 variants, 1 to 16 words):
+// 8 groups 7.26e9 transitions/s, 4 groups 6.70e9, 16 groups 6.34e9 (predicated updates of every
+// group register at each rate change cost more than the longer word walk saves)
+constexpr int MBB_GROUPS = 8;
 
 struct mbb_lane
 {
