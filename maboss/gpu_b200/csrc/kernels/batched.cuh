@@ -605,4 +605,4 @@ __device__ void mbb_body(const mb_batch_params& B)
 }
 
 extern "C" __global__ void __launch_bounds__(128, 5) mb_batched_fast(mb_batch_params B) { mbb_body<false>(B); }
-extern "C" __global__ void __launch_bounds__(128, 4) mb_batched_grad(mb_batch_params B) { mbb_body<true>(B); }
+extern "C" __global__ void __launch_bounds__(128, 5) mb_batched_grad(mb_batch_params B) { mbb_body<true>(B); }
