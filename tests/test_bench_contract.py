@@ -1,0 +1,43 @@
+"""bench.py's reference arm (the CPU oracle timed on the host) prints one JSON line with the keys
+the benchmark contract names; under a multi-rank launch only rank 0 works and prints."""
+import json
+import os
+import subprocess
+import sys
+
+from conftest import ROOT
+
+ARGS = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload", "c1",
+        "--steps", "2", "--warmup", "1", "--cpu-sample", "300"]
+
+
+def _run(env_extra):
+    env = dict(os.environ, **env_extra)
+    return subprocess.run(ARGS, cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+
+
+def test_reference_arm_prints_the_contract_line():
+    p = _run({"RANK": "0", "WORLD_SIZE": "1", "LOCAL_RANK": "0"})
+    assert p.returncode == 0, p.stderr
+    lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, p.stdout
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    assert d["metric"] == "Gillespie transitions/s" and d["unit"] == "transitions/s"
+    assert d["value"] > 0 and d["ms_per_step"] > 0
+    assert (d["n_gpus"], d["steps"], d["warmup"]) == (1, 2, 1)
+    assert d["higher_is_better"] is True and d["scaling"] == "weak" and d["vs_baseline"] is None
+    assert d["dtype"] == "f32" and d["data"] == "synthetic"
+    assert d["config"]["workload"].startswith("c1:")
+    cb = d["cpu_baseline"]
+    assert cb["value"] == d["value"] and cb["unit"] == d["unit"] and cb["cores"] >= 1
+    assert cb["kind"] == "port" and "300 trajectories" in cb["sample"]
+    e2e = d["e2e"]
+    assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
+    assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    p = _run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
+    assert p.returncode == 0, p.stderr
+    assert not [l for l in p.stdout.splitlines() if l.startswith("{")]
