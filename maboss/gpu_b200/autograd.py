@@ -21,6 +21,7 @@ class _WindowProbabilities(torch.autograd.Function):
     def forward(ctx, theta, engine_ctx, model, names, n_traj, seed):
         params = {n: float(v) for n, v in zip(names, theta.detach().cpu().tolist())}
         b = Batch(engine_ctx)
+        b.set_options(use_graph=False, autotune=False)  # one run: no graph, default launch shape
         net = b.add_model(model)
         v = b.add_variant(net, n_traj, params)
         b.run(seed)

@@ -872,6 +872,10 @@ mb_status mb_gradient(mb_context c, mb_model m, const char* const* params, const
 	return guard([&] {
 		need(c && m && cotangent && n_params >= 0 && (grad || n_params == 0), "bad argument");
 		mb::batch_engine be(*c->ctx);
+		// one run of a throw-away engine: neither a CUDA graph nor timed candidate shapes would be
+		// used again; the default shape is 128 threads with as many blocks as fit
+		be.use_graph = false;
+		be.autotune = false;
 		const int net = be.add_model(m->model);
 		std::vector<std::string> names;
 		for (int i = 0; i < n_params; i++)
