@@ -313,6 +313,22 @@ mb_status mb_batch_info(mb_batch b, int* block, int* blocks_per_sm, unsigned* gr
                         int* tuned_shapes);
 /* Shape `i` of the autotuner's timings: gradient run or not, threads per block, blocks per SM, kernel ms. */
 mb_status mb_batch_tuning(mb_batch b, int i, int* gradient, int* block, int* blocks_per_sm, float* kernel_ms);
+/* Gradients on a batch (the engine of mb_gradient kept across calls: buffers, launch shapes and
+ * graphs are reused). mb_batch_add_variant_grad adds a variant like mb_batch_add_variant whose
+ * gradient with respect to the $variables grad_params is computed by mb_batch_run_gradient.
+ * mb_batch_set_variables gives variant v new values of some of its $variables in place (its rate
+ * tables are recomputed and uploaded; prepared runs stay valid). mb_batch_run_gradient runs the
+ * batch once with cotangents (cotangents[v]: variant v's [windows * 2^k] array, NULL for zeros;
+ * n_cotangents = the number of variants): forward statistics (mb_batch_result) and, per variant,
+ * the vector-Jacobian product that mb_batch_gradient copies out (n_grad = its length, at most cap
+ * values written). Same estimator, trajectories and scaling as mb_gradient. */
+mb_status mb_batch_add_variant_grad(mb_batch b, int net, const char* const* names, const float* values,
+                                    int n_values, long long n_traj, unsigned long long first_traj,
+                                    const char* const* grad_params, int n_grad, int* variant);
+mb_status mb_batch_set_variables(mb_batch b, int v, const char* const* names, const float* values, int n_values);
+mb_status mb_batch_run_gradient(mb_batch b, unsigned long long seed, const double* const* cotangents,
+                                int n_cotangents, float* kernel_ms);
+mb_status mb_batch_gradient(mb_batch b, int v, double* grad, int cap, int* n_grad);
 
 /* Score-function (likelihood-ratio) gradient of L = sum_{w,s} cotangent[w * 2^k + s] * P_w(s) with
  * respect to the $variables `params` (set to `values`), P_w(s) the window probabilities of

@@ -102,6 +102,11 @@ def _declare(L: C.CDLL) -> None:
         "mb_batch_add_variant": (i32, [vp, i32, P(C.c_char_p), P(f32), i32, i64, u64, P(i32)]),
         "mb_batch_run": (i32, [vp, u64, P(f32)]),
         "mb_batch_result": (i32, [vp, i32, P(vp)]),
+        "mb_batch_add_variant_grad": (i32, [vp, i32, P(C.c_char_p), P(f32), i32, i64, u64, P(C.c_char_p), i32,
+                                            P(i32)]),
+        "mb_batch_set_variables": (i32, [vp, i32, P(C.c_char_p), P(f32), i32]),
+        "mb_batch_run_gradient": (i32, [vp, u64, P(C.c_void_p), i32, P(f32)]),
+        "mb_batch_gradient": (i32, [vp, i32, P(C.c_double), i32, P(i32)]),
         "mb_gradient": (i32, [vp, vp, P(C.c_char_p), P(f32), i32, i64, u64, vp, vp, P(vp)]),
         "mb_fixed_states_noalloc": (i32, [vp, i32, i32, i32, vp, vp, vp, vp, i32, P(i32)]),
         "mb_result_free": (i32, [vp]),

@@ -799,6 +799,71 @@ mb_status mb_batch_add_variant(mb_batch b, int net, const char* const* names, co
 	});
 }
 
+mb_status mb_batch_add_variant_grad(mb_batch b, int net, const char* const* names, const float* values,
+									int n_values, long long n_traj, unsigned long long first_traj,
+									const char* const* grad_params, int n_grad, int* variant)
+{
+	return guard([&] {
+		need(b && variant && n_values >= 0 && n_grad >= 0, "bad argument");
+		std::vector<std::string> gp;
+		for (int i = 0; i < n_grad; i++)
+		{
+			need(grad_params && grad_params[i], "null gradient parameter name");
+			gp.push_back(grad_params[i]);
+		}
+		need(net >= 0 && net < (int)b->b->nets.size(), "bad network index");
+		const mb::model_t& m = b->b->nets[net]->model;
+		for (auto& g : gp)
+			need(m.variables.count(g) != 0, "unknown gradient parameter");
+		*variant = b->b->add_variant(net, overrides_of(names, values, n_values), n_traj, first_traj, gp);
+	});
+}
+
+mb_status mb_batch_set_variables(mb_batch b, int v, const char* const* names, const float* values, int n_values)
+{
+	return guard([&] {
+		need(b && n_values >= 0, "bad argument");
+		b->b->set_variables(v, overrides_of(names, values, n_values));
+	});
+}
+
+mb_status mb_batch_run_gradient(mb_batch b, unsigned long long seed, const double* const* cotangents,
+								int n_cotangents, float* kernel_ms)
+{
+	return guard([&] {
+		need(b, "null batch");
+		mb::batch_engine& e = *b->b;
+		need(n_cotangents == (int)e.vars_.size() && (cotangents || n_cotangents == 0),
+			 "one cotangent per variant");
+		std::vector<std::vector<double>> cot(e.vars_.size());
+		for (size_t i = 0; i < e.vars_.size(); i++)
+		{
+			const mb::model_layout& L = e.nets[e.vars_[i]->net]->L;
+			const size_t cells = (size_t)L.windows() << L.noninternal_nodes.size();
+			cot[i] = cotangents[i] ? std::vector<double>(cotangents[i], cotangents[i] + cells)
+								   : std::vector<double>(cells, 0.0);
+		}
+		e.run(seed, &cot);
+		b->ran = true;
+		if (kernel_ms)
+			*kernel_ms = e.kernel_ms;
+	});
+}
+
+mb_status mb_batch_gradient(mb_batch b, int v, double* grad, int cap, int* n_grad)
+{
+	return guard([&] {
+		need(b && b->ran, "run the batch first");
+		need(v >= 0 && v < (int)b->b->vars_.size(), "bad variant index");
+		const std::vector<double>& g = b->b->vars_[v]->grad;
+		need(cap >= 0 && (grad || cap == 0), "bad argument");
+		for (int i = 0; i < cap && i < (int)g.size(); i++)
+			grad[i] = g[i];
+		if (n_grad)
+			*n_grad = (int)g.size();
+	});
+}
+
 mb_status mb_batch_set_options(mb_batch b, int use_graph, int autotune)
 {
 	return guard([&] {

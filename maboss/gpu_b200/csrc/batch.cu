@@ -46,7 +46,10 @@ __global__ void mbb_fixed_extract(unsigned cap, int words, const mb_key128* __re
 template <typename T>
 void upload(dbuf& b, const std::vector<T>& v, cudaStream_t s)
 {
-	b.alloc(std::max<size_t>(1, v.size()) * sizeof(T));
+	// a buffer that is large enough is kept: descriptors and captured graphs hold its address
+	const size_t need = std::max<size_t>(1, v.size()) * sizeof(T);
+	if (b.bytes < need)
+		b.alloc(need);
 	if (!v.empty())
 		MB_CUDA(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
 }
@@ -108,32 +111,113 @@ int batch_engine::add_variant(int net, const std::map<std::string, float>& overr
 	var->n_traj = n_traj;
 	var->first_traj = first_traj;
 	var->grad_params = grad_params;
-	std::map<std::string, float> vars = N.model.variables;
 	for (auto& kv : overrides)
-	{
-		if (!vars.count(kv.first))
+		if (!N.model.variables.count(kv.first))
 			throw engine_error(MB_ERR_INVALID, "unknown variable " + kv.first);
-		vars[kv.first] = kv.second;
-	}
-	const model_layout& L = N.L;
-	if (overrides.empty() && grad_params.empty())
-	{
-		// the model's own values, exactly as the compiled single-model kernels see them
-		var->rates.up = L.up;
-		var->rates.down = L.down;
-		var->rates.grad_ptr.assign(2 * L.state_size + 1, 0);
-	}
-	else
-		var->rates = fast_rates(N.model, vars, grad_params);
-	const incremental_tables t = build_incremental_tables(L, var->rates.up, var->rates.down);
-	if (!t.ok)
-		throw engine_error(MB_ERR_INVALID, "rates must be finite, non-negative, and positive rates within 2^20 of "
-										   "the largest one");
-	var->rate_shift = t.rate_shift;
-	var->q = t.q;
+	var->overrides = overrides;
+	compute_rates(*var);
 	invalidate();
 	vars_.push_back(std::move(var));
 	return (int)vars_.size() - 1;
+}
+
+// Rates, their derivatives and the integer rate tables of a variant from its variable values.
+void batch_engine::compute_rates(variant& V) const
+{
+	const network& N = *nets[V.net];
+	const model_layout& L = N.L;
+	if (V.overrides.empty() && V.grad_params.empty())
+	{
+		// the model's own values, exactly as the compiled single-model kernels see them
+		V.rates = rate_set{};
+		V.rates.up = L.up;
+		V.rates.down = L.down;
+		V.rates.grad_ptr.assign(2 * L.state_size + 1, 0);
+	}
+	else
+	{
+		std::map<std::string, float> vars = N.model.variables;
+		for (auto& kv : V.overrides)
+			vars[kv.first] = kv.second;
+		V.rates = fast_rates(N.model, vars, V.grad_params);
+	}
+	const incremental_tables t = build_incremental_tables(L, V.rates.up, V.rates.down);
+	if (!t.ok)
+		throw engine_error(MB_ERR_INVALID, "rates must be finite, non-negative, and positive rates within 2^20 of "
+										   "the largest one");
+	V.rate_shift = t.rate_shift;
+	V.q = t.q;
+}
+
+// The parameter-dependent device tables of a variant (integer rates, float rates, r log2 r, rate
+// derivatives), into its buffers (kept when large enough).
+void batch_engine::upload_tables(variant& V, cudaStream_t s)
+{
+	const model_layout& L = nets[V.net]->L;
+	std::vector<uint2> q2(L.state_size);
+	for (int n = 0; n < L.state_size; n++)
+		q2[n] = make_uint2(V.q[2 * n], V.q[2 * n + 1]);
+	std::vector<float> rate(2 * L.state_size), rlog(2 * L.state_size);
+	for (int n = 0; n < L.state_size; n++)
+	{
+		rate[2 * n] = V.rates.up[n];
+		rate[2 * n + 1] = V.rates.down[n];
+	}
+	// r log2 r of the entropy, as the generated tables of the NVRTC kernels compute it
+	for (int e = 0; e < 2 * L.state_size; e++)
+	{
+		const double r = rate[e];
+		rlog[e] = r > 0 ? (float)(r * std::log2(r)) : 0.f;
+	}
+	upload(V.d_q, q2, s);
+	upload(V.d_rate, rate, s);
+	upload(V.d_rlog, rlog, s);
+	upload(V.d_gptr, V.rates.grad_ptr, s);
+	upload(V.d_gp, V.rates.grad_p, s);
+	upload(V.d_gd, V.rates.grad_d, s);
+}
+
+void batch_engine::set_variables(int v, const std::map<std::string, float>& values)
+{
+	if (v < 0 || v >= (int)vars_.size())
+		throw engine_error(MB_ERR_INVALID, "bad variant index");
+	variant& V = *vars_[v];
+	const network& N = *nets[V.net];
+	for (auto& kv : values)
+		if (!N.model.variables.count(kv.first))
+			throw engine_error(MB_ERR_INVALID, "unknown variable " + kv.first);
+	const std::map<std::string, float> before = V.overrides;
+	for (auto& kv : values)
+		V.overrides[kv.first] = kv.second;
+	try
+	{
+		compute_rates(V);
+	}
+	catch (...)
+	{
+		V.overrides = before;
+		compute_rates(V);
+		throw;
+	}
+	if (!V.ready)
+		return; // uploaded by the first prepare
+	MB_CUDA(cudaSetDevice(ctx->device));
+	cudaStream_t s = ctx->stream;
+	upload_tables(V, s);
+	for (auto& ps : prep)
+		if (ps)
+		{
+			mb_variant& d = ps->hvars[v];
+			d.rate_shift = V.rate_shift;
+			d.q = V.d_q.as<uint2>();
+			d.rate = V.d_rate.as<float>();
+			d.rlog = V.d_rlog.as<float>();
+			d.g_ptr = V.d_gptr.as<int>();
+			d.g_p = V.d_gp.as<int>();
+			d.g_d = V.d_gd.as<float>();
+			upload(ps->d_vars, ps->hvars, s); // same size: same address, so graphs stay valid
+		}
+	MB_CUDA(cudaStreamSynchronize(s));
 }
 
 void batch_engine::invalidate()
@@ -198,34 +282,20 @@ batch_engine::prepared& batch_engine::prepare(bool grad)
 		const model_layout& L = nets[V.net]->L;
 		if (grad)
 			P = std::max(P, (int)V.grad_params.size());
-		V.st.init_plain(L.state_words, L.time_tick, L.max_time, L.discrete_time, L.noninternal_nodes, V.n_traj, s);
-		std::vector<uint2> q2(L.state_size);
-		for (int n = 0; n < L.state_size; n++)
-			q2[n] = make_uint2(V.q[2 * n], V.q[2 * n + 1]);
-		std::vector<float> rate(2 * L.state_size), rlog(2 * L.state_size);
-		for (int n = 0; n < L.state_size; n++)
+		if (!V.ready)
 		{
-			rate[2 * n] = V.rates.up[n];
-			rate[2 * n + 1] = V.rates.down[n];
+			// created once: the other kind of run (forward / gradient) shares these buffers
+			V.st.init_plain(L.state_words, L.time_tick, L.max_time, L.discrete_time, L.noninternal_nodes, V.n_traj,
+							s);
+			upload(V.d_istate, L.istate, s);
+			V.d_counters.alloc(16);
+			V.d_grad.alloc(std::max<size_t>(1, V.grad_params.size()) * sizeof(double));
+			V.d_cot.alloc((size_t)L.windows() * ((size_t)1 << L.noninternal_nodes.size()) * sizeof(double));
+			V.out_states.alloc((size_t)V.st.fp_cap * L.state_words * 4);
+			V.out_counts.alloc((size_t)V.st.fp_cap * 4);
+			upload_tables(V, s);
+			V.ready = true;
 		}
-		// r log2 r of the entropy, as the generated tables of the NVRTC kernels compute it
-		for (int e = 0; e < 2 * L.state_size; e++)
-		{
-			const double r = rate[e];
-			rlog[e] = r > 0 ? (float)(r * std::log2(r)) : 0.f;
-		}
-		upload(V.d_q, q2, s);
-		upload(V.d_rate, rate, s);
-		upload(V.d_rlog, rlog, s);
-		upload(V.d_istate, L.istate, s);
-		upload(V.d_gptr, V.rates.grad_ptr, s);
-		upload(V.d_gp, V.rates.grad_p, s);
-		upload(V.d_gd, V.rates.grad_d, s);
-		V.d_counters.alloc(16);
-		V.d_grad.alloc(std::max<size_t>(1, V.grad_params.size()) * sizeof(double));
-		V.d_cot.alloc((size_t)L.windows() * ((size_t)1 << L.noninternal_nodes.size()) * sizeof(double));
-		V.out_states.alloc((size_t)V.st.fp_cap * L.state_words * 4);
-		V.out_counts.alloc((size_t)V.st.fp_cap * 4);
 		mb_variant& d = hvars[i];
 		d.net = V.net;
 		d.rate_shift = V.rate_shift;
@@ -259,16 +329,17 @@ batch_engine::prepared& batch_engine::prepare(bool grad)
 		o.grad = host_bytes;
 		host_bytes += V.d_grad.bytes;
 	}
-	upload(d_nets, hnets, s);
-	upload(d_vars, hvars, s);
+	upload(ps->d_nets, hnets, s);
+	upload(ps->d_vars, hvars, s);
+	ps->hvars = hvars;
 	ps->counters.alloc(64);
 	MB_CUDA(cudaHostAlloc(&ps->host, std::max<size_t>(host_bytes, 8), cudaHostAllocDefault));
 	MB_CUDA(cudaEventCreate(&ps->e0));
 	MB_CUDA(cudaEventCreate(&ps->e1));
 	ps->B = std::make_unique<mb_batch_params>();
 	mb_batch_params& B = *ps->B;
-	B.nets = d_nets.as<mb_net>();
-	B.vars = d_vars.as<mb_variant>();
+	B.nets = ps->d_nets.as<mb_net>();
+	B.vars = ps->d_vars.as<mb_variant>();
 	B.n_vars = (int)hvars.size();
 	B.max_W = max_W;
 	B.P = P;

@@ -11,6 +11,7 @@
 #include "runtime.h"
 
 struct mb_batch_params; // kernels/batched.cuh
+struct mb_variant;
 
 namespace mb {
 
@@ -53,11 +54,13 @@ public:
 		long long n_traj = 0;
 		unsigned long long first_traj = 0;
 		std::vector<std::string> grad_params;
+		std::map<std::string, float> overrides; // this variant's variable values (the rest: the model's)
 		rate_set rates;
 		int rate_shift = 0;
 		std::vector<unsigned> q;
 		plain_stats st;
 		dbuf d_q, d_rate, d_rlog, d_istate, d_gptr, d_gp, d_gd, d_counters, d_grad, d_cot, out_states, out_counts;
+		bool ready = false; // accumulators and per-variant buffers exist (created once, shared by both plans)
 		std::unique_ptr<result> res;
 		std::vector<double> grad; // d (sum_ws cot[w][s] P_w(s)) / d parameter
 	};
@@ -68,6 +71,9 @@ public:
 	// `overrides`: variable values of this variant; `grad_params`: variables to differentiate
 	int add_variant(int net, const std::map<std::string, float>& overrides, long long n_traj,
 					unsigned long long first_traj, const std::vector<std::string>& grad_params = {});
+	// new values of some of variant v's variables: its rate tables are recomputed and uploaded in
+	// place, so prepared runs, launch shapes and captured graphs stay valid
+	void set_variables(int v, const std::map<std::string, float>& values);
 	// one persistent launch over every variant; with cotangents (one [windows * 2^k] vector per
 	// variant) it also computes the vector-Jacobian products
 	void run(unsigned long long seed, const std::vector<std::vector<double>>* cotangents = nullptr);
@@ -87,7 +93,6 @@ public:
 	context* ctx;
 	std::vector<std::unique_ptr<network>> nets;
 	std::vector<std::unique_ptr<variant>> vars_;
-	dbuf d_nets, d_vars;
 	float kernel_ms = 0;
 	int last_block = 0, last_per_sm = 0;
 	unsigned last_grid = 0;
@@ -113,12 +118,18 @@ private:
 		cudaGraph_t graph = nullptr;
 		cudaGraphExec_t exec = nullptr;
 		cudaGraphNode_t kernel = nullptr;
+		// this plan's device descriptors (the forward and gradient plans differ in the cotangent
+		// pointers) and their host copy
+		dbuf d_nets, d_vars;
+		std::vector<mb_variant> hvars;
 		~prepared();
 	};
 	std::unique_ptr<prepared> prep[2]; // forward, gradient
 	void invalidate();
 	prepared& prepare(bool grad);
 	int fit(prepared& ps, int block, size_t& smem) const;
+	void compute_rates(variant& V) const;
+	void upload_tables(variant& V, cudaStream_t s);
 	void set_shape(prepared& ps, int block, int per_sm);
 	void enqueue(prepared& ps, cudaStream_t s, bool capturing);
 	void tune(prepared& ps, cudaStream_t s);

@@ -312,16 +312,48 @@ class Batch:
         return n.value
 
     def add_variant(self, net: int, n_traj: int, params: dict[str, float] | None = None,
-                    first_traj: int = 0) -> int:
+                    first_traj: int = 0, grad_params: list[str] | None = None) -> int:
+        """A variant of network `net` (`params`: its $variable values); with `grad_params`, the
+        $variables whose gradient run_gradient computes for it."""
         names, values, k = _names_values(params)
         v = C.c_int()
-        check(lib().mb_batch_add_variant(self._h, net, names, values, k, n_traj, first_traj, C.byref(v)))
+        if grad_params:
+            gp = (C.c_char_p * len(grad_params))(*[g.encode() for g in grad_params])
+            check(lib().mb_batch_add_variant_grad(self._h, net, names, values, k, n_traj, first_traj, gp,
+                                                  len(grad_params), C.byref(v)))
+        else:
+            check(lib().mb_batch_add_variant(self._h, net, names, values, k, n_traj, first_traj, C.byref(v)))
+        self._n_variants = getattr(self, "_n_variants", 0) + 1
         return v.value
+
+    def set_variables(self, variant: int, params: dict[str, float]) -> None:
+        """mb_batch_set_variables: new values of some of a variant's $variables, in place."""
+        names, values, k = _names_values(params)
+        check(lib().mb_batch_set_variables(self._h, variant, names, values, k))
 
     def run(self, seed: int = 0) -> float:
         ms = C.c_float()
         check(lib().mb_batch_run(self._h, seed, C.byref(ms)))
         return ms.value
+
+    def run_gradient(self, seed: int, cotangents: dict[int, np.ndarray]) -> float:
+        """mb_batch_run_gradient: one run with a cotangent per variant (`cotangents[v]`, shape
+        [windows, 2^k]; missing variants take zeros). Returns the kernel time in ms."""
+        n = getattr(self, "_n_variants", 0)
+        arrays = {v: np.ascontiguousarray(c, dtype=np.float64).ravel() for v, c in cotangents.items()}
+        ptrs = (C.c_void_p * max(1, n))(*[arrays[v].ctypes.data if v in arrays else None for v in range(n)])
+        ms = C.c_float()
+        check(lib().mb_batch_run_gradient(self._h, seed, ptrs, n, C.byref(ms)))
+        return ms.value
+
+    def gradient(self, variant: int) -> np.ndarray:
+        """mb_batch_gradient: d sum(cotangent * window_probs) / d grad_params of the last gradient run."""
+        n = C.c_int()
+        check(lib().mb_batch_gradient(self._h, variant, None, 0, C.byref(n)))
+        out = np.zeros(max(1, n.value), np.float64)
+        check(lib().mb_batch_gradient(self._h, variant, out.ctypes.data_as(C.POINTER(C.c_double)), n.value,
+                                      C.byref(n)))
+        return out[: n.value]
 
     def result(self, variant: int) -> "Result":
         h = C.c_void_p()

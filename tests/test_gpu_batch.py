@@ -170,6 +170,79 @@ def test_gradient_equals_oracle_on_the_same_trajectories(gpu, discrete):
     assert np.all(np.abs(g - ref) <= tol), (g, ref)
 
 
+def _c4_gradient_case():
+    bnd, cfg = synth.c4()
+    model = mb.Model(bnd, cfg)
+    names = [f"$u_{i}" for i in range(4)] + [f"$d_{i}" for i in range(4)]
+    theta = {k: model.variable(k) for k in names}
+    return model, names, theta
+
+
+def test_forward_and_gradient_runs_share_one_batch(gpu):
+    """One batch runs forward, then with cotangents, then forward again: the statistics of all three
+    runs are identical (the two kinds of run share the variant's buffers, each keeps its own
+    descriptors), and the gradient equals mb_gradient's on the same trajectories."""
+    model, names, theta = _c4_gradient_case()
+    n, seed = 20_000, 3
+    b = mb.Batch(gpu)
+    v = b.add_variant(b.add_model(model), n, theta, grad_params=names)
+    b.run(seed)
+    r1 = b.result(v)
+    cot = np.random.default_rng(1).normal(size=r1.window_probs.shape)
+    b.run_gradient(seed, {v: cot})
+    g1, r2 = b.gradient(v), b.result(v)
+    b.run(seed)
+    r3 = b.result(v)
+    _same(r1, r2)
+    _same(r1, r3)
+    b.run_gradient(seed, {v: cot})
+    g2 = b.gradient(v)
+    ref, _ = mb.gradient(gpu, model, theta, cot, n, seed)
+    assert len(g1) == len(names)
+    assert np.allclose(g1, ref, rtol=1e-9, atol=1e-12) and np.allclose(g2, ref, rtol=1e-9, atol=1e-12)
+
+
+def test_set_variables_equals_a_fresh_batch(gpu):
+    """New variable values on a prepared batch (tables re-uploaded in place, graphs replayed) give
+    the statistics and the gradient of a batch built with those values."""
+    model, names, theta = _c4_gradient_case()
+    n, seed = 20_000, 5
+    b = mb.Batch(gpu)
+    v = b.add_variant(b.add_model(model), n, theta, grad_params=names)
+    b.run(seed)
+    cot = np.random.default_rng(2).normal(size=b.result(v).window_probs.shape)
+    b.run_gradient(seed, {v: cot})
+    theta2 = {k: float(np.float32(x * (1.3 if i % 2 else 0.8))) for i, (k, x) in enumerate(theta.items())}
+    b.set_variables(v, theta2)
+    b.run(seed)
+    fresh = mb.Batch(gpu)
+    fv = fresh.add_variant(fresh.add_model(model), n, theta2)
+    fresh.run(seed)
+    _same(b.result(v), fresh.result(fv))
+    b.run_gradient(seed, {v: cot})
+    ref, _ = mb.gradient(gpu, model, theta2, cot, n, seed)
+    assert np.allclose(b.gradient(v), ref, rtol=1e-9, atol=1e-12)
+
+
+def test_autograd_function_reuses_its_batch(gpu):
+    import torch
+
+    from maboss.gpu_b200.autograd import window_probabilities
+
+    model, names, theta = _c4_gradient_case()
+    n = 20_000
+    for scale in (1.0, 1.2, 0.9):
+        t = torch.tensor([theta[k] * scale for k in names], dtype=torch.float64, requires_grad=True)
+        probs = window_probabilities(t, gpu, model, names, n, seed=7)
+        w = torch.linspace(0.0, 1.0, probs.shape[1], dtype=torch.float64)
+        (probs * w).sum().backward()
+        params = {k: float(x) for k, x in zip(names, t.detach().tolist())}
+        cot = np.tile(w.numpy(), (probs.shape[0], 1))
+        g, fwd = mb.gradient(gpu, model, params, cot, n, 7)
+        assert np.array_equal(probs.detach().numpy(), fwd.window_probs)
+        assert np.allclose(t.grad.numpy(), g, rtol=1e-9, atol=1e-12)
+
+
 def test_autograd_function(gpu):
     import torch
 
