@@ -573,13 +573,14 @@ class Result:
         non-internal indices as (bits 0-63, bits 64-127) uint64 pairs."""
         nw, nf, ovf = C.c_longlong(), C.c_longlong(), C.c_uint()
         check(lib().mb_result_sparse_size(self._h, C.byref(nw), C.byref(nf), C.byref(ovf)))
-        w = np.zeros(max(1, nw.value), np.int32)
-        st = np.zeros((max(1, nw.value), 2), np.uint64)
-        raw = np.zeros(max(1, nw.value), np.int64)
-        pr = np.zeros(max(1, nw.value), np.float64)
+        # every entry is written by the C ABI: no zero fill (the arrays reach gigabytes)
+        w = np.empty(max(1, nw.value), np.int32)
+        st = np.empty((max(1, nw.value), 2), np.uint64)
+        raw = np.empty(max(1, nw.value), np.int64)
+        pr = np.empty(max(1, nw.value), np.float64)
         check(lib().mb_result_sparse_windows(self._h, w.ctypes.data, st.ctypes.data, raw.ctypes.data, pr.ctypes.data))
-        fs = np.zeros((max(1, nf.value), 2), np.uint64)
-        fc = np.zeros(max(1, nf.value), np.uint32)
+        fs = np.empty((max(1, nf.value), 2), np.uint64)
+        fc = np.empty(max(1, nf.value), np.uint32)
         check(lib().mb_result_sparse_final(self._h, fs.ctypes.data, fc.ctypes.data))
         n, m = nw.value, nf.value
         return dict(windows=w[:n], states=st[:n], raw=raw[:n], probs=pr[:n], final_states=fs[:m],
