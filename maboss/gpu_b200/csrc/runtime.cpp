@@ -2,6 +2,7 @@
 // run time with cudaGetDriverEntryPointByVersion, so the library loads on hosts without a GPU
 // driver), and the run drivers.
 #include "runtime.h"
+#include "sparse_bins.h"
 
 #include <curand_kernel.h>
 #include <nvrtc.h>
@@ -16,6 +17,7 @@
 #include <mutex>
 #include <numeric>
 #include <sstream>
+#include <thread>
 
 #include "kernels/params.cuh"
 
@@ -590,55 +592,22 @@ std::unique_ptr<result> stats_state::finalize(long long n, cudaStream_t s)
 		MB_CUDA(cudaMemcpyAsync(&nb, bin_extract_ctr(), sizeof nb, cudaMemcpyDeviceToHost, s));
 		MB_CUDA(cudaMemcpyAsync(&ovf, bin_overflow_ctr(), sizeof ovf, cudaMemcpyDeviceToHost, s));
 		MB_CUDA(cudaStreamSynchronize(s));
-		// sorted on the device
-		std::vector<mb_key128> bk(nb);
-		std::vector<long long> bv(nb);
+		// sorted on the device, copied into the kept host buffers, decoded by host threads
+		if (nb > hbin_cap)
+		{
+			hbin_keys.reset(new uint64_t[2 * (size_t)nb]);
+			hbin_vals.reset(new long long[nb]);
+			hbin_cap = nb;
+		}
 		if (nb)
 		{
 			dbuf sk((size_t)nb * sizeof(mb_key128)), sv((size_t)nb * sizeof(long long));
 			sort_bins(ok, ov, nb, sk.as<mb_key128>(), sv.as<long long>(), s);
-			MB_CUDA(cudaMemcpy(bk.data(), sk.p, nb * sizeof(mb_key128), cudaMemcpyDeviceToHost));
-			MB_CUDA(cudaMemcpy(bv.data(), sv.p, nb * sizeof(long long), cudaMemcpyDeviceToHost));
+			MB_CUDA(cudaMemcpy(hbin_keys.get(), sk.p, nb * sizeof(mb_key128), cudaMemcpyDeviceToHost));
+			MB_CUDA(cudaMemcpy(hbin_vals.get(), sv.p, nb * sizeof(long long), cudaMemcpyDeviceToHost));
 		}
-		struct bin
-		{
-			int w;
-			unsigned __int128 idx;
-			long long v;
-		};
-		std::vector<bin> bins(nb);
-		for (unsigned i = 0; i < nb; i++)
-			bins[i] = { (int)(bk[i].hi >> 48) - 1,
-						((unsigned __int128)(bk[i].hi & 0xffffffffffffull) << 64) | bk[i].lo, bv[i] };
-		r.sp_begin.assign(n_windows + 1, 0);
-		r.sp_w.reserve(nb);
-		r.sp_idx.reserve(nb);
-		r.sp_val.reserve(nb);
-		for (size_t i = 0; i < bins.size();)
-		{
-			size_t j = i;
-			long long v = 0;
-			for (; j < bins.size() && bins[j].w == bins[i].w && bins[j].idx == bins[i].idx; j++)
-				v += bins[j].v;
-			if (bins[i].w < n_windows)
-			{
-				r.sp_w.push_back(bins[i].w);
-				r.sp_idx.push_back(bins[i].idx);
-				r.sp_val.push_back(v);
-			}
-			else
-			{
-				r.fin_idx.push_back(bins[i].idx);
-				r.fin_cnt.push_back((unsigned)v);
-			}
-			i = j;
-		}
-		for (int w = 0, e = 0; w <= n_windows; w++)
-		{
-			while (e < (int)r.sp_w.size() && r.sp_w[e] < w)
-				e++;
-			r.sp_begin[w] = e;
-		}
+		decode_sorted_bins(hbin_keys.get(), hbin_vals.get(), nb, n_windows, (int)std::thread::hardware_concurrency(),
+						   r.sp_w, r.sp_idx, r.sp_val, r.sp_begin, r.fin_idx, r.fin_cnt);
 		r.bin_overflow = ovf;
 	}
 	if ((sections & 1u) && wide)

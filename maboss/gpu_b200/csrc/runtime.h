@@ -209,6 +209,10 @@ struct stats_state
 	dbuf out_counts, out_states; // compacted fixed points (finalize)
 	dbuf bin_keys, bin_vals, out_bin_keys, out_bin_vals; // sparse bins (more than 20 non-internal nodes)
 	unsigned bin_cap = 0;
+	// host copies of the sorted bins, kept across runs (no re-allocation, no first-touch page faults)
+	std::unique_ptr<uint64_t[]> hbin_keys;
+	std::unique_ptr<long long[]> hbin_vals;
+	size_t hbin_cap = 0;
 	bool wide = false;
 	unsigned fp_cap = 0;
 	int n_windows = 0;

@@ -1,0 +1,22 @@
+// Host side of the sparse window bins (more than 20 non-internal nodes): the bin table's
+// (key, value) pairs, sorted on the device, turned into a result's per-window entries and final
+// states. Plain C++ (no CUDA types), so the CPU tests compile and check it directly.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+namespace mb {
+
+// keys: two u64 per bin, {index bits 0-63, index bits 64-111 | (window + 1) << 48}, sorted by
+// (second, first) word, i.e. by window then index; vals: the bins' sums. Equal adjacent keys are
+// added together. Bins of window n_windows are final states (their sums are counts); the others
+// become (sp_w, sp_idx, sp_val) entries with sp_begin[w] = the first entry of window w
+// (n_windows + 1 values). The work is split over at most `threads` host threads, at key boundaries.
+void decode_sorted_bins(const uint64_t* keys, const long long* vals, size_t n, int n_windows, int threads,
+						std::vector<int>& sp_w, std::vector<unsigned __int128>& sp_idx,
+						std::vector<long long>& sp_val, std::vector<size_t>& sp_begin,
+						std::vector<unsigned __int128>& fin_idx, std::vector<unsigned>& fin_cnt);
+
+} // namespace mb
