@@ -9,12 +9,14 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <thread>
 
 #include "batch.h"
 #include "codegen.h"
 #include "model.h"
 #include "output.h"
 #include "runtime.h"
+#include "sparse_bins.h"
 
 struct mb_model_s
 {
@@ -1084,20 +1086,23 @@ mb_status mb_result_sparse_windows(mb_result r, int* windows, uint64_t* states, 
 	return guard([&] {
 		need(r, "null result");
 		const mb::result& x = *r->res;
-		for (size_t i = 0; i < x.sp_w.size(); i++)
-		{
-			if (windows)
-				windows[i] = x.sp_w[i];
-			if (states)
+		// independent entries (tens of millions for a large job): copied by host threads
+		mb::parallel_ranges(x.sp_w.size(), (int)std::thread::hardware_concurrency(), [&](size_t a, size_t e) {
+			for (size_t i = a; i < e; i++)
 			{
-				states[2 * i] = (uint64_t)x.sp_idx[i];
-				states[2 * i + 1] = (uint64_t)(x.sp_idx[i] >> 64);
+				if (windows)
+					windows[i] = x.sp_w[i];
+				if (states)
+				{
+					states[2 * i] = (uint64_t)x.sp_idx[i];
+					states[2 * i + 1] = (uint64_t)(x.sp_idx[i] >> 64);
+				}
+				if (raw)
+					raw[i] = x.sp_val[i];
+				if (probs)
+					probs[i] = x.sparse_prob(i);
 			}
-			if (raw)
-				raw[i] = x.sp_val[i];
-			if (probs)
-				probs[i] = x.sparse_prob(i);
-		}
+		});
 	});
 }
 

@@ -102,4 +102,10 @@ void decode_sorted_bins(const uint64_t* keys, const long long* vals, size_t n, i
 		sp_begin[w] = (size_t)(std::lower_bound(sp_w.begin(), sp_w.end(), w) - sp_w.begin());
 }
 
+void parallel_ranges(size_t n, int threads, const std::function<void(size_t, size_t)>& f)
+{
+	const int T = n < ((size_t)1 << 16) ? 1 : std::max(1, std::min(threads, 64));
+	parallel(T, [&](int t) { f(n * (size_t)t / (size_t)T, n * (size_t)(t + 1) / (size_t)T); });
+}
+
 } // namespace mb

@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <functional>
 #include <vector>
 
 namespace mb {
@@ -18,5 +19,9 @@ void decode_sorted_bins(const uint64_t* keys, const long long* vals, size_t n, i
 						std::vector<int>& sp_w, std::vector<unsigned __int128>& sp_idx,
 						std::vector<long long>& sp_val, std::vector<size_t>& sp_begin,
 						std::vector<unsigned __int128>& fin_idx, std::vector<unsigned>& fin_cnt);
+
+// f(begin, end) over [0, n) in contiguous ranges, one per host thread (at most `threads`; one
+// range on the calling thread for small n). The ranges cover every index exactly once.
+void parallel_ranges(size_t n, int threads, const std::function<void(size_t, size_t)>& f);
 
 } // namespace mb

@@ -29,6 +29,10 @@ extern "C" int decode(const uint64_t* keys, const long long* vals, size_t n, int
         fin_cnt[i] = fc[i]; }
     return 0;
 }
+extern "C" void ranges(size_t n, int threads, unsigned* hits)
+{
+    mb::parallel_ranges(n, threads, [&](size_t a, size_t b) { for (size_t i = a; i < b; i++) hits[i]++; });
+}
 """
 
 
@@ -42,6 +46,7 @@ def decoder(tmp_path_factory):
                     str(d / "shim.cpp"), os.path.join(csrc, "sparse_bins.cpp")], check=True, timeout=300)
     L = C.CDLL(str(so))
     L.decode.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_int] + [C.c_void_p] * 7
+    L.ranges.argtypes = [C.c_size_t, C.c_int, C.c_void_p]
     return L
 
 
@@ -108,3 +113,10 @@ def test_decode_sorted_bins_equals_sequential_restatement(decoder, n, threads, d
     assert begin.tolist() == rbegin
     assert [tuple(x) for x in fi.tolist()] == rfi
     assert fc.tolist() == rfc
+
+
+@pytest.mark.parametrize("n,threads", [(0, 8), (5, 8), (65_535, 8), (65_536, 7), (1_000_003, 16), (200_000, 0)])
+def test_parallel_ranges_cover_every_index_once(decoder, n, threads):
+    hits = np.zeros(max(1, n), np.uint32)
+    decoder.ranges(n, threads, hits.ctypes.data)
+    assert np.all(hits[:n] == 1)
