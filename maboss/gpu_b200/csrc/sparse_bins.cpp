@@ -16,17 +16,24 @@ inline unsigned __int128 index_of(const uint64_t* k, size_t i)
 
 inline bool same_key(const uint64_t* k, size_t a, size_t b) { return k[2 * a] == k[2 * b] && k[2 * a + 1] == k[2 * b + 1]; }
 
+// f(0) .. f(T - 1): chunk 0 on the calling thread, the others on new threads; a chunk whose thread
+// cannot be created runs on the calling thread too, and every started thread is joined
 template <typename F>
 void parallel(int T, F f)
 {
-	if (T == 1)
-	{
-		f(0);
-		return;
-	}
 	std::vector<std::thread> pool;
-	for (int t = 0; t < T; t++)
-		pool.emplace_back(f, t);
+	int t = 1;
+	try
+	{
+		for (; t < T; t++)
+			pool.emplace_back(f, t);
+	}
+	catch (...)
+	{
+	}
+	for (int u = t; u < T; u++)
+		f(u);
+	f(0);
 	for (auto& th : pool)
 		th.join();
 }
