@@ -73,11 +73,24 @@ void decode_sorted_bins(const uint64_t* keys, const long long* vals, size_t n, i
 		ow[t + 1] = ow[t] + nw[t];
 		of[t + 1] = of[t] + nf[t];
 	}
-	sp_w.resize(ow[T]);
-	sp_idx.resize(ow[T]);
-	sp_val.resize(ow[T]);
-	fin_idx.resize(of[T]);
-	fin_cnt.resize(of[T]);
+	// resize value-initialises (gigabytes for a large job): the two largest vectors on their own threads
+	auto size_part = [&](int part) {
+		if (part == 0)
+			sp_idx.resize(ow[T]);
+		else if (part == 1)
+			sp_val.resize(ow[T]);
+		else
+		{
+			sp_w.resize(ow[T]);
+			fin_idx.resize(of[T]);
+			fin_cnt.resize(of[T]);
+		}
+	};
+	if (T > 1)
+		parallel(3, size_part);
+	else
+		for (int part = 0; part < 3; part++)
+			size_part(part);
 	// pass 2: each chunk writes its entries at its offsets, adding equal adjacent keys
 	parallel(T, [&](int t) {
 		size_t a = ow[t], b = of[t];
