@@ -1,6 +1,8 @@
 #include "sparse_bins.h"
 
 #include <algorithm>
+#include <exception>
+#include <mutex>
 #include <thread>
 
 namespace mb {
@@ -16,26 +18,55 @@ inline unsigned __int128 index_of(const uint64_t* k, size_t i)
 
 inline bool same_key(const uint64_t* k, size_t a, size_t b) { return k[2 * a] == k[2 * b] && k[2 * a + 1] == k[2 * b + 1]; }
 
+} // namespace
+
 // f(0) .. f(T - 1): chunk 0 on the calling thread, the others on new threads; a chunk whose thread
-// cannot be created runs on the calling thread too, and every started thread is joined
-template <typename F>
-void parallel(int T, F f)
+// cannot be created runs on the calling thread too. Every chunk runs inside a catch: an exception
+// (std::bad_alloc from a resize, say) is kept, every started thread is joined, and then the first
+// exception is rethrown on the calling thread, so it reaches the C ABI's error translation instead
+// of std::terminate.
+void parallel_for(int T, const std::function<void(int)>& f)
 {
+	std::mutex m;
+	std::exception_ptr first;
+	auto guarded = [&](int t) {
+		try
+		{
+			f(t);
+		}
+		catch (...)
+		{
+			std::lock_guard<std::mutex> lock(m);
+			if (!first)
+				first = std::current_exception();
+		}
+	};
 	std::vector<std::thread> pool;
 	int t = 1;
 	try
 	{
+		pool.reserve(T > 1 ? (size_t)(T - 1) : 0);
 		for (; t < T; t++)
-			pool.emplace_back(f, t);
+			pool.emplace_back(guarded, t);
 	}
 	catch (...)
 	{
 	}
 	for (int u = t; u < T; u++)
-		f(u);
-	f(0);
+		guarded(u);
+	guarded(0);
 	for (auto& th : pool)
 		th.join();
+	if (first)
+		std::rethrow_exception(first);
+}
+
+namespace {
+
+template <typename F>
+void parallel(int T, F f)
+{
+	parallel_for(T, std::function<void(int)>(std::move(f)));
 }
 
 } // namespace

@@ -20,6 +20,11 @@ void decode_sorted_bins(const uint64_t* keys, const long long* vals, size_t n, i
 						std::vector<long long>& sp_val, std::vector<size_t>& sp_begin,
 						std::vector<unsigned __int128>& fin_idx, std::vector<unsigned>& fin_cnt);
 
+// f(0) .. f(T - 1), chunk 0 on the calling thread and the others on their own threads (on the
+// calling thread when a thread cannot be created). Returns after every chunk has finished; if any
+// chunk threw, the first exception is rethrown then (never std::terminate).
+void parallel_for(int T, const std::function<void(int)>& f);
+
 // f(begin, end) over [0, n) in contiguous ranges, one per host thread (at most `threads`; one
 // range on the calling thread for small n). The ranges cover every index exactly once.
 void parallel_ranges(size_t n, int threads, const std::function<void(size_t, size_t)>& f);

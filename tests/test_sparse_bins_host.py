@@ -14,6 +14,7 @@ from conftest import ROOT
 SHIM = r"""
 #include "sparse_bins.h"
 #include <cstring>
+#include <stdexcept>
 extern "C" int decode(const uint64_t* keys, const long long* vals, size_t n, int n_windows, int threads,
                       int* sp_w, uint64_t* sp_idx, long long* sp_val, size_t* sp_begin, uint64_t* fin_idx,
                       unsigned* fin_cnt, size_t* counts)
@@ -27,6 +28,23 @@ extern "C" int decode(const uint64_t* keys, const long long* vals, size_t n, int
     for (size_t i = 0; i < begin.size(); i++) sp_begin[i] = begin[i];
     for (size_t i = 0; i < fi.size(); i++) { fin_idx[2 * i] = (uint64_t)fi[i]; fin_idx[2 * i + 1] = (uint64_t)(fi[i] >> 64);
         fin_cnt[i] = fc[i]; }
+    return 0;
+}
+extern "C" int throwing(int T, int bad, unsigned* hits)
+{
+    // every chunk records that it ran; chunk `bad` then throws (bad == 0: the calling thread's chunk)
+    try
+    {
+        mb::parallel_for(T, [&](int t) {
+            __atomic_fetch_add(&hits[t], 1u, __ATOMIC_RELAXED);
+            if (t == bad)
+                throw std::runtime_error("chunk failed");
+        });
+    }
+    catch (const std::runtime_error& e)
+    {
+        return std::strcmp(e.what(), "chunk failed") == 0 ? 1 : 2;
+    }
     return 0;
 }
 extern "C" void ranges(size_t n, int threads, unsigned* hits)
@@ -47,6 +65,7 @@ def decoder(tmp_path_factory):
     L = C.CDLL(str(so))
     L.decode.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_int] + [C.c_void_p] * 7
     L.ranges.argtypes = [C.c_size_t, C.c_int, C.c_void_p]
+    L.throwing.argtypes = [C.c_int, C.c_int, C.c_void_p]
     return L
 
 
@@ -120,3 +139,12 @@ def test_parallel_ranges_cover_every_index_once(decoder, n, threads):
     hits = np.zeros(max(1, n), np.uint32)
     decoder.ranges(n, threads, hits.ctypes.data)
     assert np.all(hits[:n] == 1)
+
+
+@pytest.mark.parametrize("T,bad", [(1, 0), (4, 0), (4, 3), (8, 5), (64, 63)])
+def test_parallel_for_rethrows_after_joining(decoder, T, bad):
+    """A chunk that throws (a failed allocation, say) neither terminates the process nor leaves
+    threads unjoined: every chunk still runs once and the exception reaches the caller."""
+    hits = np.zeros(T, np.uint32)
+    assert decoder.throwing(T, bad, hits.ctypes.data) == 1
+    assert np.array_equal(hits, np.ones(T, np.uint32))
