@@ -143,8 +143,9 @@ void batch_engine::compute_rates(variant& V) const
 	}
 	const incremental_tables t = build_incremental_tables(L, V.rates.up, V.rates.down);
 	if (!t.ok)
-		throw engine_error(MB_ERR_INVALID, "rates must be finite, non-negative, and positive rates within 2^20 of "
-										   "the largest one");
+		throw engine_error(MB_ERR_INVALID, "rates must be finite and non-negative, with every positive rate at least "
+										   "2^20 units of the fixed point in which each state word's rate sum stays "
+										   "below 2^32 (rates within a factor of about 4096 of a word's rate sum)");
 	V.rate_shift = t.rate_shift;
 	V.q = t.q;
 }

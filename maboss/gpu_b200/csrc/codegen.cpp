@@ -257,6 +257,9 @@ void emit_incremental_tables(std::ostream& ss, const model_layout& L)
 		return out;
 	};
 	ss << "#define MBG_INCREMENTAL 1" << std::endl;
+	// the fast kernel's integer rates (else fast mode takes the dense fp32 kernel)
+	if (t.ok && L.integer_rates_ok)
+		ss << "#define MBG_INTEGER_RATES 1" << std::endl;
 	ss << "constexpr int mbg_inc_rate_shift = " << t.rate_shift << ";" << std::endl;
 	// the node records split in two 8-byte tables: (q_up, q_down) of every node alone: the flip selection scans these (8 bytes per node stay in L1)
 	std::vector<unsigned> q2;
@@ -425,7 +428,8 @@ model_layout analyze_model(const model_t& m)
 	// incremental tables (fast-path models with small logic fan-in only)
 	// the incremental kernels keep 12 bytes of shared memory per state word and thread: at most 600
 	// words (19200 nodes) fit a block of 32 threads; larger models take the dense kernels
-	L.incremental_ok = L.all_fast_path && N <= 65535 && L.state_words <= 600;
+	// (the incremental exact kernel's binary search over word-end rate sums needs rates >= 0)
+	L.incremental_ok = L.all_fast_path && L.rates_nonnegative && N <= 65535 && L.state_words <= 600;
 	constexpr int max_inputs = 12;
 	if (L.incremental_ok)
 	{
@@ -488,31 +492,20 @@ model_layout analyze_model(const model_t& m)
 		}
 		if (L.incremental_ok)
 		{
-			// fixed-point scale: every word's largest possible rate sum stays below 2^31
-			double worst = 0;
-			for (int w = 0; w < L.state_words; w++)
-			{
-				double sw = 0;
-				for (int i = 32 * w; i < std::min(N, 32 * w + 32); i++)
-					sw += std::max((double)L.up[i], (double)L.down[i]);
-				worst = std::max(worst, sw);
-			}
-			int shift = 30;
-			while (shift > 0 && worst * std::ldexp(1.0, shift) >= 2147483648.0)
-				shift--;
-			L.rate_shift = shift;
+			L.rate_shift = integer_rate_shift(L.up, L.down, L.state_words);
 			L.q_up.resize(N);
 			L.q_down.resize(N);
-			for (int i = 0; i < N && L.incremental_ok; i++)
+			L.integer_rates_ok = true;
+			for (int i = 0; i < N; i++)
 			{
 				for (int which = 0; which < 2; which++)
 				{
 					const double r = which ? L.down[i] : L.up[i];
-					const double q = std::nearbyint(r * std::ldexp(1.0, shift));
-					// positive rates need enough resolution (relative error below 2^-10)
-					if (r > 0 && q < 1024.0)
-						L.incremental_ok = false;
-					(which ? L.q_down[i] : L.q_up[i]) = (unsigned)q;
+					const double q = std::nearbyint(std::max(0.0, r) * std::ldexp(1.0, L.rate_shift));
+					// positive rates need enough resolution (relative rounding error at most 2^-21)
+					if (!(r >= 0.0) || (r > 0 && q < integer_rate_min_units))
+						L.integer_rates_ok = false;
+					(which ? L.q_down[i] : L.q_up[i]) = (unsigned)std::min(q, 4294967295.0);
 				}
 			}
 		}
@@ -570,23 +563,29 @@ rate_set fast_rates(const model_t& m, const std::map<std::string, float>& variab
 	return r;
 }
 
+int integer_rate_shift(const std::vector<float>& up, const std::vector<float>& down, int state_words)
+{
+	const int N = (int)up.size();
+	double worst = 0;
+	for (int w = 0; w < state_words; w++)
+	{
+		double sw = 0;
+		for (int i = 32 * w; i < std::min(N, 32 * w + 32); i++)
+			sw += std::max(std::max((double)up[i], (double)down[i]), 0.0);
+		worst = std::max(worst, sw);
+	}
+	int shift = 31;
+	while (shift > 0 && worst * std::ldexp(1.0, shift) >= 4294967296.0)
+		shift--;
+	return shift;
+}
+
 incremental_tables build_incremental_tables(const model_layout& L, const std::vector<float>& up,
 											const std::vector<float>& down)
 {
 	incremental_tables t;
 	const int N = L.state_size;
-	// fixed-point scale: every word's largest possible rate sum stays below 2^31
-	double worst = 0;
-	for (int w = 0; w < L.state_words; w++)
-	{
-		double sw = 0;
-		for (int i = 32 * w; i < std::min(N, 32 * w + 32); i++)
-			sw += std::max((double)up[i], (double)down[i]);
-		worst = std::max(worst, sw);
-	}
-	int shift = 30;
-	while (shift > 0 && worst * std::ldexp(1.0, shift) >= 2147483648.0)
-		shift--;
+	const int shift = integer_rate_shift(up, down, L.state_words);
 	t.rate_shift = shift;
 	t.ok = true;
 	std::vector<unsigned> qu(N), qd(N);
@@ -598,9 +597,9 @@ incremental_tables build_incremental_tables(const model_layout& L, const std::ve
 			if (!(r >= 0.0))
 				t.ok = false;
 			const double q = std::nearbyint(std::max(0.0, r) * std::ldexp(1.0, shift));
-			if (r > 0 && q < 1024.0)
+			if (r > 0 && q < integer_rate_min_units)
 				t.ok = false;
-			(which ? qd[i] : qu[i]) = (unsigned)q;
+			(which ? qd[i] : qu[i]) = (unsigned)std::min(q, 4294967295.0);
 		}
 		t.q.push_back(qu[i]);
 		t.q.push_back(qd[i]);

@@ -46,6 +46,10 @@ struct model_layout
 	std::vector<int> dep_ptr, dep_idx;		// nodes whose rate must be re-evaluated after a flip
 	int rate_shift = 0;						// fast-mode rates in fixed point: q = round(rate * 2^shift)
 	std::vector<unsigned> q_up, q_down;
+	// The fast kernel's integer rates are usable (valid when `incremental_ok`): every state word's
+	// largest rate sum is below 2^32 units and every positive rate is at least 2^20 units (relative
+	// rounding error at most 2^-21). Otherwise fast mode takes the dense fp32 kernel.
+	bool integer_rates_ok = false;
 
 	int windows() const; // ceil(max_time / time_tick) in float, window_average_small.cpp:305
 };
@@ -70,7 +74,7 @@ rate_set fast_rates(const model_t& m, const std::map<std::string, float>& variab
 struct incremental_tables
 {
 	int rate_shift = 0;
-	bool ok = false; // rates representable (every positive rate >= 2^10 units)
+	bool ok = false; // rates representable (rates finite and >= 0, word sums < 2^32 units, every positive rate >= 2^20 units)
 	std::vector<unsigned> node, hdr, in1, in2; // uint4 records, 4 words each
 	// compact dependent records (the NVRTC kernels): {k | m << 16 | (ni_pos(k) + 1) << 21, truth
 	// table or offset, inputs 0-1, inputs 2-3}, and inputs 4-11 of records with more than 4 inputs
@@ -79,6 +83,12 @@ struct incremental_tables
 	std::vector<int> self;
 	std::vector<unsigned> q; // (q_up, q_down) per node
 };
+// The fixed-point scale of the integer rates: the largest shift <= 31 with every state word's
+// largest possible rate sum (the larger of up and down per node) below 2^32 units, and the least
+// number of units a positive rate must get (2^20: relative rounding error at most 2^-21).
+int integer_rate_shift(const std::vector<float>& up, const std::vector<float>& down, int state_words);
+constexpr double integer_rate_min_units = 1048576.0;
+
 incremental_tables build_incremental_tables(const model_layout& L, const std::vector<float>& up,
 											const std::vector<float>& down);
 

@@ -233,7 +233,7 @@ __device__ __forceinline__ void mb_fused_body(const mb_fused_params& P)
 }
 
 
-#ifdef MBG_INCREMENTAL
+#if defined(MBG_INCREMENTAL) && defined(MBG_INTEGER_RATES)
 // ---------------------------------------------------------------- incremental fast kernel
 // Fast mode for models whose rates all have the form `@logic ? U : 0` / `@logic ? 0 : D`.
 // A node is unstable when its bit differs from its logic; only unstable nodes have a rate
@@ -401,7 +401,7 @@ __device__ __forceinline__ void mb_incr_start(const mb_fused_params& P, const mb
 	__syncwarp();
 }
 
-#endif // MBG_INCREMENTAL
+#endif // MBG_INCREMENTAL && MBG_INTEGER_RATES
 
 #if defined(MBG_INCREMENTAL) && (defined(MB_FAMILY_EXACT) || (defined(MB_FAMILY_EPOCH) && !defined(MB_EPOCH_DENSE)))
 // ---- the exact algorithm on incremental unstable sets (models whose rates all have the @logic form)
@@ -742,7 +742,9 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 #endif // MB_FAMILY_EXACT
 
 #ifdef MB_FAMILY_FAST
-#ifndef MBG_INCREMENTAL
+#if !defined(MBG_INCREMENTAL) || !defined(MBG_INTEGER_RATES)
+// dense fast kernel: models outside the @logic rate form, and @logic models whose rates the
+// integer fixed point cannot hold to 2^-21 (rates spanning more than about 2^12 within a word sum)
 extern "C" __global__ void __launch_bounds__(256) mb_fused_fast(mb_fused_params P) { mb_fused_body<false>(P); }
 #else
 // at least 5 resident blocks of 128: 89 registers on the 1000-node network, no spills. Measured
@@ -992,7 +994,7 @@ extern "C" __global__ void __launch_bounds__(128, 5) mb_fused_fast(mb_fused_para
 				atomicAdd(reinterpret_cast<unsigned long long*>(P.st.win_h + i), (unsigned long long)smem_h[i]);
 	}
 }
-#endif // MBG_INCREMENTAL
+#endif // MBG_INCREMENTAL && MBG_INTEGER_RATES
 #endif // MB_FAMILY_FAST
 
 // ---------------------------------------------------------------- buffered epoch kernels (SoA)

@@ -251,6 +251,7 @@ std::unique_ptr<module> compile_module(context& ctx, const std::string& generate
 	m->state_words = parse_constexpr(generated_code, "state_words", -1);
 	m->noninternal_count = parse_constexpr(generated_code, "mbg_noninternal_count", -1);
 	m->incremental = generated_code.find("#define MBG_INCREMENTAL 1") != std::string::npos;
+	m->integer_rates = generated_code.find("#define MBG_INTEGER_RATES 1") != std::string::npos;
 	m->source = generated_code;
 	// the fast family is compiled now so that errors in the generated code surface here
 	m->ensure(FAMILY_FAST);
@@ -831,7 +832,7 @@ unsigned launch_fused(module& m, const run_config& c, stats_state& st, long long
 	}
 	int block = c.block;
 	size_t smem = st.h_smem();
-	if (m.incremental)
+	if (c.mode == MB_MODE_FUSED_EXACT ? m.incremental : m.fast_incremental())
 	{
 		// per thread in shared memory: state words, unstable masks and word rate sums
 		const size_t per_word = 12;
@@ -1073,10 +1074,11 @@ std::vector<tuned_shape> autotune(module& m, const run_config& c)
 	// candidate shapes: the incremental kernels take at most 128 threads and 12 bytes of shared memory
 	// per state word and thread; the dense kernels any multiple of 32 up to 256
 	std::vector<std::pair<int, int>> cands;
-	const std::vector<int> blocks = m.incremental ? std::vector<int>{ 128, 96, 64 } : std::vector<int>{ 256, 128 };
+	const bool incr = c.mode == MB_MODE_FUSED_EXACT ? m.incremental : m.fast_incremental();
+	const std::vector<int> blocks = incr ? std::vector<int>{ 128, 96, 64 } : std::vector<int>{ 256, 128 };
 	for (int block : blocks)
 	{
-		size_t smem = m.incremental ? (size_t)12 * m.state_words * block : 0;
+		size_t smem = incr ? (size_t)12 * m.state_words * block : 0;
 		if (smem > 227 * 1024)
 			continue;
 		MB_CUDA(cudaSetDevice(m.ctx->device));

@@ -82,7 +82,9 @@ struct module
 	CUmodule mods[FAMILY_COUNT] = { nullptr, nullptr, nullptr, nullptr };
 	int state_size = 0, state_words = 0;
 	int noninternal_count = -1; // from the generated code (mbg_noninternal_count), -1 if absent
-	bool incremental = false;	// fast mode uses the incremental kernel (generated MBG_INCREMENTAL)
+	bool incremental = false;	// @logic-form model: exact and epoch modes use the incremental kernels (generated MBG_INCREMENTAL)
+	bool integer_rates = false; // fast mode's incremental kernel too (generated MBG_INTEGER_RATES), else its dense kernel
+	bool fast_incremental() const { return incremental && integer_rates; }
 	bool has_layout = false; // compiled from a model (full layout known)
 	model_layout layout;
 	std::string source; // generated model source that was compiled with the engine

@@ -857,25 +857,28 @@ void setup_integer_rates(compiled& cc)
 			c->integer_rates = false;
 	if (c->integer_rates)
 	{
+		// the engine's rule (codegen.cpp: integer_rate_shift): the largest shift <= 31 with every
+		// word's largest rate sum below 2^32 units; every positive rate at least 2^20 units
 		double worst = 0;
 		for (int w = 0; w < c->W; w++)
 		{
 			double sw = 0;
 			for (int i = 32 * w; i < std::min(c->N, 32 * w + 32); i++)
-				sw += std::max((double)c->up[i], (double)c->down[i]);
+				sw += std::max(std::max((double)c->up[i], (double)c->down[i]), 0.0);
 			worst = std::max(worst, sw);
 		}
-		int sh = 30;
-		while (sh > 0 && worst * std::ldexp(1.0, sh) >= 2147483648.0)
+		int sh = 31;
+		while (sh > 0 && worst * std::ldexp(1.0, sh) >= 4294967296.0)
 			sh--;
 		c->shift = sh;
 		c->q_up.resize(c->N);
 		c->q_down.resize(c->N);
 		for (int i = 0; i < c->N; i++)
 		{
-			const double qu = std::nearbyint((double)c->up[i] * std::ldexp(1.0, sh));
-			const double qd = std::nearbyint((double)c->down[i] * std::ldexp(1.0, sh));
-			if ((c->up[i] > 0 && qu < 1024.0) || (c->down[i] > 0 && qd < 1024.0))
+			const double qu = std::nearbyint(std::max(0.0, (double)c->up[i]) * std::ldexp(1.0, sh));
+			const double qd = std::nearbyint(std::max(0.0, (double)c->down[i]) * std::ldexp(1.0, sh));
+			if (!(c->up[i] >= 0.f) || !(c->down[i] >= 0.f) || (c->up[i] > 0 && qu < 1048576.0) ||
+				(c->down[i] > 0 && qd < 1048576.0))
 				c->integer_rates = false;
 			c->q_up[i] = (unsigned)qu;
 			c->q_down[i] = (unsigned)qd;

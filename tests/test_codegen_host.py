@@ -50,6 +50,11 @@ extern "C" int host_nonnegative() { return mbg_rates_nonnegative ? 1 : 0; }
 #ifdef MBG_INCREMENTAL
 extern "C" int host_has_tables() { return 1; }
 extern "C" int host_rate_shift() { return mbg_inc_rate_shift; }
+#ifdef MBG_INTEGER_RATES
+extern "C" int host_integer_rates() { return 1; }
+#else
+extern "C" int host_integer_rates() { return 0; }
+#endif
 extern "C" unsigned host_q(int e) { return mbg_inc_q[e]; }
 extern "C" float host_inc_rate(int e) { return mbg_inc_rate[e]; }
 // logic of record r's node in state s: the truth table indexed by the input pattern
@@ -101,7 +106,8 @@ def _compile(code: str, tmp_path, tag: str) -> C.CDLL:
         getattr(L, name).restype = res
         getattr(L, name).argtypes = args
     if L.host_has_tables():
-        for name, res, args in [("host_rate_shift", C.c_int, []), ("host_q", C.c_uint, [C.c_int]),
+        for name, res, args in [("host_rate_shift", C.c_int, []), ("host_integer_rates", C.c_int, []),
+                                ("host_q", C.c_uint, [C.c_int]),
                                 ("host_inc_rate", C.c_float, [C.c_int]),
                                 ("host_record_logic", C.c_int, [C.c_int, u32p]),
                                 ("host_record_node", C.c_int, [C.c_int]), ("host_record_ni", C.c_int, [C.c_int]),
@@ -140,6 +146,13 @@ def _check_model(bnd, cfg, tmp_path, tag, n_states=200, n_flip_states=20):
         for e in range(2 * N):
             r = np.float64(L.host_inc_rate(e))
             assert L.host_q(e) == int(np.rint(r * 2.0 ** shift)), (tag, e)
+        # the fixed point: the largest shift <= 31 keeping every word's largest rate sum below
+        # 2^32; the fast kernel's integer rates only when every positive rate gets >= 2^20 units
+        hi = [max(float(L.host_inc_rate(2 * i)), float(L.host_inc_rate(2 * i + 1))) for i in range(N)]
+        worst = max(sum(hi[32 * w:32 * w + 32]) for w in range(W))
+        assert worst * 2.0 ** shift < 2.0 ** 32 and (shift == 31 or worst * 2.0 ** (shift + 1) >= 2.0 ** 32)
+        fine = all(L.host_q(e) >= 2 ** 20 for e in range(2 * N) if L.host_inc_rate(e) > 0)
+        assert bool(L.host_integer_rates()) == fine, tag
         ni_pos = {node: k for k, node in enumerate(o.noninternal)}
         deps = []
         for j in range(N):
@@ -275,3 +288,28 @@ def test_generated_code_of_random_models(seed, tmp_path):
     """Even seeds: every rate of the @logic form (the tables are checked too); odd seeds: general
     expressions, which leave the model to the dense kernels."""
     assert _check_model(*_random_model(seed), tmp_path, f"rand{seed}", n_states=60) == (seed % 2 == 0)
+
+
+def wide_span_model(n=40, seed=7):
+    """A @logic-form network whose rates span 1e-3 ... 1e3 (log-uniform): too wide for 2^20 units of
+    the integer fixed point, so fast mode takes the dense fp32 kernel; exact mode keeps the
+    incremental kernel."""
+    rng = np.random.default_rng(seed)
+    names = [f"S{i}" for i in range(n)]
+    bnd = ""
+    for i in range(n):
+        a, b = rng.choice(n, 2, replace=False)
+        op = " & " if rng.random() < 0.5 else " | "
+        logic = f"{'!' if rng.random() < 0.5 else ''}{names[a]}{op}{'!' if rng.random() < 0.5 else ''}{names[b]}"
+        up, down = 10.0 ** rng.uniform(-3, 3, 2)
+        bnd += (f"node {names[i]} {{ logic = {logic}; rate_up = @logic ? {up:.6g} : 0; "
+                f"rate_down = @logic ? 0 : {down:.6g}; }}\n")
+    cfg = "".join(f"{names[i]}.is_internal = 1;\n" for i in range(6, n))
+    cfg += "max_time = 10; time_tick = 0.5; sample_count = 1000;\n"
+    return bnd, cfg
+
+
+def test_generated_code_of_a_wide_rate_span_model(tmp_path):
+    assert _check_model(*wide_span_model(), tmp_path, "wide", n_states=100)
+    L = _compile(mb.Model(*wide_span_model()).generate_code(), tmp_path, "wide2")
+    assert L.host_integer_rates() == 0
