@@ -120,3 +120,31 @@ def test_oracle_sharding_is_additive():
     assert np.array_equal(full["occ"], a["occ"] + b["occ"])
     assert np.array_equal(full["final"], a["final"] + b["final"])
     assert full["transitions"] == a["transitions"] + b["transitions"]
+
+
+@pytest.mark.parametrize("name,n", CASES)
+def test_oracle_transition_entropy_matches_golden(name, n):
+    """Per-window transition entropy (TH, window_average_small.cpp:222-223: the window's summed
+    h * slice over the trajectories, divided by their number and, in continuous time, by the tick)
+    against the `transition_entropy` of each window of the golden dump.
+
+    TH is a mean over trajectories of X = (1/tick) * integral of h over the window (continuous) or
+    the h of the window's step (discrete), with 0 <= X <= log2(k) for k non-internal nodes (h is the
+    entropy of the normalised non-internal rates). So Var(X) <= E[X^2] <= log2(k) * E[X], which
+    bounds the standard error of each estimate without assuming a distribution; late windows where
+    only a few trajectories still move are covered by the same bound. Each window within 4.5 of
+    those combined standard errors (plus the golden's 6-significant-digit printing)."""
+    bnd, cfg = model_text(name)
+    m = OracleModel(bnd, cfg)
+    g = _golden(name)
+    th = m.run(n=n, threads=0)["th"]
+    gold = np.array([win["transition_entropy"] for win in g["windows"]])
+    assert gold.shape == th.shape
+    h_max = np.log2(max(m.k, 2))
+    mean = np.maximum(th, gold)
+    se = np.sqrt(h_max * mean * (1.0 / n + 1.0 / m.sample_count))
+    tol = 4.5 * se + 5e-6 * np.abs(gold) + 1e-7
+    bad = np.nonzero(np.abs(th - gold) > tol)[0]
+    assert bad.size == 0, (name, bad[:5], th[bad[:5]], gold[bad[:5]], se[bad[:5]])
+    # and the whole run's mean transition entropy (sum over windows) within the summed bound
+    assert abs(th.sum() - gold.sum()) <= 4.5 * np.sqrt(h_max * mean.sum() * len(th) * (1.0 / n + 1.0 / m.sample_count))
