@@ -686,6 +686,9 @@ struct compiled
 	bool integer_rates = false;
 	int shift = 0;
 	std::vector<unsigned> q_up, q_down;
+	// node -> the nodes whose rate a flip of it can change (itself and every node whose logic reads
+	// it), for the incremental restatement (trajectory_integer_incremental)
+	std::vector<std::vector<int>> deps;
 	bool discrete = false;
 	float max_time_f = 0, tick_f = 0;	  // exact floats (window statistics)
 	float max_time_sim = 0, tick_sim = 0; // 6-significant-digit constexprs used by simulate
@@ -882,6 +885,14 @@ void setup_integer_rates(compiled& cc)
 				c->integer_rates = false;
 			c->q_up[i] = (unsigned)qu;
 			c->q_down[i] = (unsigned)qd;
+		}
+		c->deps.assign(c->N, {});
+		for (int i = 0; i < c->N; i++)
+		{
+			c->deps[i].push_back(i);
+			for (int x : c->tt_in[i])
+				if (x != i)
+					c->deps[x].push_back(i);
 		}
 	}
 }
@@ -1169,6 +1180,136 @@ void trajectory_integer(const compiled& c, sinks& s, unsigned long long seed, un
 		if (trace)
 			trace->emplace_back(j, time);
 		st[j / 32] ^= 1u << (j % 32);
+	}
+	acc.add_fin(s, c.ni_index(st.data()));
+	if (fixed)
+	{
+#pragma omp critical(oracle_fixed)
+		s.fixed[st]++;
+	}
+}
+
+// The same process, random numbers and results as trajectory_integer (bit for bit), computed the
+// way the engine's incremental fast kernel does: the unstable nodes (bit != logic), the integer
+// rate sum of every state word and the total are kept across steps; after a flip only the
+// flipped node and the nodes whose logic reads it are re-evaluated, and the flip is found by
+// skipping whole words by their sums, then scanning the chosen word's unstable bits in node order
+// (the first node whose cumulative integer rate exceeds r, as the full scan finds it). This is
+// the CPU baseline on the GPU kernel's algorithm (mode 2); tests check it equals mode 1.
+void trajectory_integer_incremental(const compiled& c, sinks& s, unsigned long long seed, unsigned long long traj,
+									run_acc& acc, unsigned long long& trans)
+{
+	curandStatePhilox4_32_10_t rng;
+	curand_init(seed, traj, 0ull, &rng);
+	std::vector<uint32_t> st(c.W, 0u), un(c.W, 0u);
+	std::vector<unsigned long long> wsum(c.W, 0ull);
+	for (int i = 0; i < c.N; i++)
+		if (curand_uniform(&rng) <= c.m.nodes[i].istate)
+			st[i / 32] |= 1u << (i % 32);
+	auto logic = [&](int i) {
+		unsigned p = 0;
+		const std::vector<int>& in = c.tt_in[i];
+		for (size_t k = 0; k < in.size(); k++)
+			p |= ((st[in[k] / 32] >> (in[k] % 32)) & 1u) << k;
+		return ((c.tt[i][p >> 6] >> (p & 63)) & 1u) != 0;
+	};
+	auto q_of = [&](int i) -> unsigned {
+		if (!((un[i / 32] >> (i % 32)) & 1u))
+			return 0u;
+		return ((st[i / 32] >> (i % 32)) & 1u) ? c.q_down[i] : c.q_up[i];
+	};
+	unsigned long long total = 0;
+	for (int i = 0; i < c.N; i++)
+	{
+		const bool on = (st[i / 32] >> (i % 32)) & 1u;
+		if (on != logic(i))
+			un[i / 32] |= 1u << (i % 32);
+		const unsigned q = q_of(i);
+		wsum[i / 32] += q;
+		total += q;
+	}
+	// entropy_fast over the non-internal nodes: a node contributes when its integer rate is
+	// non-zero, which holds exactly when its float rate is (positive rates have >= 2^20 units)
+	auto entropy = [&]() {
+		float t = 0.f, tl = 0.f;
+		for (int i : c.ni)
+			if (q_of(i) != 0u)
+			{
+				const bool up = (st[i / 32] >> (i % 32)) & 1u;
+				t += up ? c.down[i] : c.up[i];
+				tl += up ? c.dl[i] : c.ul[i];
+			}
+		if (!(t > 0.f))
+			return 0.f;
+		const float h = log2f(t) - tl / t;
+		return h > 0.f ? h : 0.f;
+	};
+	const float inv_scale = 1.0f / (float)(1u << c.shift);
+	curand_init(seed, traj, (unsigned long long)((c.N + 3) & ~3), &rng);
+	float time = 0.f;
+	bool fixed = false;
+	for (;;)
+	{
+		const uint4 rb = curand4(&rng);
+		float h = 0.f, tn;
+		if (total == 0)
+		{
+			fixed = true;
+			tn = c.max_time_sim;
+		}
+		else
+		{
+			if (c.discrete)
+			{
+				tn = time + c.tick_sim;
+				tn = c.max_time_sim - c.tick_sim < tn ? c.max_time_sim : tn;
+			}
+			else
+			{
+				const float total_f = (float)total * inv_scale;
+				const float u = (float)((rb.x >> 8) + 1u) * 5.9604644775390625e-8f;
+				tn = time + -logf(u) / total_f;
+			}
+			tn = std::fmin(tn, c.max_time_sim);
+			h = entropy();
+		}
+		trans += tn != 0.f;
+		record(c, s, acc, c.ni_index(st.data()), time, tn, h);
+		time = tn;
+		if (time >= c.max_time_sim)
+			break;
+		const unsigned long long r64 = ((unsigned long long)rb.y << 32) | rb.z;
+		const unsigned long long r = (unsigned long long)(((unsigned __int128)r64 * total) >> 64);
+		unsigned long long cum = 0;
+		int w = 0;
+		while (w < c.W - 1 && r >= cum + wsum[w])
+			cum += wsum[w++];
+		int j = 32 * w + 31;
+		for (uint32_t um = un[w]; um; um &= um - 1u)
+		{
+			const int i = 32 * w + __builtin_ctz(um);
+			cum += q_of(i);
+			if (r < cum)
+			{
+				j = i;
+				break;
+			}
+		}
+		st[j / 32] ^= 1u << (j % 32);
+		for (int k : c.deps[j])
+		{
+			const unsigned qo = (k == j) ? ((((st[k / 32] >> (k % 32)) & 1u) ? c.q_up[k] : c.q_down[k]) *
+											 ((un[k / 32] >> (k % 32)) & 1u))
+										 : q_of(k);
+			const bool on = (st[k / 32] >> (k % 32)) & 1u;
+			if (on != logic(k))
+				un[k / 32] |= 1u << (k % 32);
+			else
+				un[k / 32] &= ~(1u << (k % 32));
+			const unsigned qn = q_of(k);
+			wsum[k / 32] += (unsigned long long)qn - qo;
+			total += (unsigned long long)qn - qo;
+		}
 	}
 	acc.add_fin(s, c.ni_index(st.data()));
 	if (fixed)
@@ -1525,6 +1666,8 @@ oracle_result* oracle_run_ex(const oracle_model* m, int mode, long long n, unsig
 				curand_init(seed, first + (unsigned long long)t, 0ull, &rng);
 				trajectory(c, s, rng, true, traj_len, acc, trans, nullptr);
 			}
+			else if (c.integer_rates && mode == 2)
+				trajectory_integer_incremental(c, s, seed, first + (unsigned long long)t, acc, trans);
 			else if (c.integer_rates)
 				trajectory_integer(c, s, seed, first + (unsigned long long)t, acc, trans, nullptr);
 			else

@@ -118,7 +118,8 @@ class OracleModel:
     def run(self, n: int | None = None, mode: int = 0, seed: int | None = None, first: int = 0,
             traj_len: int = 100, occ_exp: int | None = None, ent_exp: int | None = None,
             threads: int = 0, sparse: bool = False) -> dict:
-        """Simulate trajectories [first, first+n) on the CPU. mode 0 = exact, 1 = fast. With more than 20
+        """Simulate trajectories [first, first+n) on the CPU. mode 0 = exact, 1 = fast, 2 = fast computed
+        incrementally like the engine's fast kernel (same results as mode 1). With more than 20
         non-internal nodes (or sparse=True) the windows and final states come back as sparse entries
         under the key "sparse" (the dense arrays are then empty; states as (bits 0-63, bits 64-127) pairs)."""
         n = self.sample_count if n is None else n

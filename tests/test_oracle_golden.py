@@ -148,3 +148,19 @@ def test_oracle_transition_entropy_matches_golden(name, n):
     assert bad.size == 0, (name, bad[:5], th[bad[:5]], gold[bad[:5]], se[bad[:5]])
     # and the whole run's mean transition entropy (sum over windows) within the summed bound
     assert abs(th.sum() - gold.sum()) <= 4.5 * np.sqrt(h_max * mean.sum() * len(th) * (1.0 / n + 1.0 / m.sample_count))
+
+
+@pytest.mark.parametrize("gen,kw,n", [("c1", {}, 3000), ("c3", dict(sample_count=200), 200),
+                                      ("c4", {}, 2000), ("c2", dict(noninternal=20, discrete=True), 500)])
+def test_oracle_incremental_fast_mode_equals_fast_mode(gen, kw, n):
+    """Mode 2 (the fast process computed incrementally, as the engine's fast kernel does: unstable
+    sets, word sums, dependents only) gives the same trajectories as mode 1 (every rate each step),
+    integer for integer; it is the CPU baseline on the GPU kernel's own algorithm."""
+    from maboss.gpu_b200 import synth
+
+    bnd, cfg = getattr(synth, gen)(**kw)
+    m = OracleModel(bnd, cfg)
+    a, b = m.run(n=n, mode=1), m.run(n=n, mode=2)
+    assert a["transitions"] == b["transitions"] > 0
+    for k in ("occ", "cnt", "h", "final", "fixed_states", "fixed_counts"):
+        assert np.array_equal(a[k], b[k]), k
