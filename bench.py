@@ -11,6 +11,17 @@ window, final-state and fixed-point statistics). Default workload: the 1000-node
 Multi-GPU (torchrun, one process per GPU): every rank simulates its own block of trajectories
 (random streams first_traj = rank * n), no collective on the data path (weak scaling); the step
 time is the maximum over ranks.
+
+The default line also carries, measured after its timed region, the two other targets of the
+engine: `batched` (the 256-variant sweep in one persistent launch against running the variants one
+by one through the NVRTC-specialised kernel, with and without the per-variant compilation the
+reference needs) and `gradient` (the score-function gradient of the 50-node network against its
+forward simulation). `cpu_baseline` is the CPU restatement of the measured mode's own algorithm
+(fast mode: the incremental integer-rate process; exact mode: the reference's dense per-step
+algorithm) on all host cores.
+
+--impl reference runs the reference's own CUDA path (oracle/_ref/ref_run, built from its sources)
+on the same B200 and workload, through simulation_runner::run_simulation with its statistics.
 """
 from __future__ import annotations
 
@@ -35,7 +46,7 @@ def bytes_per_transition(words: int, ni_words: int) -> int:
 
 
 EXTRA_WORKLOADS = {
-    "c5": "batched sweep: 256 rate-perturbed variants (lognormal sigma 0.3) of 8 networks of 20-144 nodes, "
+    "c5": "batched sweep: 256 rate-perturbed variants (lognormal sigma 0.3) of 8 networks of 20-500 nodes, "
           "1e3-1e5 trajectories each, max_time 20-200, one persistent launch",
     "c4grad": "score-function gradient of the 50-node network w.r.t. 40 rate parameters, 1e6 trajectories",
 }
@@ -127,8 +138,14 @@ def make_workload(name: str, samples: int | None):
     return bnd, cfg, desc
 
 
+ORACLE_MODES = {0: "exact (the reference's dense per-step algorithm, XORWOW)",
+                1: "fast process, every rate re-evaluated each step",
+                2: "fast process computed incrementally as the GPU fast kernel does (unstable sets, word sums, "
+                   "dependents only)"}
+
+
 def cpu_baseline(bnd: str, cfg: str, sample: int, mode: int, threads: int) -> dict:
-    """The oracle (C++/OpenMP restatement of the reference algorithm) on a bounded sample."""
+    """The oracle (C++/OpenMP restatement of the path) on a bounded sample."""
     from oracle.oracle import OracleModel, build
     build()
     o = OracleModel(bnd, cfg)
@@ -138,31 +155,78 @@ def cpu_baseline(bnd: str, cfg: str, sample: int, mode: int, threads: int) -> di
     return {"value": r["transitions"] / dt, "transitions": r["transitions"], "seconds": dt, "trajectories": sample}
 
 
+def cpu_baseline_sized(bnd: str, cfg: str, mode: int, threads: int, target_s: float, cap: int) -> dict:
+    """cpu_baseline on a sample sized from a short probe to take about target_s seconds."""
+    probe = cpu_baseline(bnd, cfg, max(64, threads * 8), mode, threads)
+    per_traj = probe["seconds"] / probe["trajectories"]
+    sample = int(max(64, min(cap, target_s / max(per_traj, 1e-9))))
+    return cpu_baseline(bnd, cfg, sample, mode, threads)
+
+
+def reference_sample(n: int, state_words: int) -> int:
+    """Trajectories of the reference arm's runs: the workload's count, capped below the size at which
+    the reference's int buffer sizes and indices overflow (batch * 100 * state words <= INT_MAX,
+    simulation_runner.cu:68, window_average_small.cu:71), rounded down to a multiple of 10,000."""
+    cap = (2147483647 // (100 * state_words)) // 10_000 * 10_000
+    return min(n, cap)
+
+
 def run_reference(args) -> None:
+    """The reference's own CUDA build (oracle/_ref/ref_run) on this workload: W warm-up runs, then K
+    timed runs of simulation_runner::run_simulation with its three statistics plugins (device time
+    by CUDA events on the legacy stream it launches on; e2e: the host clock around run_simulation +
+    finalize, which includes its allocations, initial-state upload and result copies)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
+    from oracle import reference
+
     bnd, cfg, desc = make_workload(args.workload, args.samples)
-    cores = os.cpu_count() or 1
-    sample = args.cpu_sample
-    for _ in range(args.warmup):
-        cpu_baseline(bnd, cfg, max(1, sample // 10), 0, cores)
-    vals, trans, secs = [], 0, 0.0
-    for _ in range(args.steps):
-        b = cpu_baseline(bnd, cfg, sample, 0, cores)
-        vals.append(b["value"])
-        trans += b["transitions"]
-        secs += b["seconds"]
-    value = trans / secs
+    import torch
+
+    if not torch.cuda.is_available():
+        print(json.dumps({"impl": "reference", "unavailable": "no GPU on this host: the reference's path is CUDA "
+                                                              "code (its CUDA build runs on the B200)"}))
+        return
+    if not reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "the reference build oracle/_ref/ref_run is absent "
+                                                              "(built by oracle/refbuild from the reference sources)"}))
+        return
+    import maboss.gpu_b200 as mb
+
+    model = mb.Model(bnd, cfg)
+    n_work = int(args.samples or model.constant("sample_count"))
+    words = (model.num_nodes + 31) // 32
+    n = args.ref_samples or reference_sample(n_work, words)
+    try:
+        r = reference.run_text(bnd, cfg, samples=n, warmup=args.warmup, runs=args.steps, dump=False, timeout=3000)
+    except reference.Refused as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"the reference refuses this input: {e}"}))
+        return
+    dev_ms, host_ms = r["device_ms"], r["host_ms"]
+    value = r["transitions"] * len(dev_ms) / (sum(dev_ms) / 1e3)
+    e2e = r["transitions"] * len(host_ms) / (sum(host_ms) / 1e3)
+    if n == n_work:
+        which = "the whole workload"
+    else:
+        which = (f"of the workload's {n_work}: the largest multiple of 10,000 below the reference's int "
+                 f"overflow at batch * 100 * {words} state words")
+    sample = f"{n} trajectories per run ({which}), the reference's CUDA path on the B200"
     line = {
         "impl": "reference", "metric": "Gillespie transitions/s", "value": value, "unit": "transitions/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.workload}: {desc}", "sample_trajectories_per_step": sample},
-        "cpu_baseline": {"value": value, "unit": "transitions/s", "cores": cores, "kind": "port",
-                         "sample": f"{sample} trajectories of the workload per step (CPU oracle, exact mode, "
-                                   f"{cores} OpenMP threads); the reference ships no CPU implementation"},
-        "e2e": {"value": value, "unit": "transitions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": float(np.mean(dev_ms)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: {desc}", "trajectories": n, "workload_trajectories": n_work,
+                   "transitions_per_step": r["transitions"], "nvrtc_nvjitlink_compile_s": round(r["compile_s"], 2),
+                   "build": "reference sources (src/) compiled by oracle/refbuild, MAX_NODES=1024, sm_100, "
+                            "kernels NVRTC + nvJitLink LTO-linked at run time as the reference does",
+                   "l2": "not flushed (every run allocates and writes a trajectory buffer of "
+                         f"{n * 100 * (4 * words + 8) / 1e9:.1f} GB, larger than L2)"},
+        "cpu_baseline": {"value": value, "unit": "transitions/s", "cores": 0, "kind": "reference",
+                         "sample": sample + " (a GPU run: the reference has no CPU implementation of the path)"},
+        "e2e": {"value": e2e, "unit": "transitions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "host_ms_per_step": float(np.mean(host_ms))},
     }
     print(json.dumps(line), flush=True)
 
@@ -175,126 +239,172 @@ def _timed_line(args, value, ms_per_step, config, extra) -> dict:
     return line
 
 
-def run_batched(args) -> None:
-    """C5: one persistent launch over 256 variants, against running the variants one by one."""
+def batched_record(ctx, warmup: int, steps: int, per_variant_sample: int = 8) -> dict:
+    """C5: the 256-variant sweep in one persistent launch (graph replay) against the variants run one
+    by one through the NVRTC-specialised fast kernel of each variant (the reference bakes
+    $variables into its generated code, expressions.cpp:211-214, so every variant is a compilation:
+    timed with and without it) on a stated sample of variants (one per base network)."""
     import maboss.gpu_b200 as mb
     from maboss.gpu_b200 import synth
 
-    mb.build()
-    ctx = mb.Context(0)
     bases, variants = synth.c5_sweep()
     models = [mb.Model(*b) for b in bases]
     batch = mb.Batch(ctx)
     nets = [batch.add_model(m) for m in models]
     for net, params, n in variants:
         batch.add_variant(nets[net], n, params)
-    for _ in range(args.warmup):
+    for _ in range(max(1, warmup)):
         batch.run(0)  # the first run tunes the launch shape and captures the CUDA graph
-    clocks = ClockSampler(0)
-    clocks.start()
     ms, trans = [], 0
-    for step in range(args.steps):
+    for step in range(steps):
         ms.append(batch.run(step))
         trans += sum(batch.result(v).transitions for v in range(len(variants)))
-    clk = clocks.stop()
     value = trans / (sum(ms) / 1e3)
     info = batch.info
 
     # end to end: whole runs through the public API (graph launch: clears, kernel, extraction, copies
-    # to pinned memory; then every variant's result), wall clock, with and without the graph
-    def wall(b, reps=3):
-        t0 = time.perf_counter()
-        for i in range(reps):
-            b.run(100 + i)
-            for v in range(len(variants)):
-                b.result(v).final_counts
-        return (time.perf_counter() - t0) / reps
-
-    e2e_s = wall(batch)
-    nograph = mb.Batch(ctx)
-    nograph.set_options(use_graph=False, autotune=False)
-    ng_nets = [nograph.add_model(m) for m in models]
-    for net, params, n in variants:
-        nograph.add_variant(ng_nets[net], n, params)
-    nograph.run(0)
-    e2e_nograph_s = wall(nograph)
-    # the same variants one launch each (first 32 variants), and with one compilation per variant
-    # as the reference needs ($variables are baked into its generated code)
-    single_ms, single_trans = 0.0, 0
-    for net, params, n in variants[:32]:
-        b = mb.Batch(ctx)
-        b.set_options(use_graph=False, autotune=False)
-        k = b.add_model(models[net])
-        v = b.add_variant(k, n, params)
-        b.run(0)
-        single_ms += b.run(0)
-        single_trans += b.result(v).transitions
+    # to pinned memory; then every variant's result), wall clock
+    d2h = 0
     t0 = time.perf_counter()
-    comp_trans = 0
-    for net, params, n in variants[:4]:
+    reps = max(1, steps)
+    for i in range(reps):
+        batch.run(100 + i)
+        d2h = 0
+        for v in range(len(variants)):
+            r = batch.result(v)
+            d = r.dims
+            _ = r.window_probs, r.final_counts, r.fixed
+            d2h += d.windows * d.bins * 8 + d.windows * 8 + d.bins * 4 + len(r.fixed) * (4 * d.state_words + 4) + 64
+    e2e_s = (time.perf_counter() - t0) / reps
+
+    # one variant per base network, each through its own NVRTC-specialised module
+    sample = [next(k for k, v in enumerate(variants) if v[0] == net) for net in range(len(bases))]
+    sample = sample[:per_variant_sample]
+    comp_s, comp_trans, run_ms, run_trans = 0.0, 0, 0.0, 0
+    for k in sample:
+        net, params, n = variants[k]
         m = mb.Model(*bases[net])
-        for k2, val in params.items():
-            m.set_variable(k2, val)
-        comp_trans += ctx.compile(m).run(mode="fast", sample_count=n).transitions
-    comp_s = time.perf_counter() - t0
-    line = _timed_line(args, value, sum(ms) / args.steps,
-                       {"workload": f"c5: {EXTRA_WORKLOADS['c5']}", "mode": "fast (batched kernel)",
-                        "variants": len(variants), "trajectories": sum(v[2] for v in variants),
-                        "transitions_per_step": trans // args.steps,
-                        "l2": "not flushed (the per-variant statistics are a few MB; the inputs are tables)",
-                        "launch": {"block": info["block"], "blocks_per_sm": info["blocks_per_sm"],
-                                   "graph_nodes": info["graph_nodes"], "tuned": info["tuning"]}},
-                       {"per_variant_launch": {"value": single_trans / (single_ms / 1e3), "variants": 32,
-                                               "note": "the first 32 variants, one batched launch each"},
-                        "per_variant_compile_and_run": {"value": comp_trans / comp_s, "variants": 4,
-                                                        "note": "NVRTC compile + fused fast run per variant, wall time"},
-                        "e2e": {"value": (trans / args.steps) / e2e_s, "unit": "transitions/s",
-                                "wall_ms_per_run": 1e3 * e2e_s, "wall_ms_per_run_without_graph": 1e3 * e2e_nograph_s,
-                                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": None,
-                                "api": "Batch.run + Batch.result of every variant (graph replay)"},
-                        "gpu_launches": args.steps * (1 + len(variants)), "clocks": clk})
-    print(json.dumps(line), flush=True)
+        for name, val in params.items():
+            m.set_variable(name, val)
+        t = time.perf_counter()
+        mod = ctx.compile(m)
+        res = mod.run(mode="fast", sample_count=n)
+        comp_s += time.perf_counter() - t
+        comp_trans += res.transitions
+        runner = mod.runner(mode="fast", sample_count=n)
+        runner.launch()
+        runner.result()
+        runner.launch()
+        r2 = runner.result()
+        run_ms += r2.timing[0]
+        run_trans += r2.transitions
+    precompiled = run_trans / (run_ms / 1e3)
+    with_compile = comp_trans / comp_s
+    return {
+        "workload": f"c5: {EXTRA_WORKLOADS['c5']}", "value": value, "unit": "transitions/s",
+        "ms_per_step": sum(ms) / steps, "steps": steps, "variants": len(variants),
+        "trajectories": sum(v[2] for v in variants), "transitions_per_step": trans // steps,
+        "launch": {"block": info["block"], "blocks_per_sm": info["blocks_per_sm"],
+                   "graph_nodes": info["graph_nodes"], "tuned": info["tuning"]},
+        "per_variant_precompiled": {"value": precompiled, "variants": len(sample),
+                                    "note": "one variant of each base network, each with its own NVRTC-specialised "
+                                            "fast kernel compiled beforehand; device time of its launch"},
+        "per_variant_with_compile": {"value": with_compile, "variants": len(sample),
+                                     "compile_and_run_s": comp_s,
+                                     "note": "the same variants, NVRTC compilation + fast run per variant, wall "
+                                             "time (the reference's workflow: $variables are compiled in)"},
+        "ratio_vs_precompiled": value / precompiled, "ratio_vs_with_compile": value / with_compile,
+        "e2e": {"value": (trans / steps) / e2e_s, "unit": "transitions/s", "wall_ms_per_run": 1e3 * e2e_s,
+                "h2d_bytes_per_step": 8, "d2h_bytes_per_step": d2h,
+                "api": "Batch.run (graph replay with the new seed) + Batch.result of every variant "
+                       "(window probabilities, final counts, fixed points)"},
+        "gpu_launches": 1 + len(variants),
+    }
 
 
-def run_gradient(args) -> None:
-    """C4: cost of the score-function gradient against the forward simulation."""
+def run_batched(args) -> None:
     import maboss.gpu_b200 as mb
-    from maboss.gpu_b200 import synth
 
     mb.build()
     ctx = mb.Context(0)
+    clocks = ClockSampler(0)
+    clocks.start()
+    rec = batched_record(ctx, args.warmup, args.steps)
+    clk = clocks.stop()
+    line = _timed_line(args, rec["value"], rec["ms_per_step"],
+                       {"workload": rec["workload"], "mode": "fast (batched kernel)", "variants": rec["variants"],
+                        "trajectories": rec["trajectories"], "transitions_per_step": rec["transitions_per_step"],
+                        "l2": "not flushed (the per-variant statistics are a few MB; the inputs are tables)",
+                        "launch": rec["launch"]},
+                       {k: rec[k] for k in ("per_variant_precompiled", "per_variant_with_compile",
+                                            "ratio_vs_precompiled", "ratio_vs_with_compile", "e2e")}
+                       | {"gpu_launches": args.steps * rec["gpu_launches"], "clocks": clk})
+    print(json.dumps(line), flush=True)
+
+
+def gradient_record(ctx, warmup: int, steps: int, n: int = 1_000_000) -> dict:
+    """C4: the score-function gradient (VJP) of the 50-node network's window probabilities with
+    respect to its 40 rate parameters, 1e6 trajectories, against the forward simulation: the
+    NVRTC-specialised fast kernel of the same model (the plain forward pass) and the batched kernel
+    that the gradient kernel extends (same runtime tables, without the score)."""
+    import maboss.gpu_b200 as mb
+    from maboss.gpu_b200 import synth
+
     model = mb.Model(*synth.c4())
     names = sorted(model.variables)
     theta = {k: model.variable(k) for k in names}
-    n = args.samples or 1_000_000
     b = mb.Batch(ctx)
     v = b.add_variant(b.add_model(model), n, theta)
-    dims = None
-    for _ in range(args.warmup):
+    for _ in range(max(1, warmup)):
         b.run(0)
     dims = b.result(v).dims
     cot = np.zeros((dims.windows, dims.bins))
     cot[:, [s for s in range(dims.bins) if s & 1]] = 1.0
-    for _ in range(args.warmup):
-        mb.gradient(ctx, model, theta, cot, n, 0)
-    fwd_ms, grad_ms, call_ms, trans = [], [], [], 0
+    # a gradient batch kept across calls (the way repeated gradients are taken: device buffers, launch
+    # shape and graphs reused)
+    kept = mb.Batch(ctx)
+    kv = kept.add_variant(kept.add_model(model), n, theta, grad_params=names)
+    mod = ctx.compile(model)
+    runner = mod.runner(mode="fast", sample_count=n)
+    for _ in range(max(1, warmup)):
+        runner.launch()
+        runner.result()
+        kept.run_gradient(0, {kv: cot})
+    fwd_ms, nvrtc_ms, grad_ms, call_ms, trans = [], [], [], [], 0
+    for step in range(steps):
+        fwd_ms.append(b.run(step))
+        runner.launch()
+        nvrtc_ms.append(runner.result().timing[0])
+        t = time.perf_counter()
+        grad_ms.append(kept.run_gradient(step, {kv: cot}))
+        kept.gradient(kv)
+        trans += kept.result(kv).transitions
+        call_ms.append(1e3 * (time.perf_counter() - t))
+    g_ms, f_ms, nv_ms = float(np.mean(grad_ms)), float(np.mean(fwd_ms)), float(np.mean(nvrtc_ms))
+    return {"workload": f"c4grad: {EXTRA_WORKLOADS['c4grad']}", "parameters": len(names), "trajectories": n,
+            "value": trans / (sum(grad_ms) / 1e3), "unit": "transitions/s",
+            "gradient_ms": g_ms, "forward_nvrtc_fast_ms": nv_ms, "forward_batched_ms": f_ms,
+            "gradient_over_nvrtc_forward": g_ms / nv_ms, "gradient_over_batched_forward": g_ms / f_ms,
+            "gradient_call_ms": float(np.mean(call_ms)), "steps": steps,
+            "note": "device times (CUDA events) of the launches; gradient_call_ms is the host-to-host time of "
+                    "run_gradient + gradient on a batch kept across calls"}
+
+
+def run_gradient(args) -> None:
+    import maboss.gpu_b200 as mb
+
+    mb.build()
+    ctx = mb.Context(0)
     clocks = ClockSampler(0)
     clocks.start()
-    for step in range(args.steps):
-        fwd_ms.append(b.run(step))
-        t = time.perf_counter()
-        g, res = mb.gradient(ctx, model, theta, cot, n, step)
-        call_ms.append(1e3 * (time.perf_counter() - t))
-        grad_ms.append(res.timing[0])
-        trans += res.transitions
+    rec = gradient_record(ctx, args.warmup, args.steps, args.samples or 1_000_000)
     clk = clocks.stop()
-    line = _timed_line(args, trans / (sum(grad_ms) / 1e3), sum(grad_ms) / args.steps,
-                       {"workload": f"c4grad: {EXTRA_WORKLOADS['c4grad']}", "parameters": len(names),
-                        "trajectories": n},
-                       {"forward_ms": float(np.mean(fwd_ms)), "gradient_ms": float(np.mean(grad_ms)),
-                        "gradient_call_ms": float(np.mean(call_ms)),  # wall time of mb_gradient, host to host
-                        "gradient_over_forward": float(np.mean(grad_ms) / np.mean(fwd_ms)),
-                        "gpu_launches": args.steps, "clocks": clk})
+    line = _timed_line(args, rec["value"], rec["gradient_ms"],
+                       {"workload": rec["workload"], "parameters": rec["parameters"], "trajectories": rec["trajectories"]},
+                       {k: rec[k] for k in ("forward_nvrtc_fast_ms", "forward_batched_ms", "gradient_ms",
+                                            "gradient_over_nvrtc_forward", "gradient_over_batched_forward",
+                                            "gradient_call_ms")}
+                       | {"gpu_launches": args.steps, "clocks": clk})
     print(json.dumps(line), flush=True)
 
 
@@ -421,8 +531,25 @@ def run_ours(args) -> None:
     if os.path.exists(prof):
         with open(prof) as f:
             traffic = json.load(f).get(f"{args.workload}:{args.mode}")
+    issue = None
+    if os.path.exists(prof):
+        with open(prof) as f:
+            issue = json.load(f).get("issue", {}).get(f"{args.workload}:{args.mode}")
+    # CPU baselines on all host cores, each on a sample sized to about 10 s: the measured mode's own
+    # algorithm (fast: the incremental integer-rate process, oracle mode 2; exact: the reference's
+    # dense per-step algorithm, mode 0) feeds cpu_baseline; the other is reported beside it
     cores = os.cpu_count() or 1
-    cpu = cpu_baseline(bnd, cfg, args.cpu_sample, 0, cores) if not args.no_cpu else None
+    cpu = cpu_other = None
+    same_mode = 2 if args.mode == "fast" else 0
+    other_mode = 0 if same_mode == 2 else 2
+    if not args.no_cpu:
+        cpu = cpu_baseline_sized(bnd, cfg, same_mode, cores, args.cpu_seconds, n)
+        cpu_other = cpu_baseline_sized(bnd, cfg, other_mode, cores, args.cpu_seconds / 2, n)
+    # the batched sweep and the gradient, measured after the timed region (their own device timing)
+    extras = {}
+    if not args.no_extras and world == 1:
+        extras["batched"] = batched_record(ctx, 3, 5)
+        extras["gradient"] = gradient_record(ctx, 3, 5)
     line = {
         "metric": "Gillespie transitions/s",
         "value": value,
@@ -454,10 +581,17 @@ def run_ours(args) -> None:
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peak else "absent"},
         "cpu_baseline": None if cpu is None else {
             "value": cpu["value"], "unit": "transitions/s", "cores": cores, "kind": "port",
-            "sample": f"{args.cpu_sample} trajectories of the same workload, exact mode, {cores} OpenMP threads "
-                      f"({cpu['seconds']:.1f} s)"},
+            "sample": f"{cpu['trajectories']} trajectories of the same workload, {ORACLE_MODES[same_mode]}, "
+                      f"{cores} OpenMP threads ({cpu['seconds']:.1f} s; the CPU oracle)"},
+        "cpu_baseline_other_algorithm": None if cpu_other is None else {
+            "value": cpu_other["value"], "unit": "transitions/s", "cores": cores, "kind": "port",
+            "sample": f"{cpu_other['trajectories']} trajectories, {ORACLE_MODES[other_mode]} "
+                      f"({cpu_other['seconds']:.1f} s)"},
         "clocks": clk,
     }
+    if issue:
+        line["roofline"]["issue"] = issue
+    line.update(extras)
     print(json.dumps(line), flush=True)
 
 
@@ -473,8 +607,12 @@ def main() -> None:
     p.add_argument("--block", type=int, default=0,
                    help="threads per block (0: chosen by the engine's autotuner, fused modes; 256 otherwise)")
     p.add_argument("--blocks-per-sm", type=int, default=0, help="resident blocks per SM (0: occupancy calculator)")
-    p.add_argument("--cpu-sample", type=int, default=2000, help="trajectories of the CPU baseline sample")
-    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample size, in seconds of work")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baselines")
+    p.add_argument("--no-extras", action="store_true", help="skip the batched and gradient records")
+    p.add_argument("--ref-samples", type=int, default=0,
+                   help="trajectories of the reference arm's runs (0: the workload's, capped below the "
+                        "reference's int overflow)")
     args = p.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -13,7 +13,8 @@ every consumer (the engine, the oracle, the reference) reads the same float valu
       1e6 trajectories
   c4  50 nodes, 3 inputs, 20 nodes with named $u_i/$d_i rate parameters (40 parameters,
       lognormal(0, 0.5)), 8 output nodes non-internal, 1e6 trajectories
-  c5  base networks of 20-500 nodes with 2-4 inputs (batched sweeps)
+  c5  base networks of 20-500 nodes with 2-4 inputs (batched sweeps; network 0 has 20 nodes, network 7
+      has 500)
 """
 from __future__ import annotations
 
@@ -144,10 +145,13 @@ def c4(seed: int = 0, sample_count: int = 1_000_000, sim_seed: int = 0) -> tuple
 
 
 def c5_base(index: int, sample_count: int = 10_000, sim_seed: int = 0) -> tuple[str, str]:
-    """Base network `index` (0..7) of the batched sweep: 20-500 nodes, 2-4 inputs, 8 outputs, node
-    rates given by variables $u_i / $d_i (lognormal(0, 0.5)) so that variants can rescale them."""
+    """Base network `index` (0..7) of the batched sweep: 20-500 nodes (network 0 has 20 and network 7
+    has 500, so the sweep spans the whole range; the others are log-uniform in it), 2-4 inputs,
+    8 outputs, node rates given by variables $u_i / $d_i (lognormal(0, 0.5)) so that variants can
+    rescale them."""
     rng = np.random.default_rng(1000 + index)
     n = int(np.round(np.exp(rng.uniform(np.log(20), np.log(500)))))
+    n = {0: 20, 7: 500}.get(index, n)
     kin = int(rng.integers(2, 5))
     names = [f"B{index}_{i}" for i in range(n)]
     variables = {}
