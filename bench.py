@@ -497,7 +497,9 @@ def run_ours(args) -> None:
         res = api_run()
         # with several ranks res is the job's merged result: its total counted once over the ranks
         e2e_trans += res.transitions / world if world > 1 else res.transitions
-        probs = res.sparse()["probs"] if res.is_sparse else res.window_probs  # host copy of the result
+        # host copy of the result: the entries when the windows are sparse (more than 20 non-internal
+        # nodes, or a large histogram's non-zero cells), else the dense window probabilities
+        probs = res.sparse()["probs"] if res.windows_sparse else res.window_probs
     barrier()
     e2e_s = time.perf_counter() - t
     e2e_time = torch.tensor([e2e_s], dtype=torch.float64, device=local)
@@ -510,6 +512,9 @@ def run_ours(args) -> None:
     if res.is_sparse:  # compacted bins: 16-byte key + 8-byte value each
         sp = res.sparse()
         d2h = (len(sp["raw"]) + len(sp["final_counts"])) * 24 + d.windows * 8 + len(res.fixed) * (4 * d.state_words + 4) + 64
+    elif res.windows_sparse:  # a large histogram's non-zero cells: 8-byte cell index + 8-byte value each
+        sp = res.sparse()
+        d2h = len(sp["raw"]) * 16 + d.windows * 8 + d.bins * 4 + len(res.fixed) * (4 * d.state_words + 4) + 64
     else:
         d2h = d.windows * d.bins * 8 + d.windows * 8 + d.bins * 4 + len(res.fixed) * (4 * d.state_words + 4) + 64
 

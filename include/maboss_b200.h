@@ -208,9 +208,13 @@ mb_status mb_launch_partition(mb_module mod, void* stream, int n, int stride, co
  *                     order; *out_n (host) is the number of distinct fixed points
  * Limits: state_words <= 64 (2048 nodes); at most P/2 distinct fixed points, P the largest power of
  * two with P * (20 + 4 * state_words) + 256 <= 8 MiB (131072 for 1 word, 16384 for 32 words); larger
- * inputs return MB_ERR_LIMIT with a message. Runs on `stream` and synchronises it.
- * The first call on a device looks up the array's device address with that device current; make that
- * first call before any stream capture. Every call reuses the same array and clears it first, so
+ * inputs return MB_ERR_LIMIT with a message and *out_n = -1 (the count is unknown). When only
+ * out_cap is too small, the call returns MB_ERR_LIMIT with *out_n = the number of distinct fixed
+ * points and the first out_cap of them written. Runs on `stream` and synchronises it.
+ * The device is the calling thread's current device (cudaGetDevice), not the stream's: make every
+ * call with the stream's device current. The first call on a device, and the first call after that
+ * device's context changed (cudaDeviceReset), looks up the array's device address in the current
+ * context; make that call before any stream capture. Every call reuses the same array and clears it first, so
  * calls that overlap on the GPU (other streams, other host threads) race: serialise them. Every GPU
  * that loads the library holds the 8 MiB until the process exits. */
 mb_status mb_fixed_states_noalloc(void* stream, int n, int stride, int state_words, const uint32_t* last_states,
@@ -360,6 +364,13 @@ mb_status mb_result_window_entropy(mb_result r, double* th);
 mb_status mb_result_window_raw(mb_result r, long long* occupancy, unsigned* counts, long long* entropy,
                                int* occupancy_exponent, int* entropy_exponent);
 mb_status mb_result_final_counts(mb_result r, unsigned* counts);
+/* 1 when the result's windows are stored as sparse entries: more than 20 non-internal nodes, or a
+ * dense histogram of at least 2^24 cells (windows x 2^k) of which at most a quarter are non-zero (only
+ * those cells are copied from the device; final states stay dense). The sparse getters then give the
+ * entries; the dense getters still work for the latter (they write zeros and scatter the entries).
+ * No counterpart in the reference (its window_average_small_stats::finalize copies the whole
+ * histogram, window_average_small.cpp:91-108). */
+mb_status mb_result_windows_sparse(mb_result r, int* sparse);
 /* Sparse results: entry counts and the number of bin additions lost to a full table (0 means exact). */
 mb_status mb_result_sparse_size(mb_result r, long long* window_entries, long long* final_entries,
                                 unsigned* bin_overflow);

@@ -1020,6 +1020,16 @@ mb_status mb_result_window_probs(mb_result r, double* probs)
 		const mb::result& x = *r->res;
 		need(x.sections & MB_STATS_WINDOWS, "the result has no window statistics");
 		need(!x.wide, "sparse result (more than 20 non-internal nodes): use mb_result_sparse_windows");
+		if (x.compact)
+		{
+			// zeros, then the stored (non-zero) cells
+			std::memset(probs, 0, (size_t)x.n_windows * x.n_bins * sizeof(double));
+			mb::parallel_ranges(x.sp_w.size(), (int)std::thread::hardware_concurrency(), [&](size_t a, size_t e) {
+				for (size_t i = a; i < e; i++)
+					probs[(size_t)x.sp_w[i] * x.n_bins + (size_t)x.sp_idx[i]] = x.n_traj > 0 ? x.sparse_prob(i) : 0.0;
+			});
+			return;
+		}
 		for (int w = 0; w < x.n_windows; w++)
 			for (unsigned b = 0; b < x.n_bins; b++)
 				probs[(size_t)w * x.n_bins + b] = x.n_traj > 0 ? x.window_prob(w, b) : 0.0;
@@ -1043,6 +1053,23 @@ mb_status mb_result_window_raw(mb_result r, long long* occupancy, unsigned* coun
 	return guard([&] {
 		need(r, "null result");
 		const mb::result& x = *r->res;
+		if (x.compact)
+		{
+			// the dense arrays from the stored (non-zero) cells
+			const size_t cells = (size_t)x.n_windows * x.n_bins;
+			if (occupancy && !x.discrete_time)
+			{
+				std::memset(occupancy, 0, cells * sizeof(long long));
+				for (size_t i = 0; i < x.sp_w.size(); i++)
+					occupancy[(size_t)x.sp_w[i] * x.n_bins + (size_t)x.sp_idx[i]] = x.sp_val[i];
+			}
+			if (counts && x.discrete_time)
+			{
+				std::memset(counts, 0, cells * sizeof(unsigned));
+				for (size_t i = 0; i < x.sp_w.size(); i++)
+					counts[(size_t)x.sp_w[i] * x.n_bins + (size_t)x.sp_idx[i]] = (unsigned)x.sp_val[i];
+			}
+		}
 		if (occupancy && !x.win_occ.empty())
 			std::memcpy(occupancy, x.win_occ.data(), x.win_occ.size() * sizeof(long long));
 		if (counts && !x.win_cnt.empty())
@@ -1063,6 +1090,14 @@ mb_status mb_result_final_counts(mb_result r, unsigned* counts)
 		need(r->res->sections & MB_STATS_FINAL, "the result has no final-state statistics");
 		need(!r->res->wide, "sparse result (more than 20 non-internal nodes): use mb_result_sparse_final");
 		std::memcpy(counts, r->res->final_cnt.data(), r->res->final_cnt.size() * sizeof(unsigned));
+	});
+}
+
+mb_status mb_result_windows_sparse(mb_result r, int* sparse)
+{
+	return guard([&] {
+		need(r && sparse, "null argument");
+		*sparse = r->res->sparse_windows() ? 1 : 0;
 	});
 }
 

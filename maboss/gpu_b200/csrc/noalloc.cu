@@ -159,11 +159,32 @@ __global__ void extract_fixed(unsigned char* base, unsigned cap, int words, uint
 }
 
 
-// device address of the scratch array, looked up once per device (with that device current)
+// Driver-API functions resolved through the runtime (this library does not link libcuda).
+typedef int (*ctx_get_current_fn)(void** ctx);
+typedef int (*ctx_get_id_fn)(void* ctx, unsigned long long* id);
+
+template <typename F>
+F driver_function(const char* name)
+{
+	void* p = nullptr;
+	cudaDriverEntryPointQueryResult q;
+	if (cudaGetDriverEntryPointByVersion(name, &p, 12000, cudaEnableDefault, &q) != cudaSuccess
+		|| q != cudaDriverEntryPointSuccess)
+		return nullptr;
+	return reinterpret_cast<F>(p);
+}
+
+// Device address of the scratch array in the current context. It is looked up with
+// cudaGetSymbolAddress the first time a device is used and again whenever that device's current
+// context has changed (cuCtxGetId gives every context of the process its own id, so a context
+// created after cudaDeviceReset or a primary-context reset is never served the old address).
 void* scratch_address(int device, cudaError_t& err)
 {
 	static std::mutex mu;
 	static void* addr[256] = { nullptr };
+	static unsigned long long ctx_id[256] = { 0 };
+	static ctx_get_current_fn get_current = driver_function<ctx_get_current_fn>("cuCtxGetCurrent");
+	static ctx_get_id_fn get_id = driver_function<ctx_get_id_fn>("cuCtxGetId");
 	std::lock_guard<std::mutex> lk(mu);
 	err = cudaSuccess;
 	if (device < 0 || device >= 256)
@@ -171,13 +192,20 @@ void* scratch_address(int device, cudaError_t& err)
 		err = cudaErrorInvalidDevice;
 		return nullptr;
 	}
-	if (!addr[device])
+	// before the runtime has bound a context to this thread there is no current context: id 0,
+	// and cudaGetSymbolAddress (which binds the device's primary context) runs again next time
+	unsigned long long id = 0;
+	void* ctx = nullptr;
+	if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0)
+		id = 0; // no id available: look the address up on every call
+	if (!addr[device] || id == 0 || id != ctx_id[device])
 	{
 		void* p = nullptr;
 		err = cudaGetSymbolAddress(&p, mb_noalloc_scratch);
 		if (err != cudaSuccess)
 			return nullptr;
 		addr[device] = p;
+		ctx_id[device] = id;
 	}
 	return addr[device];
 }
@@ -234,10 +262,13 @@ mb_status mb_fixed_states_noalloc(void* stream, int n, int stride, int state_wor
 	cudaStream_t s = static_cast<cudaStream_t>(stream);
 
 	// the array keeps the previous call's table: clear it first
-	clear_table<<<(cap + 255) / 256, 256, 0, s>>>(base, cap, state_words);
+	// grid sizes in size_t: n may be close to INT_MAX
+	const unsigned table_blocks = (unsigned)(((size_t)cap + 255) / 256);
+	clear_table<<<table_blocks, 256, 0, s>>>(base, cap, state_words);
 	if (n > 0)
-		insert_fixed<<<(n + 255) / 256, 256, 0, s>>>(base, cap, state_words, n, stride, last_states, statuses);
-	extract_fixed<<<(cap + 255) / 256, 256, 0, s>>>(base, cap, state_words, out_states, out_counts, out_cap);
+		insert_fixed<<<(unsigned)(((size_t)n + 255) / 256), 256, 0, s>>>(base, cap, state_words, n, stride,
+																		 last_states, statuses);
+	extract_fixed<<<table_blocks, 256, 0, s>>>(base, cap, state_words, out_states, out_counts, out_cap);
 	e = cudaGetLastError();
 	if (e != cudaSuccess)
 		return fail(MB_ERR_CUDA, std::string("mb_fixed_states_noalloc: launch: ") + cudaGetErrorString(e));
@@ -250,10 +281,14 @@ mb_status mb_fixed_states_noalloc(void* stream, int n, int stride, int state_wor
 		e = cudaStreamSynchronize(s);
 	if (e != cudaSuccess)
 		return fail(MB_ERR_CUDA, std::string("mb_fixed_states_noalloc: ") + cudaGetErrorString(e));
-	*out_n = (int)counters[1];
 	if (counters[0] != 0 || counters[1] > cap / 2)
+	{
+		// the table overflowed: the number of distinct fixed points is unknown
+		*out_n = -1;
 		return fail(MB_ERR_LIMIT, "mb_fixed_states_noalloc: more distinct fixed points than the static table holds (" +
 									  std::to_string(cap / 2) + " for " + std::to_string(state_words) + " state words)");
+	}
+	*out_n = (int)counters[1];
 	if ((int)counters[1] > out_cap)
 		return fail(MB_ERR_LIMIT, "mb_fixed_states_noalloc: " + std::to_string(counters[1]) +
 									  " distinct fixed points do not fit in out_cap = " + std::to_string(out_cap));

@@ -37,11 +37,12 @@ std::vector<unsigned> noninternal_index_to_state(const std::vector<int>& noninte
 namespace {
 
 // The non-zero probabilities of window w (as the reference prints them: floats), in increasing order
-// of the non-internal index, from the dense histogram or the sparse bins.
+// of the non-internal index, from the dense histogram or the sparse entries (more than 20
+// non-internal nodes, or a large histogram's non-zero cells).
 std::vector<std::pair<unsigned __int128, float>> window_entries(const result& r, int w)
 {
 	std::vector<std::pair<unsigned __int128, float>> out;
-	if (r.wide)
+	if (r.sparse_windows())
 	{
 		for (size_t i = r.sp_begin[w]; i < r.sp_begin[w + 1]; i++)
 		{

@@ -363,6 +363,13 @@ int entropy_exponent(long long n_traj, float tick, bool discrete)
 
 double result::window_prob(int w, unsigned bin) const
 {
+	if (compact)
+	{
+		// the window's entries are sorted by state
+		const auto a = sp_idx.begin() + (std::ptrdiff_t)sp_begin[w], e = sp_idx.begin() + (std::ptrdiff_t)sp_begin[w + 1];
+		const auto it = std::lower_bound(a, e, (unsigned __int128)bin);
+		return (it != e && *it == (unsigned __int128)bin) ? sparse_prob((size_t)(it - sp_idx.begin())) : 0.0;
+	}
 	const size_t i = (size_t)w * n_bins + bin;
 	if (discrete_time)
 		return (double)win_cnt[i] / (double)n_traj;
@@ -616,12 +623,46 @@ std::unique_ptr<result> stats_state::finalize(long long n, cudaStream_t s)
 		r.win_h.resize(n_windows);
 		MB_CUDA(cudaMemcpyAsync(r.win_h.data(), h.p, n_windows * sizeof(long long), cudaMemcpyDeviceToHost, s));
 	}
-	else if ((sections & 1u) && discrete_time)
+	// a large dense histogram: only its non-zero cells (selected on the device in cell order), when
+	// they are at most a quarter of it
+	if ((sections & 1u) && !wide && cells >= compact_min_cells)
+	{
+		const long long nz = compact_cells(discrete_time ? nullptr : occ.as<long long>(),
+										   discrete_time ? cnt.as<unsigned>() : nullptr, cells, cells / 4, cell_idx,
+										   cell_vals, m.ctx->sm_count, s);
+		if (nz >= 0)
+		{
+			std::vector<unsigned long long> idx((size_t)nz);
+			r.sp_val.resize((size_t)nz);
+			if (nz)
+			{
+				MB_CUDA(cudaMemcpyAsync(idx.data(), cell_idx.p, (size_t)nz * sizeof(unsigned long long),
+										cudaMemcpyDeviceToHost, s));
+				MB_CUDA(cudaMemcpyAsync(r.sp_val.data(), cell_vals.p, (size_t)nz * sizeof(long long),
+										cudaMemcpyDeviceToHost, s));
+				MB_CUDA(cudaStreamSynchronize(s));
+			}
+			r.sp_w.resize((size_t)nz);
+			r.sp_idx.resize((size_t)nz);
+			parallel_ranges((size_t)nz, (int)std::thread::hardware_concurrency(), [&](size_t a, size_t e) {
+				for (size_t i = a; i < e; i++)
+				{
+					r.sp_w[i] = (int)(idx[i] / n_bins);
+					r.sp_idx[i] = (unsigned __int128)(idx[i] % n_bins);
+				}
+			});
+			r.sp_begin.assign((size_t)n_windows + 1, 0);
+			for (int w = 0; w <= n_windows; w++)
+				r.sp_begin[w] = (size_t)(std::lower_bound(r.sp_w.begin(), r.sp_w.end(), w) - r.sp_w.begin());
+			r.compact = true;
+		}
+	}
+	if ((sections & 1u) && !wide && !r.compact && discrete_time)
 	{
 		r.win_cnt.resize(cells);
 		MB_CUDA(cudaMemcpyAsync(r.win_cnt.data(), cnt.p, cells * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
 	}
-	else if (sections & 1u)
+	else if ((sections & 1u) && !wide && !r.compact)
 	{
 		r.win_occ.resize(cells);
 		MB_CUDA(cudaMemcpyAsync(r.win_occ.data(), occ.p, cells * sizeof(long long), cudaMemcpyDeviceToHost, s));
@@ -725,6 +766,7 @@ std::unique_ptr<result> merge_results(const std::vector<const result*>& parts)
 	r.win_h.assign(a.win_h.size(), 0);
 	r.final_cnt.assign(a.final_cnt.size(), 0);
 	r.wide = a.wide;
+	r.compact = a.compact;
 	r.bin_overflow = 0;
 	std::map<std::vector<unsigned>, unsigned long long> fixed;
 	std::map<std::pair<int, unsigned __int128>, long long> bins;
@@ -732,7 +774,7 @@ std::unique_ptr<result> merge_results(const std::vector<const result*>& parts)
 	for (const result* p : parts)
 	{
 		const result& b = *p;
-		if (b.wide != a.wide)
+		if (b.wide != a.wide || b.compact != a.compact)
 			throw engine_error(MB_ERR_INVALID, "merge: the results are not shards of the same run");
 		for (size_t i = 0; i < b.sp_w.size(); i++)
 			bins[{ b.sp_w[i], b.sp_idx[i] }] += b.sp_val[i];
@@ -772,7 +814,7 @@ std::unique_ptr<result> merge_results(const std::vector<const result*>& parts)
 		cn.push_back((unsigned)count);
 	}
 	set_fixed_sorted(r, st, cn);
-	if (r.wide)
+	if (r.wide || r.compact)
 	{
 		for (auto& [key, v] : bins)
 		{

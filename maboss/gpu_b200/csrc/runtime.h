@@ -119,6 +119,13 @@ void simulate_epoch(module& m, bool dense, cudaStream_t s, int n, int stride, in
 
 // Sorts n sparse-bin records by their 128-bit keys (window, then non-internal index) on the device
 // (sort.cu); synchronises the stream.
+// The non-zero cells of a dense window histogram (`occ` int64 or `cnt` u32, whichever is not null), in
+// increasing cell order (window, then state): their cell indices into idx_out (u64) and values into
+// val_out (int64), both grown as needed. Returns the number of cells, or -1 without writing them
+// when there are more than max_entries (the dense copy is then cheaper).
+long long compact_cells(const long long* occ, const unsigned* cnt, unsigned long long cells,
+						unsigned long long max_entries, dbuf& idx_out, dbuf& val_out, int sm_count, cudaStream_t s);
+
 void sort_bins(const mb_key128* keys, const long long* vals, unsigned n, mb_key128* out_keys, long long* out_vals,
 			   cudaStream_t s);
 
@@ -152,6 +159,10 @@ struct run_config
 
 run_config config_from_layout(const model_layout& L, int mode);
 
+// Dense window histograms of at least this many cells (T x 2^k; 134 MB of int64 sums) are returned as
+// their non-zero cells only, when those are at most a quarter of the cells.
+constexpr unsigned long long compact_min_cells = 1ull << 24;
+
 struct result
 {
 	int state_size = 0, state_words = 0, n_windows = 0;
@@ -173,6 +184,9 @@ struct result
 	// more than 20 non-internal nodes: sparse window bins (sorted by window, then index; sp_begin[w]
 	// is the first entry of window w) and sparse final states (sorted by index); n_bins is 0
 	bool wide = false;
+	// at most 20 non-internal nodes but a large histogram (compact_min_cells or more cells): only its
+	// non-zero cells, in the same sparse form (sp_*), selected on the device; final states dense
+	bool compact = false;
 	std::vector<int> sp_w;
 	std::vector<unsigned __int128> sp_idx;
 	std::vector<long long> sp_val; // occupancy in fixed point (continuous) or count (discrete)
@@ -187,6 +201,7 @@ struct result
 	int epochs = 0;
 
 	double window_prob(int w, unsigned bin) const; // window_average_small.cpp:126-140 (fp64)
+	bool sparse_windows() const { return wide || compact; }
 	double window_th(int w) const;				   // TH column (window_average_small.cpp:222-223)
 };
 
@@ -210,6 +225,7 @@ struct stats_state
 	dbuf occ, cnt, h, fin, fp_keys, fp_counts, fp_states, counters, istate;
 	dbuf out_counts, out_states; // compacted fixed points (finalize)
 	dbuf bin_keys, bin_vals, out_bin_keys, out_bin_vals; // sparse bins (more than 20 non-internal nodes)
+	dbuf cell_idx, cell_vals; // non-zero cells of a large dense histogram (compact results), kept across runs
 	unsigned bin_cap = 0;
 	// host copies of the sorted bins, kept across runs (no re-allocation, no first-touch page faults)
 	std::unique_ptr<uint64_t[]> hbin_keys;

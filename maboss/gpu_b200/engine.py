@@ -567,6 +567,15 @@ class Result:
         """More than 20 non-internal nodes: windows and final states as sparse entries."""
         return self.dims.bins == 0 and self.dims.noninternal > 20
 
+    @property
+    def windows_sparse(self) -> bool:
+        """mb_result_windows_sparse: the windows are stored as sparse entries (more than 20 non-internal
+        nodes, or a large dense histogram of which only the non-zero cells were copied back);
+        sparse() gives them, window_probs / raw() still give the dense arrays."""
+        v = C.c_int()
+        check(lib().mb_result_windows_sparse(self._h, C.byref(v)))
+        return bool(v.value)
+
     def sparse(self) -> dict:
         """mb_result_sparse_*: window entries (window, state, raw sum, probability) sorted by window then
         state, final states and counts, and the number of bin additions lost to a full table. States are

@@ -275,3 +275,33 @@ def test_autotuner_picks_a_timed_shape_and_results_do_not_depend_on_it(gpu):
     a = mod.run(mode="exact", sample_count=3_000, block=t["block"], blocks_per_sm=t["blocks_per_sm"])
     b = mod.run(mode="exact", sample_count=3_000, block=64, blocks_per_sm=1)
     _assert_identical(a, b)
+
+
+def test_large_histograms_come_back_as_their_non_zero_cells(gpu):
+    """A dense histogram of >= 2^24 cells (the 100-node network with 20 outputs: 100 windows x 2^20
+    states) is returned as its non-zero cells, selected in cell order on the device. The dense
+    getters rebuild exactly the oracle's integers, the sparse getters give the same cells, the CSV
+    writer and shard merges read them, and a small histogram stays dense."""
+    bnd, cfg = synth.c2(noninternal=20)
+    model, res, raw, o, ref = _run_both(gpu, bnd, cfg, 1_500)
+    assert res.windows_sparse and not res.is_sparse
+    _assert_same(res, raw, ref, o.discrete)
+    assert np.array_equal(raw["occ"], ref["occ"])
+    sp = res.sparse()
+    nz = np.nonzero(ref["occ"].ravel())[0]
+    assert len(sp["raw"]) == len(nz)
+    cells = sp["windows"].astype(np.int64) * res.dims.bins + sp["states"][:, 0].astype(np.int64)
+    assert np.array_equal(cells, nz) and np.array_equal(sp["raw"], ref["occ"].ravel()[nz])
+    # discrete time: counts
+    bnd_d, cfg_d = synth.c2(noninternal=20, discrete=True)
+    _, res_d, raw_d, o_d, ref_d = _run_both(gpu, bnd_d, cfg_d, 1_000)
+    assert res_d.windows_sparse and np.array_equal(raw_d["cnt"], ref_d["cnt"])
+    # shards of one job merge to the whole run
+    mod = gpu.compile(model)
+    a = mod.run(mode="exact", sample_count=600, stats_trajectories=1_500)
+    b = mod.run(mode="exact", sample_count=900, first_traj=600, stats_trajectories=1_500)
+    m = mb.merge_results([a, b])
+    assert m.windows_sparse and np.array_equal(m.raw()["occ"], raw["occ"])
+    # a small histogram stays dense
+    small = gpu.compile(mb.Model(*synth.c1())).run(mode="fast", sample_count=1_000)
+    assert not small.windows_sparse
