@@ -55,7 +55,9 @@ def parse_res(text: str) -> dict:
 
 
 def main() -> None:
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_fixtures.py <reference checkout> (the directory holding data/ and test/)")
+    ref = sys.argv[1]
     here = os.path.dirname(os.path.abspath(__file__))
     os.makedirs(os.path.join(here, "models"), exist_ok=True)
     for name in MODELS:
