@@ -12,7 +12,7 @@ Outputs (committed):
                     "probs": {state: prob}}]}
     State names use the older "-" separator of the dumps; tests compare them as sets of nodes.
 
-usage: python tests/golden/make_fixtures.py [/path/to/reference]
+usage: python tests/golden/make_fixtures.py /path/to/reference
 """
 import json
 import os

@@ -97,8 +97,9 @@ def test_noalloc_rejects_sizes_beyond_its_limits():
     n = 40_000
     last, stat = _inputs(torch, n, n, words, pool=n, seed=3)
     stat.fill_(2)
-    st, _, _, _ = _noalloc(torch, n, n, words, last, stat, 64)
+    st, got_n, _, _ = _noalloc(torch, n, n, words, last, stat, 64)
     assert st == 5 and b"static table" in mb.lib().mb_last_error()  # MB_ERR_LIMIT
+    assert got_n == -1  # the number of distinct fixed points is unknown after an overflow
     # state words beyond the maximum
     st, _, _, _ = _noalloc(torch, 10, 10, 65, last, stat, 64)
     assert st == 5 and b"state_words" in mb.lib().mb_last_error()
