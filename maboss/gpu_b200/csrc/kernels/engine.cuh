@@ -233,7 +233,7 @@ __device__ __forceinline__ void mb_fused_body(const mb_fused_params& P)
 }
 
 
-#if defined(MBG_INCREMENTAL) && defined(MBG_INTEGER_RATES)
+#ifdef MBG_INCREMENTAL
 // ---------------------------------------------------------------- incremental fast kernel
 // Fast mode for models whose rates all have the form `@logic ? U : 0` / `@logic ? 0 : D`.
 // A node is unstable when its bit differs from its logic; only unstable nodes have a rate
@@ -401,7 +401,7 @@ __device__ __forceinline__ void mb_incr_start(const mb_fused_params& P, const mb
 	__syncwarp();
 }
 
-#endif // MBG_INCREMENTAL && MBG_INTEGER_RATES
+#endif // MBG_INCREMENTAL
 
 #if defined(MBG_INCREMENTAL) && (defined(MB_FAMILY_EXACT) || (defined(MB_FAMILY_EPOCH) && !defined(MB_EPOCH_DENSE)))
 // ---- the exact algorithm on incremental unstable sets (models whose rates all have the @logic form)

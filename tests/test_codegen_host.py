@@ -25,7 +25,7 @@ import numpy as np
 import pytest
 
 import maboss.gpu_b200 as mb
-from conftest import model_text
+from conftest import ROOT, model_text
 from maboss.gpu_b200 import synth
 from oracle.oracle import OracleModel
 
@@ -313,3 +313,19 @@ def test_generated_code_of_a_wide_rate_span_model(tmp_path):
     assert _check_model(*wide_span_model(), tmp_path, "wide", n_states=100)
     L = _compile(mb.Model(*wide_span_model()).generate_code(), tmp_path, "wide2")
     assert L.host_integer_rates() == 0
+
+
+@pytest.mark.parametrize("family", ["EXACT", "FAST", "EPOCH"])
+def test_wide_rate_span_model_compiles_for_sm100a(family, tmp_path):
+    """The generated code of a model whose rates are too wide for the integer rates (fast mode: dense
+    kernel; exact and epoch modes: incremental kernels) compiles in every kernel family with nvcc
+    for sm_100a, as NVRTC compiles it at run time."""
+    csrc = os.path.join(ROOT, "maboss", "gpu_b200", "csrc", "kernels")
+    src = mb.Model(*wide_span_model()).generate_code() + f"\n#define MB_FAMILY_{family} 1\n"
+    for f in ("params.cuh", "common.cuh", "engine.cuh"):
+        src += open(os.path.join(csrc, f)).read() + "\n"
+    (tmp_path / "m.cu").write_text(src)
+    p = subprocess.run(["nvcc", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-O1", "-cubin",
+                        "-o", str(tmp_path / "m.cubin"), str(tmp_path / "m.cu")], capture_output=True, text=True,
+                       timeout=600)
+    assert p.returncode == 0, p.stderr[-3000:]

@@ -286,12 +286,15 @@ def test_large_histograms_come_back_as_their_non_zero_cells(gpu):
     model, res, raw, o, ref = _run_both(gpu, bnd, cfg, 1_500)
     assert res.windows_sparse and not res.is_sparse
     _assert_same(res, raw, ref, o.discrete)
-    assert np.array_equal(raw["occ"], ref["occ"])
-    sp = res.sparse()
+    # the same trajectories occupy the same cells; the occupancy sums agree to the slices' last ulp
+    # (device and host logf), so the cells are compared exactly and the sums with a tolerance
     nz = np.nonzero(ref["occ"].ravel())[0]
+    assert np.array_equal(np.nonzero(raw["occ"].ravel())[0], nz)
+    assert np.allclose(raw["occ"].ravel()[nz], ref["occ"].ravel()[nz], rtol=1e-5, atol=0)
+    sp = res.sparse()
     assert len(sp["raw"]) == len(nz)
     cells = sp["windows"].astype(np.int64) * res.dims.bins + sp["states"][:, 0].astype(np.int64)
-    assert np.array_equal(cells, nz) and np.array_equal(sp["raw"], ref["occ"].ravel()[nz])
+    assert np.array_equal(cells, nz) and np.array_equal(sp["raw"], raw["occ"].ravel()[nz])
     # discrete time: counts
     bnd_d, cfg_d = synth.c2(noninternal=20, discrete=True)
     _, res_d, raw_d, o_d, ref_d = _run_both(gpu, bnd_d, cfg_d, 1_000)

@@ -77,14 +77,22 @@ def test_exact_mode_equals_reference_build_with_other_seeds(gpu):
 def test_csv_files_equal_reference_build(gpu, tmp_path):
     """The command-line front-end's out_probtraj.csv / out_fp.csv against the reference's writers
     (window_average_small.cpp:181-250, fixed_states.cu:154-187) on a discrete-time model: equal
-    counts print equal text, byte for byte."""
+    counts print equal text. The fixed-point file is equal byte for byte; in the trajectory file
+    every column but TH is (times, entropies, states and probabilities come from the same integer
+    counts), and TH, which the reference sums with fp32 atomics in a run-dependent order, agrees
+    within 2e-4 relative."""
     bnd, cfg = model_files("cellcycle")
     (tmp_path / "m.cfg").write_text(open(cfg).read() + "\nsample_count = 30000;\n")
     reference.run(bnd, str(tmp_path / "m.cfg"), dump=False, csv_prefix=str(tmp_path / "ref"))
     cli = os.path.join(ROOT, "maboss", "gpu_b200", "MaBoSS.GPU")
     subprocess.run([cli, "--mode", "exact", "-o", str(tmp_path / "ours"), bnd, str(tmp_path / "m.cfg")],
                    check=True, capture_output=True)
-    for suffix in ("_probtraj.csv", "_fp.csv"):
-        a = (tmp_path / f"ref{suffix}").read_bytes()
-        b = (tmp_path / f"ours{suffix}").read_bytes()
-        assert a == b, suffix
+    assert (tmp_path / "ref_fp.csv").read_bytes() == (tmp_path / "ours_fp.csv").read_bytes()
+    a = (tmp_path / "ref_probtraj.csv").read_text().splitlines()
+    b = (tmp_path / "ours_probtraj.csv").read_text().splitlines()
+    assert len(a) == len(b) and a[0] == b[0]
+    for la, lb in zip(a[1:], b[1:]):
+        fa, fb = la.split("\t"), lb.split("\t")
+        assert len(fa) == len(fb)
+        assert fa[0] == fb[0] and fa[2:] == fb[2:], (la, lb)
+        assert abs(float(fa[1]) - float(fb[1])) <= 2e-4 * abs(float(fa[1])) + 1e-6, (fa[1], fb[1])
