@@ -81,6 +81,12 @@ mb_status mb_model_set_istate(mb_model m, int i, float istate);
 
 /* driver::constants and driver::variables (src/parser/driver.h:41-42). Missing constants read
  * as 0 like std::map::operator[] in src/main.cpp:128-132; missing variables are an error. */
+/* Opt-in front-end change, no counterpart in the reference: every node attribute defined more than
+ * once (in the .bnd and again in the .cfg) takes its last definition. The reference keeps the first
+ * (src/parser/driver.cpp:65-77 appends the .cfg's attribute, src/parser/parse_types.cpp:6-13 returns
+ * the first match), so by default a .cfg cannot override a .bnd rate or logic; call this after
+ * parsing (before compiling) to let it. */
+mb_status mb_model_apply_cfg_overrides(mb_model m);
 mb_status mb_model_get_constant(mb_model m, const char* name, float* value);
 mb_status mb_model_set_constant(mb_model m, const char* name, float value);
 mb_status mb_model_get_variable(mb_model m, const char* name, float* value);
@@ -386,6 +392,10 @@ mb_status mb_result_fixed(mb_result r, int i, uint32_t* state_words, unsigned* c
  * (fixed_states.cu:154-187); visualize() text of all three plugins (stdout format of
  * src/main.cpp:85-99). Node names come from the model. */
 mb_status mb_result_write_csv(mb_result r, mb_model m, const char* prefix);
+/* Opt-in, no counterpart in the reference (final_states_stats::write_csv writes nothing,
+ * src/statistics/final_states.cpp:70): the final-state distribution to <prefix>_finalprob.csv in the
+ * MB_FORMAT_CSV_FINAL_STATES layout. */
+mb_status mb_result_write_final_csv(mb_result r, mb_model m, const char* prefix);
 mb_status mb_result_visualize(mb_result r, mb_model m, char* buf, size_t cap, size_t* len);
 /* A result from raw accumulators (for instance the per-rank sums of a sharded run after a
  * collective). Window sums are fixed point: occupancy = time * 2^occupancy_exponent (continuous),
@@ -429,6 +439,10 @@ mb_status mb_result_merge(const mb_result* parts, int n_parts, mb_result* out);
 #define MB_SECTION_WINDOWS 2
 #define MB_FORMAT_VISUALIZE 0
 #define MB_FORMAT_CSV 1
+/* Opt-in, no counterpart in the reference: MB_SECTION_FINAL as a CSV file ("Final States (n)",
+ * "Proba<TAB>State", one line per final state in non-internal index order); other sections as
+ * MB_FORMAT_CSV. */
+#define MB_FORMAT_CSV_FINAL_STATES 2
 mb_status mb_result_format(mb_result r, int section, int format, const char* const* node_names, int n_names,
                            char* buf, size_t cap, size_t* len);
 

@@ -62,6 +62,8 @@ def _declare(L: C.CDLL) -> None:
         "mb_result_create": (i32, [vp, P(vp)]),
         "mb_result_sparse_size": (i32, [vp, P(i64), P(i64), P(C.c_uint)]),
         "mb_result_windows_sparse": (i32, [vp, P(i32)]),
+        "mb_result_write_final_csv": (i32, [vp, vp, C.c_char_p]),
+        "mb_model_apply_cfg_overrides": (i32, [vp]),
         "mb_result_sparse_windows": (i32, [vp, vp, vp, vp, vp]),
         "mb_result_sparse_final": (i32, [vp, vp, vp]),
         "mb_batch_set_options": (i32, [vp, i32, i32]),

@@ -193,6 +193,14 @@ mb_status mb_model_set_istate(mb_model m, int i, float istate)
 	});
 }
 
+mb_status mb_model_apply_cfg_overrides(mb_model m)
+{
+	return guard([&] {
+		need(m, "null model");
+		mb::apply_cfg_overrides(m->model);
+	});
+}
+
 mb_status mb_model_get_constant(mb_model m, const char* name, float* value)
 {
 	return guard([&] {
@@ -1204,6 +1212,19 @@ mb_status mb_result_write_csv(mb_result r, mb_model m, const char* prefix)
 	});
 }
 
+mb_status mb_result_write_final_csv(mb_result r, mb_model m, const char* prefix)
+{
+	return guard([&] {
+		need(r && m && prefix, "null argument");
+		need(r->res->sections & MB_STATS_FINAL, "the result has no final-state statistics");
+		need((int)m->model.nodes.size() == r->res->state_size, "model does not match the result");
+		std::ofstream f(std::string(prefix) + "_finalprob.csv");
+		if (!f)
+			throw mb::engine_error(MB_ERR_INVALID, std::string("cannot write ") + prefix + "_finalprob.csv");
+		f << mb::format_final_csv(*r->res, names_of(m->model));
+	});
+}
+
 mb_status mb_result_info(mb_result r, long long* n_trajectories, int* discrete_time, float* time_tick,
 						 float* max_time, int* noninternal_nodes)
 {
@@ -1302,7 +1323,8 @@ mb_status mb_result_format(mb_result r, int section, int format, const char* con
 		need(r && (node_names || n_names == 0), "null argument");
 		const mb::result& res = *r->res;
 		need(n_names == res.state_size, "one name per node is needed");
-		need(format == MB_FORMAT_VISUALIZE || format == MB_FORMAT_CSV, "unknown format");
+		need(format == MB_FORMAT_VISUALIZE || format == MB_FORMAT_CSV || format == MB_FORMAT_CSV_FINAL_STATES,
+			 "unknown format");
 		std::vector<std::string> names(node_names, node_names + n_names);
 		std::string text;
 		switch (section)
@@ -1311,6 +1333,8 @@ mb_status mb_result_format(mb_result r, int section, int format, const char* con
 			need(res.sections & MB_STATS_FINAL, "the result has no final-state statistics");
 			if (format == MB_FORMAT_VISUALIZE)
 				text = mb::format_final_visualize(res, names);
+			else if (format == MB_FORMAT_CSV_FINAL_STATES)
+				text = mb::format_final_csv(res, names);
 			break;
 		case MB_SECTION_FIXED:
 			need(res.sections & MB_STATS_FIXED, "the result has no fixed-point statistics");

@@ -40,6 +40,23 @@ const expr* node_t::find_attr(const std::string& attr) const
 	return nullptr;
 }
 
+void apply_cfg_overrides(model_t& m)
+{
+	for (auto& node : m.nodes)
+	{
+		decltype(node.attrs) kept;
+		for (auto& a : node.attrs)
+		{
+			auto it = std::find_if(kept.begin(), kept.end(), [&](auto& k) { return k.first == a.first; });
+			if (it == kept.end())
+				kept.push_back(a);
+			else
+				it->second = a.second; // a later definition replaces the earlier one in place
+		}
+		node.attrs = std::move(kept);
+	}
+}
+
 const expr& node_t::get_attr(const std::string& attr) const
 {
 	const expr* e = find_attr(attr);

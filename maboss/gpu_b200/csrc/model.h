@@ -102,6 +102,12 @@ void parse_bnd(model_t& m, const std::string& text, const std::string& file);
 void parse_cfg(model_t& m, const std::string& text, const std::string& file);
 void parse_model_files(model_t& m, const std::string& bnd_path, const std::string& cfg_path);
 
+// Opt-in: every node attribute defined more than once (in the .bnd and again in the .cfg, say) takes
+// its last definition, at the position of its first. The reference keeps the first one
+// (driver.cpp:65-77 appends a .cfg attribute, parse_types.cpp:6-13 returns the first match), so a
+// .cfg cannot change a rate or a logic defined in the .bnd; MaBoSS users expect the .cfg to win.
+void apply_cfg_overrides(model_t& m);
+
 // Float evaluation used for $variables, constants, istate and is_internal
 // (expressions.cpp: every `evaluate` method).
 float evaluate(const model_t& m, const expr& e);

@@ -138,6 +138,25 @@ std::string format_final_visualize(const result& r, const std::vector<std::strin
 	return os.str();
 }
 
+std::string format_final_csv(const result& r, const std::vector<std::string>& names)
+{
+	// the final-state distribution in the layout of the fixed-point file (no counterpart in the
+	// reference, whose final_states_stats::write_csv writes nothing, final_states.cpp:70)
+	std::vector<std::pair<unsigned __int128, unsigned>> rows;
+	if (r.wide)
+		for (size_t i = 0; i < r.fin_idx.size(); i++)
+			rows.push_back({ r.fin_idx[i], r.fin_cnt[i] });
+	for (unsigned b = 0; b < r.n_bins && b < r.final_cnt.size(); b++)
+		if (r.final_cnt[b] != 0)
+			rows.push_back({ b, r.final_cnt[b] });
+	std::ostringstream os;
+	os << "Final States (" << rows.size() << ")" << std::endl;
+	os << "Proba\tState" << std::endl;
+	for (auto& [idx, c] : rows)
+		os << (float)c / (float)r.n_traj << "\t" << idx_name(r, names, idx) << std::endl;
+	return os.str();
+}
+
 std::string format_fixed_visualize(const result& r, const std::vector<std::string>& names)
 {
 	std::ostringstream os;

@@ -19,6 +19,9 @@ std::vector<unsigned> noninternal_index_to_state(const std::vector<int>& noninte
 std::string format_probtraj_csv(const result& r, const std::vector<std::string>& names);
 // <prefix>_fp.csv (fixed_states.cu:154-187).
 std::string format_fp_csv(const result& r, const std::vector<std::string>& names);
+// The final-state distribution as a CSV file (opt-in; the reference writes no such file):
+// "Final States (n)", "Proba\tState", then one line per final state in non-internal index order.
+std::string format_final_csv(const result& r, const std::vector<std::string>& names);
 // stdout output of final_states_stats, fixed_states_stats and window_average_small_stats
 // visualize() in the order of src/main.cpp:65-74.
 std::string format_visualize(const result& r, const std::vector<std::string>& names);

@@ -121,6 +121,11 @@ class Model:
         names = [read_string(lib().mb_model_variable_name, self._h, i) for i in range(n.value)]
         return {k: self.variable(k) for k in names}
 
+    def apply_cfg_overrides(self) -> None:
+        """mb_model_apply_cfg_overrides: node attributes defined again in the .cfg replace the .bnd's
+        (opt-in; the reference keeps the first definition)."""
+        check(lib().mb_model_apply_cfg_overrides(self._h))
+
     def generate_code(self) -> str:
         return read_string(lib().mb_model_generate_code, self._h)
 
@@ -597,6 +602,10 @@ class Result:
 
     def write_csv(self, model: Model, prefix: str) -> None:
         check(lib().mb_result_write_csv(self._h, model._h, prefix.encode()))
+
+    def write_final_csv(self, model: Model, prefix: str) -> None:
+        """mb_result_write_final_csv: <prefix>_finalprob.csv (opt-in; the reference writes no such file)."""
+        check(lib().mb_result_write_final_csv(self._h, model._h, prefix.encode()))
 
     def visualize(self, model: Model) -> str:
         return read_string(lib().mb_result_visualize, self._h, model._h)

@@ -11,6 +11,10 @@
 //     --stats          print transitions and epochs to stderr
 //     --max-noninternal K  accept up to K non-internal nodes (default 20 as the reference; at most
 //                      112: above 20 the window statistics are sparse bins)
+//     --cfg-overrides  node attributes defined again in the .cfg replace the .bnd's (the reference
+//                      keeps the first definition)
+//     --final-csv      with -o, also write <prefix>_finalprob.csv (the reference writes no
+//                      final-state file)
 //   MABOSS_DIAGS=1 prints the timer_stats scopes to stderr.
 #include <algorithm>
 #include <iostream>
@@ -57,14 +61,16 @@ int do_compilation(driver& drv, bool discrete_time, int device, std::optional<ke
 stats_composite do_simulation(bool discrete_time, float max_time, float time_tick, int sample_count, int state_size,
 							  unsigned long long seed, std::vector<float> initial_probs,
 							  const state_t& noninternals_mask, int noninternals_count, kernel_compiler& compiler,
-							  int mode, bool print_stats)
+							  int mode, bool print_stats, bool final_csv)
 {
 	timer_stats stats("main> simulation");
 	simulation_runner r(sample_count, state_size, seed, std::move(initial_probs));
 	r.mode = mode;
 	stats_composite stats_runner;
 	// the three plugins in the order of src/main.cpp:65-74
-	stats_runner.add(std::make_unique<final_states_stats>(noninternals_mask, noninternals_count, compiler.final_states));
+	auto final_stats = std::make_unique<final_states_stats>(noninternals_mask, noninternals_count, compiler.final_states);
+	final_stats->final_csv = final_csv;
+	stats_runner.add(std::move(final_stats));
 	fixed_states_stats_builder::add_fixed_states_stats(stats_runner, (int)noninternals_mask.words_n());
 	stats_runner.add(std::make_unique<window_average_small_stats>(
 		time_tick, max_time, discrete_time, noninternals_mask, noninternals_count, r.trajectory_len_limit,
@@ -89,7 +95,7 @@ void do_visualization(stats_composite& stats_runner, int sample_count, const std
 void usage()
 {
 	std::cout << "Usage: MaBoSS.GPU [--mode exact|fast|epoch] [--device D] [--emit-code] [--stats] "
-				 "[--max-noninternal K] [-o prefix] bnd_file cfg_file"
+				 "[--max-noninternal K] [--cfg-overrides] [--final-csv] [-o prefix] bnd_file cfg_file"
 			  << std::endl;
 }
 
@@ -100,7 +106,7 @@ int main(int argc, char** argv)
 	std::vector<std::string> args(argv + 1, argv + argc);
 	std::string output_prefix, mode_name = "exact";
 	int device = 0, max_noninternal = 20;
-	bool emit = false, print_stats = false;
+	bool emit = false, print_stats = false, cfg_overrides = false, final_csv = false;
 	std::vector<std::string> files;
 	for (size_t i = 0; i < args.size(); i++)
 	{
@@ -117,6 +123,10 @@ int main(int argc, char** argv)
 			emit = true;
 		else if (a == "--stats")
 			print_stats = true;
+		else if (a == "--cfg-overrides")
+			cfg_overrides = true;
+		else if (a == "--final-csv")
+			final_csv = true;
 		else if (!a.empty() && a[0] == '-')
 		{
 			usage();
@@ -140,6 +150,8 @@ int main(int argc, char** argv)
 			timer_stats stats("main> parse");
 			if (drv.parse(files[0], files[1]))
 				return 1;
+			if (cfg_overrides)
+				drv.apply_cfg_overrides();
 		}
 		if (emit)
 		{
@@ -173,7 +185,8 @@ int main(int argc, char** argv)
 			return 1;
 		auto stats_runner =
 			do_simulation(discrete_time, max_time, time_tick, sample_count, (int)drv.nodes.size(), seed,
-						  std::move(initial_probs), noninternals_mask, noninternals_count, *compiler, mode, print_stats);
+						  std::move(initial_probs), noninternals_mask, noninternals_count, *compiler, mode, print_stats,
+						  final_csv);
 		do_visualization(stats_runner, sample_count, node_names, output_prefix);
 	}
 	catch (const std::exception& e)

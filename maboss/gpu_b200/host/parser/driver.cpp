@@ -96,3 +96,11 @@ mb_model driver::model()
 		mirror::check(mb_model_set_istate(model_, (int)i, nodes[i].istate), "driver nodes");
 	return model_;
 }
+
+void driver::apply_cfg_overrides()
+{
+	if (!model_)
+		throw std::runtime_error("driver: no model has been parsed");
+	mirror::check(mb_model_apply_cfg_overrides(model_), "driver");
+	load_members(); // is_internal may have changed
+}

@@ -43,6 +43,10 @@ public:
 	// The parsed model with the public members written back (variables, constants, istate).
 	mb_model model();
 
+	// Opt-in (no counterpart in the reference): node attributes defined again in the .cfg replace
+	// the .bnd's (mb_model_apply_cfg_overrides); the reference keeps the first definition.
+	void apply_cfg_overrides();
+
 private:
 	mb_model model_ = nullptr;
 	void load_members();

@@ -1,5 +1,7 @@
 #include "final_states.h"
 
+#include <fstream>
+
 final_states_stats::final_states_stats(state_t noninternals_mask, int noninternals, kernel_wrapper&)
 	: builtin_stats(MB_STATS_FINAL, MB_SECTION_FINAL),
 	  noninternals_mask_(std::move(noninternals_mask)),
@@ -35,5 +37,15 @@ void final_states_stats::process_batch(soa_ptr<state_word_t>, soa_ptr<float>, so
 				  "final_states");
 }
 
-// final states are printed only (src/statistics/final_states.cpp:70)
-void final_states_stats::write_csv(int, const std::vector<std::string>&, const std::string&) {}
+// final states are printed only (src/statistics/final_states.cpp:70), unless final_csv is set
+void final_states_stats::write_csv(int, const std::vector<std::string>& nodes, const std::string& prefix)
+{
+	if (!final_csv)
+		return;
+	if (!result_)
+		throw std::runtime_error("final_states_stats: write_csv before finalize");
+	std::ofstream f(prefix + "_finalprob.csv");
+	if (!f)
+		throw std::runtime_error("cannot write " + prefix + "_finalprob.csv");
+	f << mirror::format_section(result_->r, MB_SECTION_FINAL, MB_FORMAT_CSV_FINAL_STATES, nodes);
+}

@@ -167,3 +167,49 @@ def test_synthetic_generators_are_seeded_and_parse(gen, kw, nodes, k):
         assert m.num_nodes == nodes
     assert len(m.noninternal_nodes) == k == o.k
     assert m.noninternal_nodes == o.noninternal
+
+
+def test_cfg_overrides_are_opt_in():
+    """A node attribute given again in the .cfg: the reference keeps the .bnd's first definition
+    (driver.cpp:65-77, parse_types.cpp:6-13), so by default the generated rate is the .bnd's;
+    mb_model_apply_cfg_overrides (CLI --cfg-overrides) makes the .cfg's win."""
+    bnd = ("node A { logic = !B; rate_up = @logic ? 2 : 0; rate_down = @logic ? 0 : 3; }\n"
+           "node B { logic = A; rate_up = @logic ? 1 : 0; rate_down = @logic ? 0 : 1; }\n")
+    cfg = "A.rate_up = @logic ? 7.5 : 0; B.is_internal = 1; B.is_internal = 0; max_time = 1; time_tick = 0.5;\n"
+    m = mb.Model(bnd, cfg)
+    code = m.generate_code()
+    assert "(is_up ? 3 : 2)" in code and "7.5" not in code
+    assert m.node_info(1)[1]  # B internal by its first definition
+    assert m.noninternal_nodes == [0]
+    m.apply_cfg_overrides()
+    code = m.generate_code()
+    assert "(is_up ? 3 : 7.5)" in code
+    assert m.noninternal_nodes == [0, 1]
+
+
+def test_cfg_overrides_on_the_command_line(tmp_path):
+    bnd = "node A { logic = !A; rate_up = @logic ? 2 : 0; rate_down = @logic ? 0 : 3; }\n"
+    (tmp_path / "m.bnd").write_text(bnd)
+    (tmp_path / "m.cfg").write_text("A.rate_down = @logic ? 0 : 9; max_time = 1; time_tick = 0.5;\n")
+    cli = os.path.join(ROOT, "maboss", "gpu_b200", "MaBoSS.GPU")
+    a = subprocess.run([cli, "--emit-code", str(tmp_path / "m.bnd"), str(tmp_path / "m.cfg")],
+                       capture_output=True, text=True, check=True).stdout
+    b = subprocess.run([cli, "--cfg-overrides", "--emit-code", str(tmp_path / "m.bnd"), str(tmp_path / "m.cfg")],
+                       capture_output=True, text=True, check=True).stdout
+    assert "(is_up ? 3 : 2)" in a and "(is_up ? 9 : 2)" in b
+
+
+def test_final_states_csv_is_opt_in(tmp_path):
+    """mb_result_write_final_csv (CLI --final-csv): the final-state distribution, which the
+    reference only prints (final_states.cpp:53-70), as <prefix>_finalprob.csv."""
+    names = ["A", "B", "C"]
+    res = mb.Result.from_raw(n_nodes=3, n_windows=2, discrete=True, time_tick=1.0, max_time=2.0,
+                             noninternal=[0, 2], n_trajectories=10, occ_exp=0, ent_exp=0,
+                             cnt=np.zeros(8, np.uint32), h=np.zeros(2, np.int64),
+                             final=np.array([4, 0, 1, 5], np.uint32))
+    bnd = "".join(f"node {n} {{ logic = {n}; rate_up = @logic ? 1 : 0; rate_down = @logic ? 0 : 1; }}\n"
+                  for n in names)
+    model = mb.Model(bnd, "B.is_internal = 1; max_time = 2; time_tick = 1; discrete_time = 1;")
+    res.write_final_csv(model, str(tmp_path / "out"))
+    text = (tmp_path / "out_finalprob.csv").read_text().splitlines()
+    assert text == ["Final States (3)", "Proba\tState", "0.4\t<nil>", "0.1\tC", "0.5\tA -- C"]
