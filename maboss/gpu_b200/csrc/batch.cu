@@ -261,6 +261,11 @@ batch_engine::prepared& batch_engine::prepare(bool grad)
 		mb_net& d = hnets[i];
 		d.N = L.state_size;
 		d.W = L.state_words;
+		// words per register group sum: the smallest power of two >= ceil(W / MBB_GROUPS), so that
+		// the kernel finds a word's group with a shift
+		d.wpg_shift = 0;
+		while ((1 << d.wpg_shift) * MBB_GROUPS < d.W)
+			d.wpg_shift++;
 		d.k = (int)L.noninternal_nodes.size();
 		d.discrete = L.discrete_time ? 1 : 0;
 		d.max_time = print6(L.max_time); // the generated code's 6-digit constants

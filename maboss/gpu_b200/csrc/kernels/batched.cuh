@@ -21,6 +21,7 @@
 struct mb_net
 {
 	int N, W, k, discrete;
+	int wpg_shift; // log2 of the state words per register group sum: 2^wpg_shift >= ceil(W / MBB_GROUPS)
 	float max_time, tick; // simulation constants (as the generated code of the network has them)
 	const uint2* dep;	  // per node: {first record, dependents | (ni_pos + 1) << 16}
 	const uint4* rec;	  // {k | m << 16 | (ni_pos + 1) << 21, truth table or offset, inputs 0-1, inputs 2-3}
@@ -364,7 +365,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 				gsx[g] = 0;
 			unsigned long long tot = 0;
 			uint32_t ix = 0;
-			const int wpg = (net.W + MBB_GROUPS - 1) / MBB_GROUPS;
+			const int wsh = net.wpg_shift;
 			for (int w = 0; w < net.W; w++)
 			{
 				const int i = 32 * w + lane;
@@ -389,7 +390,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 					c.U(w) = um;
 					c.Q(w) = qw;
 				}
-				mbb_group_add(gsx, w / wpg, qw);
+				mbb_group_add(gsx, w >> wsh, qw);
 				tot += qw;
 			}
 			__syncwarp();
@@ -487,8 +488,8 @@ __device__ void mbb_body(const mb_batch_params& B)
 			else
 			{
 				const unsigned long long r = __umul64hi(((unsigned long long)rb.y << 32) | rb.z, total);
-				const int wpg = (net.W + MBB_GROUPS - 1) / MBB_GROUPS;
-				const int ng = (net.W + wpg - 1) / wpg; // groups of this network
+				const int wsh = net.wpg_shift, wpg = 1 << wsh;
+				const int ng = (net.W + wpg - 1) >> wsh; // groups of this network
 				unsigned long long cum = 0;
 				int g = 0;
 				// the first group whose running sum exceeds r (the group sums add up to total, so
@@ -577,7 +578,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 					{
 						const long long dq = (long long)qn - (long long)qo;
 						v.Q(wk) += (uint32_t)dq;
-						mbb_group_add(gs, wk / wpg, dq);
+						mbb_group_add(gs, wk >> wsh, dq);
 						total += (unsigned long long)dq;
 					}
 					if (GRAD && (unstable != was_unstable || on != was_on))

@@ -141,6 +141,58 @@ def test_gradient_matches_common_random_number_finite_differences(gpu, discrete)
     assert np.all(diff <= 4 * se + 0.02 * np.abs(fd.mean(axis=0))), (sf.mean(axis=0), fd.mean(axis=0), se)
 
 
+def _fd_and_sf(gpu, model, names, cot, n, rel_step, seeds):
+    theta = {k: model.variable(k) for k in names}
+    sf, fd = [], []
+    for seed in seeds:
+        g, _ = mb.gradient(gpu, model, theta, cot, n, seed=seed)
+        sf.append(g)
+        b = mb.Batch(gpu)
+        net = b.add_model(model)
+        pairs = []
+        for k in names:
+            hk = rel_step * theta[k]
+            pairs.append((b.add_variant(net, n, dict(theta, **{k: theta[k] + hk})),
+                          b.add_variant(net, n, dict(theta, **{k: theta[k] - hk})), 2 * hk))
+        b.run(seed)
+        fd.append([((b.result(p).window_probs - b.result(m).window_probs) * cot).sum() / span
+                   for p, m, span in pairs])
+    return np.array(sf), np.array(fd)
+
+
+def test_gradient_at_the_gradient_configuration(gpu):
+    """The gradient configuration itself: the 50-node network, all 40 rate parameters, 1e6
+    trajectories, central finite differences with common random numbers at h = 1e-3 relative
+    (variants sharing random streams in one batched launch), 4 seeds. Criterion per parameter:
+    |SF - FD| <= 4 combined standard errors + 2 % of |FD| (both are Monte-Carlo estimates). The
+    measured standard errors at h = 1e-3 and h = 1e-2 and the largest relative deviation among the
+    parameters whose finite difference is resolved (standard error below 2 % of its value) are
+    printed."""
+    model = mb.Model(*synth.c4())
+    names = sorted(model.variables)
+    assert len(names) == 40
+    n = 1_000_000
+    dims = gpu.compile(model).run(mode="fast", sample_count=10).dims
+    cot = np.zeros((dims.windows, dims.bins))
+    cot[:, [s for s in range(dims.bins) if s & 1]] = 1.0
+    seeds = range(4)
+    sf, fd = _fd_and_sf(gpu, model, names, cot, n, 1e-3, seeds)
+    m_sf, m_fd = sf.mean(axis=0), fd.mean(axis=0)
+    se_sf, se_fd = sf.std(axis=0, ddof=1) / 2.0, fd.std(axis=0, ddof=1) / 2.0
+    se = np.sqrt(se_sf ** 2 + se_fd ** 2)
+    diff = np.abs(m_sf - m_fd)
+    _, fd2 = _fd_and_sf(gpu, model, names, cot, n, 1e-2, seeds)
+    se_fd2 = fd2.std(axis=0, ddof=1) / 2.0
+    resolved = se_fd < 0.02 * np.abs(m_fd)
+    rel = diff / np.maximum(np.abs(m_fd), 1e-30)
+    print(f"\ngradient configuration: median |SF| {np.median(np.abs(m_sf)):.4g}, median SE(SF) "
+          f"{np.median(se_sf):.3g}, median SE(FD) at h=1e-3 {np.median(se_fd):.3g}, at h=1e-2 "
+          f"{np.median(se_fd2):.3g}; resolved at h=1e-3: {int(resolved.sum())} of 40; max relative deviation "
+          f"among them {rel[resolved].max() if resolved.any() else float('nan'):.4f}; max deviation in "
+          f"combined standard errors {np.max(diff / se):.2f}")
+    assert np.all(diff <= 4 * se + 0.02 * np.abs(m_fd)), (m_sf, m_fd, se)
+
+
 @pytest.mark.parametrize("discrete", [False, True], ids=["continuous", "discrete"])
 def test_gradient_equals_oracle_on_the_same_trajectories(gpu, discrete):
     """The kernel's gradient (incremental d a0 / d theta, slices summed by parts, fp32 scores)
