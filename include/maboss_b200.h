@@ -317,6 +317,12 @@ mb_status mb_batch_result(mb_batch b, int v, mb_result* out);
  * (threads per block, resident blocks per SM) is chosen by timing candidates on the batch itself.
  * Changing the batch (add_model / add_variant) drops the graph and the chosen shape. */
 mb_status mb_batch_set_options(mb_batch b, int use_graph, int autotune);
+/* A batch of one network runs by default kernels compiled for that network (NVRTC on its first run:
+ * the network's sizes and tables are compile-time, the variants' rates and derivatives stay runtime,
+ * so mb_batch_set_variables needs no recompilation); on = 0 selects the ahead-of-time kernels that
+ * take any set of networks. Both give the same results. No counterpart in the reference (it has no
+ * batched runs). */
+mb_status mb_batch_set_specialize(mb_batch b, int on);
 /* The launch shape of the last run, the node count of its graph (0 without one) and the number of
  * launch shapes timed by the autotuner so far. */
 mb_status mb_batch_info(mb_batch b, int* block, int* blocks_per_sm, unsigned* grid, unsigned* graph_nodes,

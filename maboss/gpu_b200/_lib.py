@@ -67,6 +67,7 @@ def _declare(L: C.CDLL) -> None:
         "mb_result_sparse_windows": (i32, [vp, vp, vp, vp, vp]),
         "mb_result_sparse_final": (i32, [vp, vp, vp]),
         "mb_batch_set_options": (i32, [vp, i32, i32]),
+        "mb_batch_set_specialize": (i32, [vp, i32]),
         "mb_autotune": (i32, [vp, vp, P(f32), P(i32), P(f32), i32, P(i32)]),
         "mb_batch_info": (i32, [vp, P(i32), P(i32), P(C.c_uint), P(C.c_uint), P(i32)]),
         "mb_batch_tuning": (i32, [vp, i32, P(i32), P(i32), P(i32), P(f32)]),

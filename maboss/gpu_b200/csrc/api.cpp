@@ -883,6 +883,14 @@ mb_status mb_batch_set_options(mb_batch b, int use_graph, int autotune)
 	});
 }
 
+mb_status mb_batch_set_specialize(mb_batch b, int on)
+{
+	return guard([&] {
+		need(b, "null batch");
+		b->b->specialize = on != 0;
+	});
+}
+
 mb_status mb_batch_info(mb_batch b, int* block, int* blocks_per_sm, unsigned* grid, unsigned* graph_nodes,
 						int* tuned_shapes)
 {

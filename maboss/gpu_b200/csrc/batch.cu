@@ -353,6 +353,14 @@ batch_engine::prepared& batch_engine::prepare(bool grad)
 	B.next = ps->counters.as<unsigned long long>();
 	B.errors = ps->counters.as<unsigned>() + 4;
 	ps->fn = grad ? (const void*)mb_batched_grad : (const void*)mb_batched_fast;
+	if (specialize && nets.size() == 1)
+	{
+		network& N = *nets[0];
+		if (!N.mod)
+			N.mod = compile_batch_module(*ctx, generate_code(N.model));
+		N.mod->ensure(FAMILY_BATCH);
+		ps->fn = grad ? N.mod->batched_grad_static : N.mod->batched_fast_static;
+	}
 	ps->smem_per_thread = (3 * (size_t)max_W + (grad ? 2 * (size_t)P : 0)) * 4;
 	MB_CUDA(cudaStreamSynchronize(s));
 	slot = std::move(ps);

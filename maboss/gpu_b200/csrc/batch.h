@@ -47,6 +47,8 @@ public:
 		model_t model;
 		model_layout L;
 		dbuf dep, rec, ext, tt, self, ni_node;
+		// the batched kernels compiled for this network alone (NVRTC, FAMILY_BATCH; on first use)
+		std::unique_ptr<module> mod;
 	};
 	struct variant
 	{
@@ -82,6 +84,10 @@ public:
 	// with the seed updated; the launch shape is chosen by timing candidates on the batch first.
 	bool use_graph = true;
 	bool autotune = true;
+	// A batch of one network runs the batched kernels compiled for that network (its sizes and
+	// tables compile-time, the variants' rates runtime; NVRTC on the first run, a few seconds);
+	// false: the ahead-of-time kernels that take any networks.
+	bool specialize = true;
 	struct tuning_point
 	{
 		bool grad;

@@ -1,6 +1,6 @@
 """Embed the engine's CUDA sources as C++ raw-string constants (build step).
 
-usage: python embed.py OUT.inc params.cuh common.cuh engine.cuh
+usage: python embed.py OUT.inc params.cuh common.cuh engine.cuh batched.cuh
 """
 import sys
 
@@ -16,13 +16,13 @@ def raw(name: str, path: str) -> str:
 
 
 def main() -> None:
-    out, params, common, engine = sys.argv[1:5]
+    out, params, common, engine, batched = sys.argv[1:6]
     src = "// generated by embed.py -- do not edit\n"
     text = open(params, encoding="utf-8").read() + "\n" + open(common, encoding="utf-8").read()
     tmp = out + ".params.tmp"
     with open(tmp, "w", encoding="utf-8") as f:
         f.write(text)
-    src += raw("mb_params_source", tmp) + raw("mb_engine_source", engine)
+    src += raw("mb_params_source", tmp) + raw("mb_engine_source", engine) + raw("mb_batched_source", batched)
     import os
     os.remove(tmp)
     with open(out, "w", encoding="utf-8") as f:

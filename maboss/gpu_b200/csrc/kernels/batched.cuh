@@ -67,6 +67,30 @@ struct mb_batch_params
 	unsigned gstride;	  // gstride = the launch's thread count
 };
 
+// Network access of the kernel body. mbb_net_rt reads a network's descriptor (every network of a
+// batch is runtime data: one launch covers networks of different sizes); the NVRTC build of a
+// single network's batch (MB_FAMILY_BATCH, below) instead gives the same quantities as compile-time
+// constants and tables of that network's generated code, so that loops over its words unroll and
+// no descriptor is read. The variant data (rates, derivatives, accumulators) stays runtime in both.
+struct mbb_net_rt
+{
+	const mb_net& n;
+	__device__ __forceinline__ mbb_net_rt(const mb_batch_params& B, const mb_variant& v) : n(B.nets[v.net]) {}
+	__device__ __forceinline__ int N() const { return n.N; }
+	__device__ __forceinline__ int W() const { return n.W; }
+	__device__ __forceinline__ int k() const { return n.k; }
+	__device__ __forceinline__ bool discrete() const { return n.discrete != 0; }
+	__device__ __forceinline__ float max_time() const { return n.max_time; }
+	__device__ __forceinline__ float tick() const { return n.tick; }
+	__device__ __forceinline__ int wpg_shift() const { return n.wpg_shift; }
+	__device__ __forceinline__ const uint2* dep() const { return n.dep; }
+	__device__ __forceinline__ const uint4* rec() const { return n.rec; }
+	__device__ __forceinline__ const uint4* ext() const { return n.ext; }
+	__device__ __forceinline__ const unsigned* tt() const { return n.tt; }
+	__device__ __forceinline__ const int* self() const { return n.self; }
+	__device__ __forceinline__ const int* ni_node() const { return n.ni_node; }
+};
+
 // register group sums; words per group = ceil(W / 8). Measured on C5 (256 variants, 1 to 16 words):
 // 8 groups 7.26e9 transitions/s, 4 groups 6.70e9, 16 groups 6.34e9 (predicated updates of every
 // group register at each rate change cost more than the longer word walk saves)
@@ -93,7 +117,8 @@ struct mbb_lane
 	__device__ __forceinline__ double* GR(int p) const { return gR + (size_t)p * gstride; }
 };
 
-__device__ __forceinline__ bool mbb_logic(const mb_net& net, const mbb_lane& v, int r, const uint4& rec)
+template <class NET>
+__device__ __forceinline__ bool mbb_logic(const NET& net, const mbb_lane& v, int r, const uint4& rec)
 {
 	const int m = (rec.x >> 16) & 31;
 	const unsigned ins[2] = { rec.z, rec.w };
@@ -109,7 +134,7 @@ __device__ __forceinline__ bool mbb_logic(const mb_net& net, const mbb_lane& v, 
 	}
 	if (m > 4)
 	{
-		const uint4 ext = __ldg(net.ext + r);
+		const uint4 ext = __ldg(net.ext() + r);
 		const unsigned ins2[4] = { ext.x, ext.y, ext.z, ext.w };
 #pragma unroll
 		for (int t = 4; t < 12; t++)
@@ -121,7 +146,7 @@ __device__ __forceinline__ bool mbb_logic(const mb_net& net, const mbb_lane& v, 
 			}
 		}
 	}
-	const unsigned ttw = m <= 5 ? rec.y : __ldg(net.tt + rec.y + (p >> 5));
+	const unsigned ttw = m <= 5 ? rec.y : __ldg(net.tt() + rec.y + (p >> 5));
 	return (ttw >> (p & 31)) & 1u;
 }
 
@@ -132,12 +157,13 @@ __device__ __forceinline__ void mbb_group_add(unsigned long long (&gs)[MBB_GROUP
 		gs[i] += (i == g) ? (unsigned long long)d : 0ull;
 }
 
-__device__ __forceinline__ float mbb_entropy(const mb_net& net, const mb_variant& var, const mbb_lane& v)
+template <class NET>
+__device__ __forceinline__ float mbb_entropy(const NET& net, const mb_variant& var, const mbb_lane& v)
 {
 	float t = 0.f, tl = 0.f;
-	for (int k = 0; k < net.k; k++)
+	for (int k = 0; k < net.k(); k++)
 	{
-		const int i = __ldg(net.ni_node + k);
+		const int i = __ldg(net.ni_node() + k);
 		const uint32_t bit = 1u << (i & 31);
 		if (v.U(i >> 5) & bit)
 		{
@@ -266,7 +292,7 @@ __device__ __forceinline__ void mbb_record(const mb_variant& var, const mbb_lane
 	}
 }
 
-template <bool GRAD>
+template <bool GRAD, class NET>
 __device__ void mbb_body(const mb_batch_params& B)
 {
 	extern __shared__ uint32_t mbb_smem[];
@@ -337,18 +363,18 @@ __device__ void mbb_body(const mb_batch_params& B)
 			const unsigned long long ts = __shfl_sync(0xffffffffu, t, src);
 			const int vs = __shfl_sync(0xffffffffu, tv, src);
 			const mb_variant& var = B.vars[vs];
-			const mb_net& net = B.nets[var.net];
+			const NET net(B, var);
 			const unsigned long long stream = var.first_traj + (ts - var.begin);
 			mbb_lane c = v;
 			const int off = (int)threadIdx.x - ((threadIdx.x & ~31) + src);
 			c.st = v.st - off;
 			c.un = v.un - off;
 			c.ws = v.ws - off;
-			for (int w = 0; w < net.W; w++)
+			for (int w = 0; w < net.W(); w++)
 			{
 				const int i = 32 * w + lane;
 				bool on = false;
-				if (i < net.N)
+				if (i < net.N())
 				{
 					curandStatePhilox4_32_10_t r;
 					curand_init(B.seed, stream, (unsigned long long)i, &r);
@@ -365,17 +391,17 @@ __device__ void mbb_body(const mb_batch_params& B)
 				gsx[g] = 0;
 			unsigned long long tot = 0;
 			uint32_t ix = 0;
-			const int wsh = net.wpg_shift;
-			for (int w = 0; w < net.W; w++)
+			const int wsh = net.wpg_shift();
+			for (int w = 0; w < net.W(); w++)
 			{
 				const int i = 32 * w + lane;
 				const bool on = (c.S(w) >> lane) & 1u;
 				bool unstable = false;
 				uint32_t q = 0, nibit = 0;
-				if (i < net.N)
+				if (i < net.N())
 				{
-					const int r = __ldg(net.self + i);
-					const uint4 rec = __ldg(net.rec + r);
+					const int r = __ldg(net.self() + i);
+					const uint4 rec = __ldg(net.rec() + r);
 					unstable = on != mbb_logic(net, c, r, rec);
 					const uint2 qq = __ldg(var.q + i);
 					q = unstable ? (on ? qq.y : qq.x) : 0u;
@@ -407,9 +433,9 @@ __device__ void mbb_body(const mb_batch_params& B)
 		{
 			vi = tv;
 			const mb_variant& var = B.vars[vi];
-			const mb_net& net = B.nets[var.net];
+			const NET net(B, var);
 			const unsigned long long stream = var.first_traj + (t - var.begin);
-			curand_init(B.seed, stream, (unsigned long long)((net.N + 3) & ~3), &rng);
+			curand_init(B.seed, stream, (unsigned long long)((net.N() + 3) & ~3), &rng);
 			h = mbb_entropy(net, var, v);
 			time = 0.f;
 			running = true;
@@ -427,7 +453,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 			{
 				C1 = C2 = 0.0;
 				// d a0 / d theta of the initial state: every unstable node's active-direction derivatives
-				for (int w = 0; w < net.W; w++)
+				for (int w = 0; w < net.W(); w++)
 				{
 					uint32_t um = v.U(w);
 					const uint32_t sw = v.S(w);
@@ -435,7 +461,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 					{
 						const int b = __ffs(um) - 1;
 						um &= um - 1u;
-						mbb_grad_active(var, v, 32 * w + b, (sw >> b) & 1u, 1.f, 0.f, net.discrete, C1, C2);
+						mbb_grad_active(var, v, 32 * w + b, (sw >> b) & 1u, 1.f, 0.f, net.discrete(), C1, C2);
 					}
 				}
 			}
@@ -444,9 +470,9 @@ __device__ void mbb_body(const mb_batch_params& B)
 		if (running)
 		{
 			const mb_variant& var = B.vars[vi];
-			const mb_net& net = B.nets[var.net];
-			const bool discrete = net.discrete != 0;
-			const float max_time = net.max_time, tick = net.tick;
+			const NET net(B, var);
+			const bool discrete = net.discrete();
+			const float max_time = net.max_time(), tick = net.tick();
 			const uint4 rb = curand4(&rng);
 			float tn;
 			if (total == 0)
@@ -475,7 +501,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 				if (total == 0)
 				{
 					unsigned st[64];
-					const int W = net.W < 64 ? net.W : 64;
+					const int W = net.W() < 64 ? net.W() : 64;
 					for (int w = 0; w < W; w++)
 						st[w] = v.S(w);
 					mb_fixed_insert_rt(var.st, st, W);
@@ -488,8 +514,8 @@ __device__ void mbb_body(const mb_batch_params& B)
 			else
 			{
 				const unsigned long long r = __umul64hi(((unsigned long long)rb.y << 32) | rb.z, total);
-				const int wsh = net.wpg_shift, wpg = 1 << wsh;
-				const int ng = (net.W + wpg - 1) >> wsh; // groups of this network
+				const int wsh = net.wpg_shift(), wpg = 1 << wsh;
+				const int ng = (net.W() + wpg - 1) >> wsh; // groups of this network
 				unsigned long long cum = 0;
 				int g = 0;
 				// the first group whose running sum exceeds r (the group sums add up to total, so
@@ -506,7 +532,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 				for (int i = 0; i < wpg; i++)
 				{
 					const int w = g * wpg + i;
-					if (w >= net.W)
+					if (w >= net.W())
 						break;
 					word = w;
 					const uint32_t q = v.Q(w);
@@ -552,7 +578,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 
 				// flip j and re-evaluate it and the nodes whose logic reads it
 				v.S(j >> 5) ^= 1u << (j & 31);
-				const uint2 nj = __ldg(net.dep + j);
+				const uint2 nj = __ldg(net.dep() + j);
 				const int pj = (int)(nj.y >> 16) - 1;
 				if (pj >= 0)
 					idx ^= 1u << pj;
@@ -560,7 +586,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 				const int d0 = (int)nj.x, d1 = d0 + (int)(nj.y & 0xffffu);
 				for (int d = d0; d < d1; d++)
 				{
-					const uint4 rec = __ldg(net.rec + d);
+					const uint4 rec = __ldg(net.rec() + d);
 					const int k = (int)(rec.x & 0xffffu);
 					const int wk = k >> 5;
 					const uint32_t bk = 1u << (k & 31);
@@ -605,5 +631,38 @@ __device__ void mbb_body(const mb_batch_params& B)
 	}
 }
 
-extern "C" __global__ void __launch_bounds__(128, 5) mb_batched_fast(mb_batch_params B) { mbb_body<false>(B); }
-extern "C" __global__ void __launch_bounds__(128, 5) mb_batched_grad(mb_batch_params B) { mbb_body<true>(B); }
+#ifndef MB_FAMILY_BATCH
+extern "C" __global__ void __launch_bounds__(128, 5) mb_batched_fast(mb_batch_params B) { mbb_body<false, mbb_net_rt>(B); }
+extern "C" __global__ void __launch_bounds__(128, 5) mb_batched_grad(mb_batch_params B) { mbb_body<true, mbb_net_rt>(B); }
+#else
+// NVRTC build for a batch of one network (compiled together with that network's generated code):
+// its structure is compile-time, its rates stay the variants' runtime tables.
+struct mbb_net_static
+{
+	__device__ __forceinline__ mbb_net_static(const mb_batch_params&, const mb_variant&) {}
+	__device__ __forceinline__ static constexpr int N() { return state_size; }
+	__device__ __forceinline__ static constexpr int W() { return state_words; }
+	__device__ __forceinline__ static constexpr int k() { return mbg_noninternal_count; }
+	__device__ __forceinline__ static constexpr bool discrete() { return discrete_time; }
+	__device__ __forceinline__ static constexpr float max_time() { return ::max_time; }
+	__device__ __forceinline__ static constexpr float tick() { return time_tick; }
+	__device__ __forceinline__ static constexpr int wpg_shift()
+	{
+		return state_words <= MBB_GROUPS ? 0 : state_words <= 2 * MBB_GROUPS ? 1 : state_words <= 4 * MBB_GROUPS ? 2 : 3;
+	}
+	__device__ __forceinline__ static const uint2* dep() { return reinterpret_cast<const uint2*>(mbg_inc_dep); }
+	__device__ __forceinline__ static const uint4* rec() { return mbg_inc_crec; }
+	__device__ __forceinline__ static const uint4* ext() { return mbg_inc_cext; }
+	__device__ __forceinline__ static const unsigned* tt() { return mbg_inc_tt; }
+	__device__ __forceinline__ static const int* self() { return mbg_inc_self; }
+	__device__ __forceinline__ static const int* ni_node() { return mbg_inc_ni_node; }
+};
+extern "C" __global__ void __launch_bounds__(128, 5) mb_batched_fast_static(mb_batch_params B)
+{
+	mbb_body<false, mbb_net_static>(B);
+}
+extern "C" __global__ void __launch_bounds__(128, 5) mb_batched_grad_static(mb_batch_params B)
+{
+	mbb_body<true, mbb_net_static>(B);
+}
+#endif

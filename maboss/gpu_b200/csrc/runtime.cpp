@@ -191,20 +191,28 @@ module::~module()
 {
 	cudaSetDevice(ctx->device);
 	last_runner.reset();
-	for (CUmodule& m : mods)
-		if (m)
-			drv().ModuleUnload(m);
+	for (int f = 0; f < FAMILY_COUNT; f++)
+		if (mods[f] && f != FAMILY_BATCH)
+			drv().ModuleUnload(mods[f]);
+	if (batch_lib)
+		cudaLibraryUnload(batch_lib);
 }
 
 std::vector<char> compile_cubin(const std::string& generated_code, std::string& log, int family)
 {
 	static const char* defines[FAMILY_COUNT] = { "#define MB_FAMILY_EXACT 1\n", "#define MB_FAMILY_FAST 1\n",
 												 "#define MB_FAMILY_EPOCH 1\n",
-												 "#define MB_FAMILY_EPOCH 1\n#define MB_EPOCH_DENSE 1\n" };
+												 "#define MB_FAMILY_EPOCH 1\n#define MB_EPOCH_DENSE 1\n",
+												 "#define MB_FAMILY_BATCH 1\n" };
 	if (family < 0 || family >= FAMILY_COUNT)
 		throw engine_error(MB_ERR_INVALID, "bad kernel family");
+	if (family == FAMILY_BATCH && generated_code.find("#define MBG_INCREMENTAL 1") == std::string::npos)
+		throw engine_error(MB_ERR_INVALID, "the batched kernels need a model whose rates all have the @logic form");
 	const std::string source = generated_code + "\n// ---- engine: kernel parameter blocks\n" + mb_params_source +
-							   "\n// ---- engine: kernels\n" + defines[family] + mb_engine_source;
+							   "\n// ---- engine: kernels\n" + defines[family] + mb_engine_source +
+							   (family == FAMILY_BATCH ? std::string("\n// ---- engine: batched kernels\n") +
+															 mb_batched_source
+													   : std::string());
 	const int N = parse_constexpr(generated_code, "state_size", -1);
 	const int W = parse_constexpr(generated_code, "state_words", -1);
 	if (N <= 0 || W != (N + 31) / 32)
@@ -258,6 +266,19 @@ std::unique_ptr<module> compile_module(context& ctx, const std::string& generate
 	return m;
 }
 
+std::unique_ptr<module> compile_batch_module(context& ctx, const std::string& generated_code)
+{
+	auto m = std::make_unique<module>();
+	m->ctx = &ctx;
+	m->state_size = parse_constexpr(generated_code, "state_size", -1);
+	m->state_words = parse_constexpr(generated_code, "state_words", -1);
+	m->noninternal_count = parse_constexpr(generated_code, "mbg_noninternal_count", -1);
+	m->incremental = generated_code.find("#define MBG_INCREMENTAL 1") != std::string::npos;
+	m->integer_rates = generated_code.find("#define MBG_INTEGER_RATES 1") != std::string::npos;
+	m->source = generated_code;
+	return m;
+}
+
 namespace {
 std::mutex family_mu;
 }
@@ -274,6 +295,17 @@ void module::ensure(int family)
 	compile_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 	if (!lg.empty())
 		log += lg;
+	if (family == FAMILY_BATCH)
+	{
+		cudaKernel_t kf = nullptr, kg = nullptr;
+		MB_CUDA(cudaLibraryLoadData(&batch_lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+		MB_CUDA(cudaLibraryGetKernel(&kf, batch_lib, "mb_batched_fast_static"));
+		MB_CUDA(cudaLibraryGetKernel(&kg, batch_lib, "mb_batched_grad_static"));
+		batched_fast_static = reinterpret_cast<const void*>(kf);
+		batched_grad_static = reinterpret_cast<const void*>(kg);
+		mods[family] = reinterpret_cast<CUmodule>(batch_lib); // marks the family as loaded
+		return;
+	}
 	CUmodule cm = nullptr;
 	cu_throw(drv().ModuleLoadData(&cm, cubin.data()), "cuModuleLoadData");
 	mods[family] = cm;

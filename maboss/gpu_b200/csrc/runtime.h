@@ -72,14 +72,20 @@ enum kernel_family : int
 	FAMILY_FAST = 1,  // mb_fused_fast (incremental or dense)
 	FAMILY_EPOCH = 2, // mb_simulate_epoch (incremental for @logic-form models, else dense)
 	FAMILY_EPOCH_DENSE = 3, // mb_simulate_epoch with every node's rate function evaluated per step
-	FAMILY_COUNT = 4
+	FAMILY_BATCH = 4, // mb_batched_fast_static / mb_batched_grad_static: the batched kernels for this network
+	FAMILY_COUNT = 5
 };
 
 // Kernel handles resolved from NVRTC-compiled modules.
 struct module
 {
 	context* ctx = nullptr;
-	CUmodule mods[FAMILY_COUNT] = { nullptr, nullptr, nullptr, nullptr };
+	CUmodule mods[FAMILY_COUNT] = { nullptr, nullptr, nullptr, nullptr, nullptr };
+	// FAMILY_BATCH is loaded as a runtime-API library: its kernels are cudaKernel_t handles, which the
+	// batch engine's runtime-API launches, occupancy queries and graph nodes take like its own kernels
+	cudaLibrary_t batch_lib = nullptr;
+	const void* batched_fast_static = nullptr;
+	const void* batched_grad_static = nullptr;
 	int state_size = 0, state_words = 0;
 	int noninternal_count = -1; // from the generated code (mbg_noninternal_count), -1 if absent
 	bool incremental = false;	// @logic-form model: exact and epoch modes use the incremental kernels (generated MBG_INCREMENTAL)
@@ -106,6 +112,9 @@ struct module
 
 // Compile generated model code together with the engine kernels (NVRTC, -arch=sm_100a).
 std::unique_ptr<module> compile_module(context& ctx, const std::string& generated_code);
+// A module whose kernel families are all compiled on first use (compile_module compiles the fast
+// family at once); the batch engine uses it for FAMILY_BATCH only.
+std::unique_ptr<module> compile_batch_module(context& ctx, const std::string& generated_code);
 // NVRTC compilation only (no device needed): returns the cubin, throws on failure.
 std::vector<char> compile_cubin(const std::string& generated_code, std::string& log, int family = FAMILY_FAST);
 

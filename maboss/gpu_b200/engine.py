@@ -365,6 +365,11 @@ class Batch:
         check(lib().mb_batch_result(self._h, variant, C.byref(h)))
         return Result(h)
 
+    def set_specialize(self, on: bool = True) -> None:
+        """mb_batch_set_specialize: a batch of one network runs kernels compiled for it (default) or
+        the ahead-of-time kernels that take any networks; both give the same results."""
+        check(lib().mb_batch_set_specialize(self._h, 1 if on else 0))
+
     def set_options(self, use_graph: bool = True, autotune: bool = True) -> None:
         """mb_batch_set_options: CUDA-graph replay of runs and launch-shape autotuning."""
         check(lib().mb_batch_set_options(self._h, 1 if use_graph else 0, 1 if autotune else 0))
