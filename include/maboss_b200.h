@@ -245,6 +245,11 @@ typedef struct mb_run_config_s
                                       so that mb_result_merge of the shards is exact */
     int bin_capacity_log2;         /* more than 20 non-internal nodes: log2 of the sparse-bin table size
                                       (24 bytes a slot), 0 = automatic (4 (T+1) n slots, 2^16 to 2^28) */
+    int refill_reuse_rng;          /* epoch modes with more trajectories than one batch: 0 (default), a refilled
+                                      slot's trajectory gets its own random stream (trajectory id); 1, it
+                                      continues the random state of the trajectory that finished in that slot,
+                                      in the order thrust::partition leaves them, as the reference does
+                                      (simulation_runner.cu:126-153): the reference's results for n > batch */
 } mb_run_config;
 
 /* Defaults from the model's .cfg constants: mode FUSED_EXACT, traj_len 100, batch 1e6. */

@@ -624,6 +624,7 @@ mb_status mb_run_config_default(mb_model m, mb_run_config* cfg)
 		c.fixed_capacity_log2 = 0;
 		c.stats_trajectories = 0;
 		c.bin_capacity_log2 = 0;
+		c.refill_reuse_rng = 0;
 		*cfg = c;
 	});
 }
@@ -643,6 +644,7 @@ mb::run_config to_config(mb_module mod, const mb_run_config* cfg)
 	c.fixed_capacity_log2 = cfg->fixed_capacity_log2;
 	c.stats_trajectories = cfg->stats_trajectories;
 	c.bin_capacity_log2 = cfg->bin_capacity_log2;
+	c.refill_reuse_rng = cfg->refill_reuse_rng != 0;
 	return c;
 }
 } // namespace
@@ -744,6 +746,7 @@ mb_status mb_run_module(mb_module mod, const mb_run_config* cfg, const mb_run_pa
 		c.fixed_capacity_log2 = cfg->fixed_capacity_log2;
 		c.stats_trajectories = cfg->stats_trajectories;
 		c.bin_capacity_log2 = cfg->bin_capacity_log2;
+		c.refill_reuse_rng = cfg->refill_reuse_rng != 0;
 		auto r = std::make_unique<mb_result_s>();
 		r->res = mb::run(*mod->mod, c);
 		*out = r.release();

@@ -1469,7 +1469,8 @@ extern "C" __global__ void __launch_bounds__(MB_SCAN_BLOCK)
 	mb_compact_scatter(int n, int stride, const uint8_t* __restrict__ statuses,
 					   const unsigned* __restrict__ block_offsets, const uint32_t* __restrict__ src_states,
 					   const float* __restrict__ src_times, const curandState* __restrict__ src_rands,
-					   uint32_t* __restrict__ dst_states, float* __restrict__ dst_times, curandState* __restrict__ dst_rands)
+					   uint32_t* __restrict__ dst_states, float* __restrict__ dst_times, curandState* __restrict__ dst_rands,
+					   int rejected_rands)
 {
 	__shared__ unsigned warp_sums[MB_SCAN_BLOCK / 32];
 	const int id = blockIdx.x * MB_SCAN_BLOCK + threadIdx.x;
@@ -1493,16 +1494,24 @@ extern "C" __global__ void __launch_bounds__(MB_SCAN_BLOCK)
 		warp_sums[lane] = inc - v;
 	}
 	__syncthreads();
+	const unsigned kept_before = block_offsets[blockIdx.x] + warp_sums[warp] + __popc(ballot & ((1u << lane) - 1u));
 	if (keep)
 	{
-		const unsigned dst = block_offsets[blockIdx.x] + warp_sums[warp] + __popc(ballot & ((1u << lane) - 1u));
+		const unsigned dst = kept_before;
 #pragma unroll
 		for (int w = 0; w < state_words; w++)
 			dst_states[(size_t)w * stride + dst] = src_states[(size_t)w * stride + id];
 		dst_times[dst] = src_times[id];
 		dst_rands[dst] = src_rands[id];
 	}
+	else if (rejected_rands && id < n)
+	{
+		// the finished trajectories' random states behind the kept ones, last first: where
+		// thrust::partition (simulation_runner.cu:133-137) leaves them for the refill to continue
+		dst_rands[n - 1 - (id - kept_before)] = src_rands[id];
+	}
 }
+
 
 // ---- compaction of the fixed-point table into (state, count) records
 extern "C" __global__ void mb_fixed_extract(unsigned cap, const mb_key128* __restrict__ keys,

@@ -976,7 +976,7 @@ size_t partition_scratch_bytes(int n)
 
 void partition(module& m, cudaStream_t s, int n, int stride, const unsigned char* statuses, const unsigned* states,
 			   const float* times, const void* rands, unsigned* out_states, float* out_times, void* out_rands,
-			   void* scratch, unsigned* kept)
+			   void* scratch, unsigned* kept, bool rejected_rands)
 {
 	if (n < 0 || stride < n)
 		throw engine_error(MB_ERR_INVALID, "partition: need 0 <= n <= stride");
@@ -995,7 +995,8 @@ void partition(module& m, cudaStream_t s, int n, int stride, const unsigned char
 	launch(m.compact_count, nb, 1024, 0, s, a1);
 	void* a2[] = { &nb, &bcp, &bop };
 	launch(m.compact_scan, 1, 1024, 0, s, a2);
-	void* a3[] = { &n, &stride, &statuses, &bop, &states, &times, &rands, &out_states, &out_times, &out_rands };
+	int rej = rejected_rands ? 1 : 0;
+	void* a3[] = { &n, &stride, &statuses, &bop, &states, &times, &rands, &out_states, &out_times, &out_rands, &rej };
 	launch(m.compact_scatter, nb, 1024, 0, s, a3);
 	MB_CUDA(cudaMemcpyAsync(kept, bop + nb, sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
 }
@@ -1019,20 +1020,27 @@ void run_epochs(module& m, const run_config& c, stats_state& st, long long n, cu
 	unsigned long long* trans = st.transitions();
 	float* istate = st.istate.as<float>();
 
-	auto init = [&](int cnt, int offset, unsigned long long first, dbuf& sbuf, dbuf& tbuf, dbuf& rbuf) {
+	// fresh_rng: new random streams (trajectory id `first` + i); else the refilled slots continue the
+	// random states that the partition left there (the reference's refill, simulation_runner.cu:150-153)
+	auto init = [&](int cnt, int offset, unsigned long long first, dbuf& sbuf, dbuf& tbuf, dbuf& rbuf,
+					bool fresh_rng) {
 		unsigned long long seed = c.seed;
 		void* rptr = rbuf.as<char>() + (size_t)offset * sizeof(curandState);
 		void* a1[] = { &cnt, &seed, &first, &rptr };
-		launch(m.init_random, (cnt + 255) / 256, 256, 0, s, a1);
+		if (fresh_rng)
+		{
+			launch(m.init_random, (cnt + 255) / 256, 256, 0, s, a1);
+			launches++;
+		}
 		int stride = B;
 		unsigned* sp = sbuf.as<unsigned>() + offset;
 		float* tp = tbuf.as<float>() + offset;
 		void* a2[] = { &cnt, &stride, &istate, &sp, &tp, &rptr };
 		launch(m.init_state, (cnt + 255) / 256, 256, 0, s, a2);
-		launches += 2;
+		launches++;
 	};
 
-	init(B, 0, c.first_traj, st0, t0, r0);
+	init(B, 0, c.first_traj, st0, t0, r0, true);
 	long long next_id = B;
 	int in_batch = B;
 	dbuf *cs = &st0, *ct = &t0, *cr = &r0, *ns = &st1, *nt = &t1, *nr = &r1;
@@ -1057,7 +1065,7 @@ void run_epochs(module& m, const run_config& c, stats_state& st, long long n, cu
 		// partition CONTINUE trajectories to the front of the other buffer set
 		unsigned* kept_dev = scratch.as<unsigned>();
 		partition(m, s, in_batch, stride, stp, ls, lt, rr, ns->as<unsigned>(), nt->as<float>(), nr->p,
-				  scratch.as<char>() + 256, kept_dev);
+				  scratch.as<char>() + 256, kept_dev, c.refill_reuse_rng);
 		unsigned kept = 0;
 		MB_CUDA(cudaMemcpyAsync(&kept, kept_dev, sizeof kept, cudaMemcpyDeviceToHost, s));
 		MB_CUDA(cudaStreamSynchronize(s));
@@ -1067,7 +1075,7 @@ void run_epochs(module& m, const run_config& c, stats_state& st, long long n, cu
 		const int add = (int)std::max(0LL, std::min<long long>(B - (long long)kept, n - next_id));
 		if (add > 0)
 		{
-			init(add, (int)kept, c.first_traj + next_id, *cs, *ct, *cr);
+			init(add, (int)kept, c.first_traj + next_id, *cs, *ct, *cr, !c.refill_reuse_rng);
 			next_id += add;
 		}
 		in_batch = (int)kept + add;
@@ -1200,7 +1208,7 @@ bool same_run(const run_config& a, const run_config& b)
 		   a.istate == b.istate && a.noninternal_nodes == b.noninternal_nodes && a.traj_len == b.traj_len &&
 		   a.batch_limit == b.batch_limit && a.block == b.block && a.blocks_per_sm == b.blocks_per_sm &&
 		   a.fixed_capacity_log2 == b.fixed_capacity_log2 && a.stats_trajectories == b.stats_trajectories &&
-		   a.bin_capacity_log2 == b.bin_capacity_log2;
+		   a.bin_capacity_log2 == b.bin_capacity_log2 && a.refill_reuse_rng == b.refill_reuse_rng;
 }
 
 std::unique_ptr<result> run(module& m, const run_config& c)

@@ -140,11 +140,12 @@ void sort_bins(const mb_key128* keys, const long long* vals, unsigned n, mb_key1
 
 // Stable partition of the CONTINUE trajectories of an epoch batch into another buffer set
 // (last_states SoA [word * stride + i], last_times, random states); the number kept is written to
-// the device word *kept. `scratch` holds partition_scratch_bytes(n) bytes.
+// the device word *kept. `scratch` holds partition_scratch_bytes(n) bytes. With rejected_rands the
+// random states of the other trajectories fill out_rands[kept, n), last first.
 size_t partition_scratch_bytes(int n);
 void partition(module& m, cudaStream_t s, int n, int stride, const unsigned char* statuses, const unsigned* states,
 			   const float* times, const void* rands, unsigned* out_states, float* out_times, void* out_rands,
-			   void* scratch, unsigned* kept);
+			   void* scratch, unsigned* kept, bool rejected_rands = false);
 int occupancy_blocks(CUfunction f, int block, size_t smem);
 
 struct run_config
@@ -164,6 +165,7 @@ struct run_config
 	int fixed_capacity_log2 = 0;	 // 0 = automatic
 	long long stats_trajectories = 0; // trajectory count the fixed-point scales are chosen for (0 = sample_count)
 	int bin_capacity_log2 = 0;		  // sparse bins (more than 20 non-internal nodes): table size, 0 = automatic
+	bool refill_reuse_rng = false;	  // epoch modes: refilled slots continue the finished trajectories' random states
 };
 
 run_config config_from_layout(const model_layout& L, int mode);

@@ -26,6 +26,7 @@ class RunConfig(C.Structure):
         ("fixed_capacity_log2", C.c_int),
         ("stats_trajectories", C.c_longlong),
         ("bin_capacity_log2", C.c_int),
+        ("refill_reuse_rng", C.c_int),
     ]
 
 
@@ -191,7 +192,7 @@ class Module:
     def config(self, mode: str = "exact", sample_count: int | None = None, seed: int | None = None,
                first_traj: int = 0, traj_len: int = 100, batch_limit: int = 1_000_000, block: int = 256,
                blocks_per_sm: int = 0, fixed_capacity_log2: int = 0, stats_trajectories: int = 0,
-               bin_capacity_log2: int = 0) -> RunConfig:
+               bin_capacity_log2: int = 0, refill_reuse_rng: bool = False) -> RunConfig:
         cfg = RunConfig()
         check(lib().mb_run_config_default(self.model._h, C.byref(cfg)))
         cfg.mode = MODES[mode]
@@ -207,6 +208,7 @@ class Module:
         cfg.fixed_capacity_log2 = fixed_capacity_log2
         cfg.stats_trajectories = stats_trajectories
         cfg.bin_capacity_log2 = bin_capacity_log2
+        cfg.refill_reuse_rng = 1 if refill_reuse_rng else 0
         return cfg
 
     def autotune(self, mode: str = "fast", sample_count: int | None = None, **kw) -> dict:

@@ -96,3 +96,38 @@ def test_csv_files_equal_reference_build(gpu, tmp_path):
         assert len(fa) == len(fb)
         assert fa[0] == fb[0] and fa[2:] == fb[2:], (la, lb)
         assert abs(float(fa[1]) - float(fb[1])) <= 2e-4 * abs(float(fa[1])) + 1e-6, (fa[1], fb[1])
+
+
+@pytest.mark.parametrize("name", ["c1", "cellcycle"])
+def test_refill_beyond_one_batch_equals_reference_build(gpu, name, tmp_path):
+    """More trajectories than one batch (1.1e6 > 1e6): the reference refills the slots freed in an
+    epoch with new trajectories that continue the random states the finished ones left there, in
+    the order thrust::partition leaves them (simulation_runner.cu:126-153; quirk Q2). Epoch mode
+    with refill_reuse_rng does the same: transitions, final states, fixed points and (cellcycle,
+    discrete time) window counts identical to the reference build."""
+    if name == "c1":
+        bnd_path, cfg_path = str(tmp_path / "m.bnd"), str(tmp_path / "m.cfg")
+        bnd, cfg = synth.c1()
+        (tmp_path / "m.bnd").write_text(bnd)
+        (tmp_path / "m.cfg").write_text(cfg)
+    else:
+        bnd_path, cfg_path = model_files(name)
+    n = 1_100_000
+    ref = reference.run(bnd_path, cfg_path, samples=n)["result"]
+    model = mb.Model.from_files(bnd_path, cfg_path)
+    mod = gpu.compile(model)
+    res = mod.run(mode="epoch", sample_count=n, refill_reuse_rng=True)
+    assert res.transitions == ref["transitions"]
+    assert np.array_equal(res.final_counts.astype(np.int64), ref["final"].astype(np.int64))
+    fx = res.fixed
+    assert len(fx) == len(ref["fixed_counts"])
+    for (st, c), st2, c2 in zip(fx, ref["fixed_states"], ref["fixed_counts"]):
+        assert np.array_equal(st, st2) and c == c2
+    if ref["discrete"]:
+        assert np.array_equal(res.raw()["cnt"].astype(np.int64), ref["window"].astype(np.int64))
+    else:
+        p, q = res.window_probs, ref["probs"]
+        assert np.all(np.abs(p - q) <= P_ABS + P_REL * q), float(np.abs(p - q).max())
+    # fresh streams for the refills (the default) give other trajectories
+    other = mod.run(mode="epoch", sample_count=n)
+    assert other.transitions != res.transitions or not np.array_equal(other.final_counts, res.final_counts)
