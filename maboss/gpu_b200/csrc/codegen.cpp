@@ -305,6 +305,31 @@ void emit_incremental_tables(std::ostream& ss, const model_layout& L)
 	emit_array(ss, "float", "mbg_inc_ni_ul", f_ul);
 	emit_array(ss, "float", "mbg_inc_ni_dl", f_dl);
 	emit_array(ss, "int", "mbg_inc_ni_node", L.noninternal_nodes);
+	// The fast kernels' entropy sums (sum of the unstable non-internal nodes' rates and of their
+	// r log2 r, in non-internal order) straight-line: node words, bit masks and rates are constants,
+	// and each state word is read once. Same operations in the same order as the loop over the
+	// tables above (mbg_inc_ni_*).
+	ss << "template <class V>" << std::endl;
+	ss << "__device__ __forceinline__ void mbg_ni_rate_sums(const V& v, float& t, float& tl)" << std::endl;
+	ss << "{" << std::endl;
+	int cur_word = -1;
+	for (size_t k = 0; k < L.noninternal_nodes.size(); k++)
+	{
+		const int i = L.noninternal_nodes[k];
+		if (i / 32 != cur_word)
+		{
+			cur_word = i / 32;
+			ss << "    {" << std::endl;
+			ss << "        const uint32_t s = v.S(" << cur_word << "), u = v.U(" << cur_word << ");" << std::endl;
+		}
+		const unsigned bit = 1u << (i % 32);
+		ss << "        if (u & " << bit << "u) { const bool on = (s & " << bit << "u) != 0u; t += on ? " << f_down[k]
+		   << " : " << f_up[k] << "; tl += on ? " << f_dl[k] << " : " << f_ul[k] << "; }" << std::endl;
+		const bool last_in_word = k + 1 == L.noninternal_nodes.size() || L.noninternal_nodes[k + 1] / 32 != cur_word;
+		if (last_in_word)
+			ss << "    }" << std::endl;
+	}
+	ss << "}" << std::endl;
 }
 
 // forward-mode derivative of the float evaluation (expressions.cpp evaluate) w.r.t. one variable

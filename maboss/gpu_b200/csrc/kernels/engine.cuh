@@ -316,18 +316,9 @@ __device__ __forceinline__ void mb_group_add(unsigned long long (&gs)[MB_GROUPS]
 // entropy of the non-internal rates, h = log2(S) - sum(r log2 r) / S
 __device__ __forceinline__ float mb_incr_entropy(const mb_incr_view& v)
 {
+	// the sums over the non-internal nodes in their order, straight-line (generated code)
 	float t = 0.f, tl = 0.f;
-	for (int k = 0; k < mbg_noninternal_count; k++)
-	{
-		const int i = __ldg(mbg_inc_ni_node + k);
-		const uint32_t bit = 1u << (i & 31);
-		if (v.U(i >> 5) & bit)
-		{
-			const bool up = (v.S(i >> 5) & bit) != 0;
-			t += up ? __ldg(mbg_inc_ni_down + k) : __ldg(mbg_inc_ni_up + k);
-			tl += up ? __ldg(mbg_inc_ni_dl + k) : __ldg(mbg_inc_ni_ul + k);
-		}
-	}
+	mbg_ni_rate_sums(v, t, tl);
 	if (!(t > 0.f))
 		return 0.f;
 	const float h = log2f(t) - tl / t;

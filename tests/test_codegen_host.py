@@ -84,6 +84,26 @@ extern "C" int host_record_ni(int r) { return (int)((mbg_inc_crec[r].x >> 21) & 
 extern "C" int host_self(int i) { return mbg_inc_self[i]; }
 extern "C" int host_dep_first(int j) { return (int)mbg_inc_dep[2 * j]; }
 extern "C" int host_dep_count(int j) { return (int)(mbg_inc_dep[2 * j + 1] & 0xffffu); }
+struct host_view { const uint32_t *s, *u; uint32_t S(int w) const { return s[w]; } uint32_t U(int w) const { return u[w]; } };
+// the generated straight-line entropy sums, and the same sums by the loop over the tables
+extern "C" void host_ni_sums(const uint32_t* s, const uint32_t* u, float* out)
+{
+    float t = 0.f, tl = 0.f;
+    mbg_ni_rate_sums(host_view{ s, u }, t, tl);
+    float t2 = 0.f, tl2 = 0.f;
+    for (int k = 0; k < mbg_noninternal_count; k++)
+    {
+        const int i = mbg_inc_ni_node[k];
+        const uint32_t bit = 1u << (i & 31);
+        if (u[i >> 5] & bit)
+        {
+            const bool up = (s[i >> 5] & bit) != 0;
+            t2 += up ? mbg_inc_ni_down[k] : mbg_inc_ni_up[k];
+            tl2 += up ? mbg_inc_ni_dl[k] : mbg_inc_ni_ul[k];
+        }
+    }
+    out[0] = t; out[1] = tl; out[2] = t2; out[3] = tl2;
+}
 extern "C" int host_dep_ni(int j) { return (int)(mbg_inc_dep[2 * j + 1] >> 16) - 1; }
 #else
 extern "C" int host_has_tables() { return 0; }
@@ -114,7 +134,8 @@ def _compile(code: str, tmp_path, tag: str) -> C.CDLL:
                                 ("host_record_inputs", C.c_int, [C.c_int]),
                                 ("host_record_input", C.c_int, [C.c_int, C.c_int]),
                                 ("host_self", C.c_int, [C.c_int]), ("host_dep_first", C.c_int, [C.c_int]),
-                                ("host_dep_count", C.c_int, [C.c_int]), ("host_dep_ni", C.c_int, [C.c_int])]:
+                                ("host_dep_count", C.c_int, [C.c_int]), ("host_dep_ni", C.c_int, [C.c_int]),
+                                ("host_ni_sums", None, [C.c_void_p, C.c_void_p, C.c_void_p])]:
             getattr(L, name).restype = res
             getattr(L, name).argtypes = args
     return L
@@ -210,6 +231,11 @@ def _check_model(bnd, cfg, tmp_path, tag, n_states=200, n_flip_states=20):
                     L.host_rates(_ptr(r2, C.c_float), _ptr(st2, C.c_uint32))
                     changed = set(np.nonzero(r2 != rates)[0].tolist())
                     assert changed <= deps[j], (tag, j, changed - deps[j])
+            # the straight-line entropy sums equal the table loop bit for bit (random unstable masks)
+            un = _random_state(rng, N, W)
+            sums = np.zeros(4, np.float32)
+            L.host_ni_sums(st.ctypes.data, un.ctypes.data, sums.ctypes.data)
+            assert sums[0] == sums[2] and sums[1] == sums[3], (tag, sums)
     return tables
 
 
