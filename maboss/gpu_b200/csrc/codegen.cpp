@@ -330,6 +330,31 @@ void emit_incremental_tables(std::ostream& ss, const model_layout& L)
 			ss << "    }" << std::endl;
 	}
 	ss << "}" << std::endl;
+	// the same sums with the rates of a parameter variant (batched kernels compiled for this
+	// network): rate[2 i + on], rlog[2 i + on]
+	ss << "template <class V>" << std::endl;
+	ss << "__device__ __forceinline__ void mbg_ni_rate_sums_var(const V& v, const float* rate, const float* rlog, "
+		  "float& t, float& tl)"
+	   << std::endl;
+	ss << "{" << std::endl;
+	cur_word = -1;
+	for (size_t k = 0; k < L.noninternal_nodes.size(); k++)
+	{
+		const int i = L.noninternal_nodes[k];
+		if (i / 32 != cur_word)
+		{
+			cur_word = i / 32;
+			ss << "    {" << std::endl;
+			ss << "        const uint32_t s = v.S(" << cur_word << "), u = v.U(" << cur_word << ");" << std::endl;
+		}
+		const unsigned bit = 1u << (i % 32);
+		ss << "        if (u & " << bit << "u) { const int e = " << 2 * i << " + ((s & " << bit
+		   << "u) != 0u ? 1 : 0); t += __ldg(rate + e); tl += __ldg(rlog + e); }" << std::endl;
+		const bool last_in_word = k + 1 == L.noninternal_nodes.size() || L.noninternal_nodes[k + 1] / 32 != cur_word;
+		if (last_in_word)
+			ss << "    }" << std::endl;
+	}
+	ss << "}" << std::endl;
 }
 
 // forward-mode derivative of the float evaluation (expressions.cpp evaluate) w.r.t. one variable

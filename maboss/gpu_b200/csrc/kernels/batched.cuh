@@ -89,6 +89,22 @@ struct mbb_net_rt
 	__device__ __forceinline__ const unsigned* tt() const { return n.tt; }
 	__device__ __forceinline__ const int* self() const { return n.self; }
 	__device__ __forceinline__ const int* ni_node() const { return n.ni_node; }
+	// rate sums of the unstable non-internal nodes, in their order
+	template <class V>
+	__device__ __forceinline__ void ni_rate_sums(const V& v, const mb_variant& var, float& t, float& tl) const
+	{
+		for (int kk = 0; kk < n.k; kk++)
+		{
+			const int i = __ldg(n.ni_node + kk);
+			const uint32_t bit = 1u << (i & 31);
+			if (v.U(i >> 5) & bit)
+			{
+				const int e = 2 * i + ((v.S(i >> 5) & bit) ? 1 : 0);
+				t += __ldg(var.rate + e);
+				tl += __ldg(var.rlog + e);
+			}
+		}
+	}
 };
 
 // register group sums; words per group = ceil(W / 8). Measured on C5 (256 variants, 1 to 16 words):
@@ -161,17 +177,7 @@ template <class NET>
 __device__ __forceinline__ float mbb_entropy(const NET& net, const mb_variant& var, const mbb_lane& v)
 {
 	float t = 0.f, tl = 0.f;
-	for (int k = 0; k < net.k(); k++)
-	{
-		const int i = __ldg(net.ni_node() + k);
-		const uint32_t bit = 1u << (i & 31);
-		if (v.U(i >> 5) & bit)
-		{
-			const int e = 2 * i + ((v.S(i >> 5) & bit) ? 1 : 0);
-			t += __ldg(var.rate + e);
-			tl += __ldg(var.rlog + e);
-		}
-	}
+	net.ni_rate_sums(v, var, t, tl);
 	if (!(t > 0.f))
 		return 0.f;
 	const float h = log2f(t) - tl / t;
@@ -656,6 +662,12 @@ struct mbb_net_static
 	__device__ __forceinline__ static const unsigned* tt() { return mbg_inc_tt; }
 	__device__ __forceinline__ static const int* self() { return mbg_inc_self; }
 	__device__ __forceinline__ static const int* ni_node() { return mbg_inc_ni_node; }
+	// the same sums straight-line (generated code: constant node words and masks)
+	template <class V>
+	__device__ __forceinline__ static void ni_rate_sums(const V& v, const mb_variant& var, float& t, float& tl)
+	{
+		mbg_ni_rate_sums_var(v, var.rate, var.rlog, t, tl);
+	}
 };
 extern "C" __global__ void __launch_bounds__(128, 5) mb_batched_fast_static(mb_batch_params B)
 {
