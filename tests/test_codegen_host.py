@@ -37,6 +37,7 @@ PRELUDE = r"""
 #define __constant__
 struct uint2 { unsigned x, y; };
 struct uint4 { unsigned x, y, z, w; };
+template <class T> T __ldg(const T* p) { return *p; }
 """
 
 WRAPPER = r"""
