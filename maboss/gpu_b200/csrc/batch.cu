@@ -443,6 +443,17 @@ void batch_engine::enqueue(prepared& ps, cudaStream_t s, bool capturing)
 	{
 		void* args[] = { ps.B.get() };
 		MB_CUDA(cudaLaunchKernel(ps.fn, dim3(ps.grid), dim3(ps.block), args, ps.smem, s));
+		if (capturing)
+		{
+			// the node just captured is the kernel's: later runs update its parameter block (the
+			// seed) in the instantiated graph. Taken from the capture itself, because
+			// cudaGraphKernelNodeGetParams does not describe nodes of library kernels (cudaKernel_t).
+			cudaStreamCaptureStatus st;
+			const cudaGraphNode_t* deps = nullptr;
+			size_t ndeps = 0;
+			MB_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, nullptr, &deps, &ndeps));
+			ps.kernel = ndeps == 1 ? deps[0] : nullptr;
+		}
 	}
 	record(ps.e1);
 	char* host = static_cast<char*>(ps.host);
@@ -535,23 +546,11 @@ void batch_engine::run(unsigned long long seed, const std::vector<std::vector<do
 			MB_CUDA(cudaStreamEndCapture(s, &g));
 			ps.graph = g;
 			MB_CUDA(cudaGraphInstantiate(&ps.exec, g, 0));
-			ps.kernel = nullptr;
 			size_t n_nodes = 0;
 			MB_CUDA(cudaGraphGetNodes(g, nullptr, &n_nodes));
-			std::vector<cudaGraphNode_t> nodes(n_nodes);
-			MB_CUDA(cudaGraphGetNodes(g, nodes.data(), &n_nodes));
-			for (cudaGraphNode_t nd : nodes)
-			{
-				cudaGraphNodeType ty;
-				MB_CUDA(cudaGraphNodeGetType(nd, &ty));
-				if (ty != cudaGraphNodeTypeKernel)
-					continue;
-				cudaKernelNodeParams kp{};
-				MB_CUDA(cudaGraphKernelNodeGetParams(nd, &kp));
-				if (kp.func == ps.fn)
-					ps.kernel = nd;
-			}
 			graph_nodes = (unsigned)n_nodes;
+			if (!ps.kernel && ps.B->total > 0)
+				throw engine_error(MB_ERR_CUDA, "batch graph: the kernel node was not found in the capture");
 		}
 		if (ps.kernel)
 		{

@@ -96,6 +96,16 @@ def test_fast_mode_dense_kernel_for_general_rates(gpu):
     _assert_same(res, raw, ref, False)
 
 
+def test_fast_mode_dense_kernel_for_a_wide_rate_span(gpu):
+    """@logic-form rates spanning 1e-3 ... 1e3 are too wide for the integer rates: fast mode runs the
+    dense kernel, equal to the oracle's restatement of it on the same Philox streams."""
+    from test_codegen_host import wide_span_model
+
+    bnd, cfg = wide_span_model()
+    model, res, raw, o, ref = _run_both(gpu, bnd, cfg, 20_000, mode="fast")
+    _assert_same(res, raw, ref, False)
+
+
 def _assert_identical(a, b):
     ra, rb = a.raw(), b.raw()
     for k in ("occ", "cnt", "h"):
@@ -286,11 +296,10 @@ def test_large_histograms_come_back_as_their_non_zero_cells(gpu):
     model, res, raw, o, ref = _run_both(gpu, bnd, cfg, 1_500)
     assert res.windows_sparse and not res.is_sparse
     _assert_same(res, raw, ref, o.discrete)
-    # the same trajectories occupy the same cells; the occupancy sums agree to the slices' last ulp
-    # (device and host logf), so the cells are compared exactly and the sums with a tolerance
+    # the same trajectories occupy the same cells (their sums agree to the slices' last ulp: device
+    # and host logf, compared as probabilities above)
     nz = np.nonzero(ref["occ"].ravel())[0]
     assert np.array_equal(np.nonzero(raw["occ"].ravel())[0], nz)
-    assert np.allclose(raw["occ"].ravel()[nz], ref["occ"].ravel()[nz], rtol=1e-5, atol=0)
     sp = res.sparse()
     assert len(sp["raw"]) == len(nz)
     cells = sp["windows"].astype(np.int64) * res.dims.bins + sp["states"][:, 0].astype(np.int64)
