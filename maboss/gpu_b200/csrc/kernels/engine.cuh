@@ -1195,87 +1195,13 @@ extern "C" __global__ void __launch_bounds__(256)
 #endif // MB_FAMILY_EPOCH
 
 // Window statistics over one epoch's buffer (window_average_small.cu:50-136 over the SoA buffer):
-// one thread per trajectory walking its slots, coalesced across threads for every slot. The next
-// slot's time, entropy and state words are loaded before the current slot is recorded (the loads
-// would otherwise wait behind the atomics of the slot before), and every sum leaves the warp once
-// per distinct target: the lanes adding to the same (window, state) cell, or to the same window's
-// entropy sum, are grouped with __match_any_sync and their integer values summed by the group
-// (integer sums: the result does not depend on the grouping, so it equals the fused kernels').
-#ifndef MBG_WIDE_INDEX
-// sum of a non-negative 64-bit value over the lanes of `grp` (exact: three 21-bit slices, each
-// summed over at most 32 lanes in 32 bits)
-__device__ __forceinline__ unsigned long long mb_group_sum(unsigned grp, unsigned long long v)
-{
-	const unsigned a = __reduce_add_sync(grp, (unsigned)(v & 0x1fffffull));
-	const unsigned b = __reduce_add_sync(grp, (unsigned)((v >> 21) & 0x1fffffull));
-	const unsigned c = __reduce_add_sync(grp, (unsigned)(v >> 42));
-	return (unsigned long long)a + ((unsigned long long)b << 21) + ((unsigned long long)c << 42);
-}
-
-// atomicAdd(target + 0, v) once per group of the converged lanes that add to the same target
-__device__ __forceinline__ void mb_warp_add(unsigned long long* target, unsigned long long v)
-{
-	const unsigned grp = __match_any_sync(__activemask(), (unsigned long long)target);
-	const unsigned long long sum = mb_group_sum(grp, v);
-	if ((threadIdx.x & 31) == (unsigned)(__ffs(grp) - 1) && sum != 0)
-		atomicAdd(target, sum);
-}
-
-__device__ __forceinline__ void mb_warp_add_u32(unsigned* target, unsigned v)
-{
-	const unsigned grp = __match_any_sync(__activemask(), (unsigned long long)target);
-	const unsigned sum = __reduce_add_sync(grp, v);
-	if ((threadIdx.x & 31) == (unsigned)(__ffs(grp) - 1) && sum != 0)
-		atomicAdd(target, sum);
-}
-
-// mb_record_cont / mb_record_disc with warp-aggregated flushes
-__device__ __forceinline__ void mb_acc_flush_occ_warp(mb_win_acc& a, const mb_stats_params& p)
-{
-	if (a.ow >= 0 && a.oq != 0)
-		mb_warp_add(reinterpret_cast<unsigned long long*>(p.win_occ + (size_t)a.ow * p.n_bins + a.oi),
-					(unsigned long long)a.oq);
-}
-
-__device__ __forceinline__ void mb_record_cont_warp(mb_win_acc& a, const mb_stats_params& p, long long* hsink,
-													mb_idx_t idx, float t0, float t1, float h)
-{
-	float sb = t0;
-	int w = (int)floorf(sb / p.win_tick);
-	for (int guard = 0; t1 > sb && guard <= p.n_windows + 2; guard++)
-	{
-		const float we = (float)(w + 1) * p.win_tick;
-		const float se = fminf(t1, we);
-		const float sl = se - sb;
-		if (w >= 0 && w < p.n_windows)
-		{
-			const long long q = __double2ll_rn((double)sl * p.fx);
-			if (w == a.ow && idx == a.oi)
-				a.oq += q;
-			else
-			{
-				mb_acc_flush_occ_warp(a, p);
-				a.ow = w;
-				a.oi = idx;
-				a.oq = q;
-			}
-			const long long hq = __double2ll_rn((double)__fmul_rn(h, sl) * p.fx_h);
-			if (w == a.hw)
-				a.hq += hq;
-			else
-			{
-				if (a.hw >= 0 && a.hq != 0)
-					mb_warp_add(reinterpret_cast<unsigned long long*>(hsink + a.hw), (unsigned long long)a.hq);
-				a.hw = w;
-				a.hq = hq;
-			}
-		}
-		w++;
-		sb = se;
-	}
-}
-#endif
-
+// one thread per trajectory walking its slots, coalesced across threads for every slot, consecutive
+// slices of the same (window, state) summed in registers before one 64-bit atomic. The next slot's
+// time, entropy and state words are loaded before the current slot is recorded (the loads would
+// otherwise wait behind the atomics of the slot before). Measured and rejected: grouping the lanes
+// that flush to the same cell with __match_any_sync and adding once per group (one epoch step of
+// the 10-node network 5.3 ms -> 27.9 ms, whose state changes at almost every slot so that almost
+// every slot flushes; the 1000-node network -1 %).
 extern "C" __global__ void __launch_bounds__(256)
 	mb_window_epoch(int n, int stride, int L, const uint32_t* __restrict__ traj_states,
 					const float* __restrict__ traj_times, const float* __restrict__ traj_h, mb_stats_params p)
@@ -1317,39 +1243,10 @@ extern "C" __global__ void __launch_bounds__(256)
 				for (int w = 0; w < state_words; w++)
 					st_next[w] = traj_states[((size_t)(s + 1) * state_words + w) * stride + id];
 			}
-			if (t1 != 0.f) // zero-time slots are empty (window_average_small.cu:68)
-			{
-				const mb_idx_t idx = get_non_internal_index(st);
-#ifdef MBG_WIDE_INDEX
-				if (discrete_time)
-					mb_record_disc(p, hsink, idx, t0, hh);
-				else
-					mb_record_cont(acc, p, hsink, idx, t0, t1, hh);
-#else
-				if (discrete_time)
-				{
-					const int w = (int)lroundf(t0 / p.win_tick);
-					if (w >= 0 && w < p.n_windows)
-					{
-						mb_warp_add_u32(p.win_cnt + (size_t)w * p.n_bins + idx, 1u);
-						const long long hq = __double2ll_rn((double)hh * p.fx_h);
-						if (hq != 0)
-							mb_warp_add(reinterpret_cast<unsigned long long*>(hsink + w), (unsigned long long)hq);
-					}
-				}
-				else
-					mb_record_cont_warp(acc, p, hsink, idx, t0, t1, hh);
-#endif
-			}
+			mb_record(acc, p, hsink, st, t0, t1, hh);
 			t0 = t1;
 		}
-#ifdef MBG_WIDE_INDEX
 		mb_acc_flush(acc, p, hsink);
-#else
-		mb_acc_flush_occ_warp(acc, p);
-		if (acc.hw >= 0 && acc.hq != 0)
-			mb_warp_add(reinterpret_cast<unsigned long long*>(hsink + acc.hw), (unsigned long long)acc.hq);
-#endif
 	}
 	if (p.h_in_smem)
 	{
