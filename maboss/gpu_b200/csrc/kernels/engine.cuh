@@ -907,17 +907,28 @@ extern "C" __global__ void __launch_bounds__(128, 5) mb_fused_fast(mb_fused_para
 				uint32_t um = v.U(word);
 				int j = 32 * word + 31 - __clz(um | 1u);
 				const uint2* q2 = reinterpret_cast<const uint2*>(mbg_inc_q);
+				// the chosen word's unstable nodes two at a time: both rate loads are issued before
+				// the first comparison (+1.9 % on the 1000-node network over one load per step)
 				while (um)
 				{
-					const int b = __ffs(um) - 1;
-					const int i = 32 * word + b;
-					const uint2 qq = __ldg(q2 + i);
-					const uint32_t q = ((sw >> b) & 1u) ? qq.y : qq.x;
-					j = i;
-					if (r < cum + q)
+					const int b0 = __ffs(um) - 1;
+					const uint32_t um1 = um & (um - 1u);
+					const int b1 = um1 ? __ffs(um1) - 1 : b0;
+					const uint2 qq0 = __ldg(q2 + 32 * word + b0);
+					const uint2 qq1 = __ldg(q2 + 32 * word + b1);
+					const uint32_t qa = ((sw >> b0) & 1u) ? qq0.y : qq0.x;
+					j = 32 * word + b0;
+					if (r < cum + qa)
 						break;
-					cum += q;
-					um &= um - 1u;
+					cum += qa;
+					if (!um1)
+						break;
+					const uint32_t qb = ((sw >> b1) & 1u) ? qq1.y : qq1.x;
+					j = 32 * word + b1;
+					if (r < cum + qb)
+						break;
+					cum += qb;
+					um = um1 & (um1 - 1u);
 				}
 				const uint2 nj = __ldg(reinterpret_cast<const uint2*>(mbg_inc_dep) + j);
 
