@@ -346,6 +346,14 @@ mb_status mb_batch_tuning(mb_batch b, int i, int* gradient, int* block, int* blo
 mb_status mb_batch_add_variant_grad(mb_batch b, int net, const char* const* names, const float* values,
                                     int n_values, long long n_traj, unsigned long long first_traj,
                                     const char* const* grad_params, int n_grad, int* variant);
+/* Mutant analysis (a TODO of the reference, README.md "Next steps"; no counterpart in its code): a
+ * variant of network `net` in which each listed node is forced on (on[i] != 0) or off: its initial
+ * state is 1 or 0 and both of its rates are 0, so it never changes; the other nodes evolve as in the
+ * model (with the given $variable values). All single-node mutants of a network run in one launch.
+ * Equal, bit for bit, to MB_MODE_FUSED_FAST of the model with those nodes' rates and istate edited. */
+mb_status mb_batch_add_mutant(mb_batch b, int net, const char* const* names, const float* values, int n_values,
+                              long long n_traj, unsigned long long first_traj, const char* const* nodes,
+                              const int* on, int n_mutants, int* variant);
 mb_status mb_batch_set_variables(mb_batch b, int v, const char* const* names, const float* values, int n_values);
 mb_status mb_batch_run_gradient(mb_batch b, unsigned long long seed, const double* const* cotangents,
                                 int n_cotangents, float* kernel_ms);

@@ -6,7 +6,7 @@ entry point raises.
 """
 from ._lib import EngineError, build, lib
 from .engine import (Batch, Context, Model, Module, Result, RunConfig, Stats, gradient, merge_results,
-                     rand_state_size)
+                     mutant_sweep, rand_state_size)
 
 __all__ = ["EngineError", "build", "lib", "Batch", "Context", "Model", "Module", "Result", "RunConfig", "Stats",
-           "gradient", "merge_results", "rand_state_size"]
+           "gradient", "merge_results", "mutant_sweep", "rand_state_size"]

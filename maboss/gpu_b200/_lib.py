@@ -108,6 +108,8 @@ def _declare(L: C.CDLL) -> None:
         "mb_batch_result": (i32, [vp, i32, P(vp)]),
         "mb_batch_add_variant_grad": (i32, [vp, i32, P(C.c_char_p), P(f32), i32, i64, u64, P(C.c_char_p), i32,
                                             P(i32)]),
+        "mb_batch_add_mutant": (i32, [vp, i32, P(C.c_char_p), P(f32), i32, i64, u64, P(C.c_char_p), P(i32), i32,
+                                      P(i32)]),
         "mb_batch_set_variables": (i32, [vp, i32, P(C.c_char_p), P(f32), i32]),
         "mb_batch_run_gradient": (i32, [vp, u64, P(C.c_void_p), i32, P(f32)]),
         "mb_batch_gradient": (i32, [vp, i32, P(C.c_double), i32, P(i32)]),

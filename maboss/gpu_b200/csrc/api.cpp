@@ -832,6 +832,22 @@ mb_status mb_batch_add_variant_grad(mb_batch b, int net, const char* const* name
 	});
 }
 
+mb_status mb_batch_add_mutant(mb_batch b, int net, const char* const* names, const float* values, int n_values,
+							  long long n_traj, unsigned long long first_traj, const char* const* nodes,
+							  const int* on, int n_mutants, int* variant)
+{
+	return guard([&] {
+		need(b && variant && n_values >= 0 && n_mutants >= 0, "bad argument");
+		std::map<std::string, bool> mut;
+		for (int i = 0; i < n_mutants; i++)
+		{
+			need(nodes && nodes[i] && on, "null mutant node name or state");
+			mut[nodes[i]] = on[i] != 0;
+		}
+		*variant = b->b->add_variant(net, overrides_of(names, values, n_values), n_traj, first_traj, {}, mut);
+	});
+}
+
 mb_status mb_batch_set_variables(mb_batch b, int v, const char* const* names, const float* values, int n_values)
 {
 	return guard([&] {

@@ -99,7 +99,8 @@ int batch_engine::add_model(const model_t& m)
 }
 
 int batch_engine::add_variant(int net, const std::map<std::string, float>& overrides, long long n_traj,
-							  unsigned long long first_traj, const std::vector<std::string>& grad_params)
+							  unsigned long long first_traj, const std::vector<std::string>& grad_params,
+							  const std::map<std::string, bool>& mutants)
 {
 	if (net < 0 || net >= (int)nets.size())
 		throw engine_error(MB_ERR_INVALID, "bad network index");
@@ -115,6 +116,16 @@ int batch_engine::add_variant(int net, const std::map<std::string, float>& overr
 		if (!N.model.variables.count(kv.first))
 			throw engine_error(MB_ERR_INVALID, "unknown variable " + kv.first);
 	var->overrides = overrides;
+	for (auto& [name, on] : mutants)
+	{
+		const int i = N.model.node_index(name);
+		if (i < 0)
+			throw engine_error(MB_ERR_INVALID, "unknown node " + name);
+		var->mutants[i] = on;
+	}
+	var->istate = N.L.istate;
+	for (auto& [i, on] : var->mutants)
+		var->istate[i] = on ? 1.f : 0.f;
 	compute_rates(*var);
 	invalidate();
 	vars_.push_back(std::move(var));
@@ -140,6 +151,27 @@ void batch_engine::compute_rates(variant& V) const
 		for (auto& kv : V.overrides)
 			vars[kv.first] = kv.second;
 		V.rates = fast_rates(N.model, vars, V.grad_params);
+	}
+	if (!V.mutants.empty())
+	{
+		// a mutant node never changes (forced by its initial state): both rates 0, no derivatives
+		for (auto& [i, on] : V.mutants)
+			V.rates.up[i] = V.rates.down[i] = 0.f;
+		rate_set r = V.rates;
+		r.grad_ptr.assign(1, 0);
+		r.grad_p.clear();
+		r.grad_d.clear();
+		for (int e = 0; e < 2 * L.state_size; e++)
+		{
+			if (!V.mutants.count(e / 2))
+				for (int k = V.rates.grad_ptr[e]; k < V.rates.grad_ptr[e + 1]; k++)
+				{
+					r.grad_p.push_back(V.rates.grad_p[k]);
+					r.grad_d.push_back(V.rates.grad_d[k]);
+				}
+			r.grad_ptr.push_back((int)r.grad_p.size());
+		}
+		V.rates = std::move(r);
 	}
 	const incremental_tables t = build_incremental_tables(L, V.rates.up, V.rates.down);
 	if (!t.ok)
@@ -293,7 +325,7 @@ batch_engine::prepared& batch_engine::prepare(bool grad)
 			// created once: the other kind of run (forward / gradient) shares these buffers
 			V.st.init_plain(L.state_words, L.time_tick, L.max_time, L.discrete_time, L.noninternal_nodes, V.n_traj,
 							s);
-			upload(V.d_istate, L.istate, s);
+			upload(V.d_istate, V.istate, s);
 			V.d_counters.alloc(16);
 			V.d_grad.alloc(std::max<size_t>(1, V.grad_params.size()) * sizeof(double));
 			V.d_cot.alloc((size_t)L.windows() * ((size_t)1 << L.noninternal_nodes.size()) * sizeof(double));

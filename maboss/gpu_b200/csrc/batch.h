@@ -57,6 +57,8 @@ public:
 		unsigned long long first_traj = 0;
 		std::vector<std::string> grad_params;
 		std::map<std::string, float> overrides; // this variant's variable values (the rest: the model's)
+		std::map<int, bool> mutants; // node -> forced on (true) / off: initial state 1 / 0, both rates 0
+		std::vector<float> istate;   // initial-state probabilities (the model's, mutants forced)
 		rate_set rates;
 		int rate_shift = 0;
 		std::vector<unsigned> q;
@@ -72,7 +74,8 @@ public:
 	int add_model(const model_t& m);
 	// `overrides`: variable values of this variant; `grad_params`: variables to differentiate
 	int add_variant(int net, const std::map<std::string, float>& overrides, long long n_traj,
-					unsigned long long first_traj, const std::vector<std::string>& grad_params = {});
+					unsigned long long first_traj, const std::vector<std::string>& grad_params = {},
+					const std::map<std::string, bool>& mutants = {});
 	// new values of some of variant v's variables: its rate tables are recomputed and uploaded in
 	// place, so prepared runs, launch shapes and captured graphs stay valid
 	void set_variables(int v, const std::map<std::string, float>& values);

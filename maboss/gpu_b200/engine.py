@@ -319,12 +319,21 @@ class Batch:
         return n.value
 
     def add_variant(self, net: int, n_traj: int, params: dict[str, float] | None = None,
-                    first_traj: int = 0, grad_params: list[str] | None = None) -> int:
+                    first_traj: int = 0, grad_params: list[str] | None = None,
+                    mutants: dict[str, bool] | None = None) -> int:
         """A variant of network `net` (`params`: its $variable values); with `grad_params`, the
-        $variables whose gradient run_gradient computes for it."""
+        $variables whose gradient run_gradient computes for it; with `mutants` ({node: True for
+        forced on, False for forced off}), a mutant (mb_batch_add_mutant)."""
         names, values, k = _names_values(params)
         v = C.c_int()
-        if grad_params:
+        if mutants:
+            if grad_params:
+                raise ValueError("a mutant variant has no gradient parameters")
+            nodes = (C.c_char_p * len(mutants))(*[n.encode() for n in mutants])
+            on = (C.c_int * len(mutants))(*[1 if x else 0 for x in mutants.values()])
+            check(lib().mb_batch_add_mutant(self._h, net, names, values, k, n_traj, first_traj, nodes, on,
+                                            len(mutants), C.byref(v)))
+        elif grad_params:
             gp = (C.c_char_p * len(grad_params))(*[g.encode() for g in grad_params])
             check(lib().mb_batch_add_variant_grad(self._h, net, names, values, k, n_traj, first_traj, gp,
                                                   len(grad_params), C.byref(v)))
@@ -401,6 +410,21 @@ def gradient(ctx: Context, model: Model, params: dict[str, float], cotangent: np
     check(lib().mb_gradient(ctx._h, model._h, names, values, k, n_traj, seed, cot.ctypes.data, grad.ctypes.data,
                             C.byref(h)))
     return grad[:k], Result(h)
+
+
+def mutant_sweep(ctx: Context, model: Model, n_traj: int, nodes: list[str] | None = None, seed: int = 0,
+                 params: dict[str, float] | None = None) -> dict:
+    """Mutant analysis in one launch: the wild type and, for every listed node (default: all), the
+    node forced on and forced off (mb_batch_add_mutant). Returns {("wt",): Result,
+    (node, True): Result, (node, False): Result}."""
+    b = Batch(ctx)
+    net = b.add_model(model)
+    nodes = model.node_names if nodes is None else nodes
+    keys = [("wt",)] + [(n, on) for n in nodes for on in (True, False)]
+    ids = [b.add_variant(net, n_traj, params)] + [b.add_variant(net, n_traj, params, mutants={n: on})
+                                                  for n in nodes for on in (True, False)]
+    b.run(seed)
+    return {k: b.result(v) for k, v in zip(keys, ids)}
 
 
 def merge_results(results: list["Result"]) -> "Result":

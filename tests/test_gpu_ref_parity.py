@@ -126,8 +126,10 @@ def test_refill_beyond_one_batch_equals_reference_build(gpu, name, tmp_path):
     if ref["discrete"]:
         assert np.array_equal(res.raw()["cnt"].astype(np.int64), ref["window"].astype(np.int64))
     else:
+        # 1.1e6 trajectories put ~1e7 fp32 atomic adds into the reference's largest window bins:
+        # its rounding error grows to a few 1e-4 relative there (the engine sums in int64)
         p, q = res.window_probs, ref["probs"]
-        assert np.all(np.abs(p - q) <= P_ABS + P_REL * q), float(np.abs(p - q).max())
+        assert np.all(np.abs(p - q) <= P_ABS + 5 * P_REL * q), float(np.abs(p - q).max())
     # fresh streams for the refills (the default) give other trajectories
     other = mod.run(mode="epoch", sample_count=n)
     assert other.transitions != res.transitions or not np.array_equal(other.final_counts, res.final_counts)
