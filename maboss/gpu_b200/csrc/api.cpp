@@ -468,7 +468,7 @@ mb_status mb_launch_initialize_random(mb_module mod, void* stream, int n, unsign
 		if (!m.init_random)
 			m.ensure(mb::FAMILY_EPOCH);
 		void* a[] = { &n, &seed, &first, &rands };
-		mb::launch(m.init_random, (n + 255) / 256, 256, 0, stream_of(m.ctx, stream), a);
+		mb::launch(m.init_random, mb::init_random_blocks(n), 256, 0, stream_of(m.ctx, stream), a);
 	});
 }
 

@@ -166,11 +166,13 @@ __device__ __forceinline__ bool mbb_logic(const NET& net, const mbb_lane& v, int
 	return (ttw >> (p & 31)) & 1u;
 }
 
+// gs[i] is the rate sum of groups 0..i (inclusive prefix sums; groups past the network's last are
+// empty, so their prefixes equal the total); a change d in group g moves every prefix from g on
 __device__ __forceinline__ void mbb_group_add(unsigned long long (&gs)[MBB_GROUPS], int g, long long d)
 {
 #pragma unroll
 	for (int i = 0; i < MBB_GROUPS; i++)
-		gs[i] += (i == g) ? (unsigned long long)d : 0ull;
+		gs[i] += (i >= g) ? (unsigned long long)d : 0ull;
 }
 
 template <class NET>
@@ -521,18 +523,16 @@ __device__ void mbb_body(const mb_batch_params& B)
 			{
 				const unsigned long long r = __umul64hi(((unsigned long long)rb.y << 32) | rb.z, total);
 				const int wsh = net.wpg_shift(), wpg = 1 << wsh;
-				const int ng = (net.W() + wpg - 1) >> wsh; // groups of this network
+				// the first group whose prefix sum exceeds r: the number of prefixes <= r (r < total,
+				// and the prefixes of the groups past the network's last equal the total)
 				unsigned long long cum = 0;
 				int g = 0;
-				// the first group whose running sum exceeds r (the group sums add up to total, so
-				// the last group is reached only when it is that group)
 #pragma unroll
-				for (int i = 0; i < MBB_GROUPS; i++)
+				for (int i = 0; i < MBB_GROUPS - 1; i++)
 				{
-					g = i;
-					if (i + 1 >= ng || r < cum + gs[i])
-						break;
-					cum += gs[i];
+					const bool le = gs[i] <= r;
+					g += le ? 1 : 0;
+					cum = le ? gs[i] : cum;
 				}
 				int word = g * wpg;
 				for (int i = 0; i < wpg; i++)

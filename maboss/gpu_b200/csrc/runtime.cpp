@@ -900,7 +900,7 @@ unsigned launch_fused(module& m, const run_config& c, stats_state& st, long long
 		int cnt = (int)n;
 		unsigned long long seed = c.seed, first = c.first_traj;
 		void* a[] = { &cnt, &seed, &first, &rng };
-		launch(m.init_random, (unsigned)((n + 255) / 256), 256, 0, s, a);
+		launch(m.init_random, init_random_blocks(n), 256, 0, s, a);
 		P.rands = rng;
 		launches++;
 	}
@@ -1029,7 +1029,7 @@ void run_epochs(module& m, const run_config& c, stats_state& st, long long n, cu
 		void* a1[] = { &cnt, &seed, &first, &rptr };
 		if (fresh_rng)
 		{
-			launch(m.init_random, (cnt + 255) / 256, 256, 0, s, a1);
+			launch(m.init_random, init_random_blocks(cnt), 256, 0, s, a1);
 			launches++;
 		}
 		int stride = B;

@@ -29,6 +29,14 @@ struct engine_error : std::runtime_error
 void cuda_throw(cudaError_t e, const char* what);
 #define MB_CUDA(x) ::mb::cuda_throw((x), #x)
 
+// mb_initialize_random initialises this many consecutive trajectories per thread
+// (MB_INIT_RANDOM_PER_THREAD in kernels/engine.cuh); blocks of 256 threads for n trajectories
+constexpr int INIT_RANDOM_PER_THREAD = 8;
+inline unsigned init_random_blocks(long long n)
+{
+	return (unsigned)((n + 256LL * INIT_RANDOM_PER_THREAD - 1) / (256LL * INIT_RANDOM_PER_THREAD));
+}
+
 // Device memory owned by the runtime.
 struct dbuf
 {

@@ -185,11 +185,17 @@ def test_gradient_at_the_gradient_configuration(gpu):
     se_fd2 = fd2.std(axis=0, ddof=1) / 2.0
     resolved = se_fd < 0.02 * np.abs(m_fd)
     rel = diff / np.maximum(np.abs(m_fd), 1e-30)
+    # the same estimate against the ten times wider step, whose finite differences resolve more
+    m_fd2 = fd2.mean(axis=0)
+    resolved2 = se_fd2 < 0.02 * np.abs(m_fd2)
+    rel2 = np.abs(m_sf - m_fd2) / np.maximum(np.abs(m_fd2), 1e-30)
     print(f"\ngradient configuration: median |SF| {np.median(np.abs(m_sf)):.4g}, median SE(SF) "
           f"{np.median(se_sf):.3g}, median SE(FD) at h=1e-3 {np.median(se_fd):.3g}, at h=1e-2 "
           f"{np.median(se_fd2):.3g}; resolved at h=1e-3: {int(resolved.sum())} of 40; max relative deviation "
-          f"among them {rel[resolved].max() if resolved.any() else float('nan'):.4f}; max deviation in "
-          f"combined standard errors {np.max(diff / se):.2f}")
+          f"among them {rel[resolved].max() if resolved.any() else float('nan'):.4f}; resolved at h=1e-2: "
+          f"{int(resolved2.sum())} of 40, max relative deviation among them "
+          f"{rel2[resolved2].max() if resolved2.any() else float('nan'):.4f}; max deviation in "
+          f"combined standard errors {np.max(diff[se > 0] / se[se > 0]):.2f}")
     assert np.all(diff <= 4 * se + 0.02 * np.abs(m_fd)), (m_sf, m_fd, se)
 
 
@@ -438,7 +444,8 @@ def test_mutant_equals_the_edited_model(gpu, name, node, on):
         bins_with = np.array([(s >> k) & 1 for s in range(probs.shape[1])], bool)
         mass = probs[:, bins_with].sum(axis=1) if on else probs[:, ~bins_with].sum(axis=1)
         assert np.allclose(mass[probs.sum(axis=1) > 0], 1.0, atol=1e-6)
-    assert b.result(wt).transitions != got.transitions
+    rw = b.result(wt).raw()
+    assert not (np.array_equal(rw["occ"], ra["occ"]) and np.array_equal(rw["cnt"], ra["cnt"]))
 
 
 def test_mutant_sweep_runs_every_single_node_mutant(gpu):
