@@ -467,8 +467,9 @@ mb_status mb_launch_initialize_random(mb_module mod, void* stream, int n, unsign
 		MB_CUDA(cudaSetDevice(m.ctx->device));
 		if (!m.init_random)
 			m.ensure(mb::FAMILY_EPOCH);
-		void* a[] = { &n, &seed, &first, &rands };
-		mb::launch(m.init_random, mb::init_random_blocks(n), 256, 0, stream_of(m.ctx, stream), a);
+		int per = mb::init_random_per(n);
+		void* a[] = { &n, &seed, &first, &rands, &per };
+		mb::launch(m.init_random, mb::init_random_blocks(n, per), 256, 0, stream_of(m.ctx, stream), a);
 	});
 }
 

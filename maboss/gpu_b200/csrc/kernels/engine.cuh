@@ -1010,20 +1010,20 @@ extern "C" __global__ void __launch_bounds__(128, 5) mb_fused_fast(mb_fused_para
 #if defined(MB_FAMILY_EXACT) || defined(MB_FAMILY_EPOCH)
 // (kept out of the fast family: curand_init's XORWOW skip-ahead tables are megabytes of code)
 // The state of trajectory i is curand_init(seed, first + i, 0) (simulation.cu:23-32). A thread
-// initialises MB_INIT_RANDOM_PER_THREAD consecutive trajectories: curand_init for the first, then
-// one subsequence jump each (skipahead_sequence(1)), one matrix product instead of the one per
-// digit of the trajectory number that curand_init applies; the states are the same.
-#define MB_INIT_RANDOM_PER_THREAD 8
+// initialises `per` consecutive trajectories: curand_init for the first, then one subsequence jump
+// each (skipahead_sequence(1)), one matrix product instead of the one per digit of the trajectory
+// number that curand_init applies; the states are the same. The host takes per > 1 only when the
+// threads still fill the GPU (the initialisation is latency bound below that).
 extern "C" __global__ void mb_initialize_random(int n, unsigned long long seed, unsigned long long first,
-												 curandState* __restrict__ rands)
+												 curandState* __restrict__ rands, int per)
 {
-	const long long id0 = (long long)(blockIdx.x * blockDim.x + threadIdx.x) * MB_INIT_RANDOM_PER_THREAD;
+	const long long id0 = (long long)(blockIdx.x * blockDim.x + threadIdx.x) * per;
 	if (id0 >= n)
 		return;
 	curandState st;
 	curand_init(seed, first + (unsigned long long)id0, 0ull, &st);
 	rands[id0] = st;
-	for (int k = 1; k < MB_INIT_RANDOM_PER_THREAD && id0 + k < n; k++)
+	for (int k = 1; k < per && id0 + k < n; k++)
 	{
 		skipahead_sequence(1ull, &st);
 		rands[id0 + k] = st;

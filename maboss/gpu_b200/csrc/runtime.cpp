@@ -897,10 +897,10 @@ unsigned launch_fused(module& m, const run_config& c, stats_state& st, long long
 	unsigned launches = 0;
 	if (c.mode == MB_MODE_FUSED_EXACT && rng)
 	{
-		int cnt = (int)n;
+		int cnt = (int)n, per = init_random_per(n);
 		unsigned long long seed = c.seed, first = c.first_traj;
-		void* a[] = { &cnt, &seed, &first, &rng };
-		launch(m.init_random, init_random_blocks(n), 256, 0, s, a);
+		void* a[] = { &cnt, &seed, &first, &rng, &per };
+		launch(m.init_random, init_random_blocks(n, per), 256, 0, s, a);
 		P.rands = rng;
 		launches++;
 	}
@@ -1026,10 +1026,11 @@ void run_epochs(module& m, const run_config& c, stats_state& st, long long n, cu
 					bool fresh_rng) {
 		unsigned long long seed = c.seed;
 		void* rptr = rbuf.as<char>() + (size_t)offset * sizeof(curandState);
-		void* a1[] = { &cnt, &seed, &first, &rptr };
+		int per = init_random_per(cnt);
+		void* a1[] = { &cnt, &seed, &first, &rptr, &per };
 		if (fresh_rng)
 		{
-			launch(m.init_random, init_random_blocks(cnt), 256, 0, s, a1);
+			launch(m.init_random, init_random_blocks(cnt, per), 256, 0, s, a1);
 			launches++;
 		}
 		int stride = B;

@@ -29,12 +29,18 @@ struct engine_error : std::runtime_error
 void cuda_throw(cudaError_t e, const char* what);
 #define MB_CUDA(x) ::mb::cuda_throw((x), #x)
 
-// mb_initialize_random initialises this many consecutive trajectories per thread
-// (MB_INIT_RANDOM_PER_THREAD in kernels/engine.cuh); blocks of 256 threads for n trajectories
-constexpr int INIT_RANDOM_PER_THREAD = 8;
-inline unsigned init_random_blocks(long long n)
+// mb_initialize_random: trajectories initialised per thread (consecutive ones, by subsequence jumps)
+// and the grid of 256-thread blocks for n trajectories. Up to 8 per thread, as long as the threads
+// still number 148 SMs x 512; below that the initialisation is latency bound and each thread takes
+// one.
+inline int init_random_per(long long n)
 {
-	return (unsigned)((n + 256LL * INIT_RANDOM_PER_THREAD - 1) / (256LL * INIT_RANDOM_PER_THREAD));
+	const long long per = n / (148LL * 512);
+	return per < 1 ? 1 : per > 8 ? 8 : (int)per;
+}
+inline unsigned init_random_blocks(long long n, int per)
+{
+	return (unsigned)((n + 256LL * per - 1) / (256LL * per));
 }
 
 // Device memory owned by the runtime.

@@ -357,12 +357,3 @@ def test_wide_rate_span_model_compiles_for_sm100a(family, tmp_path):
                        timeout=600)
     assert p.returncode == 0, p.stderr[-3000:]
 
-
-def test_initialize_random_grid_matches_kernel():
-    """The host sizes mb_initialize_random's grid by the trajectories one thread initialises; that
-    count is defined twice (kernel source compiled by NVRTC, host runtime) and must agree."""
-    import re
-    csrc = os.path.join(ROOT, "maboss", "gpu_b200", "csrc")
-    k = re.search(r"#define MB_INIT_RANDOM_PER_THREAD (\d+)", open(os.path.join(csrc, "kernels", "engine.cuh")).read())
-    h = re.search(r"constexpr int INIT_RANDOM_PER_THREAD = (\d+);", open(os.path.join(csrc, "runtime.h")).read())
-    assert k and h and k.group(1) == h.group(1)
