@@ -111,6 +111,7 @@ struct mbb_net_rt
 // 8 groups 7.26e9 transitions/s, 4 groups 6.70e9, 16 groups 6.34e9 (predicated updates of every
 // group register at each rate change cost more than the longer word walk saves)
 constexpr int MBB_GROUPS = 8;
+constexpr int MBB_STEPS_PER_PASS = 4;
 
 struct mbb_lane
 {
@@ -495,7 +496,9 @@ __device__ void mbb_body(const mb_batch_params& B)
 			}
 		}
 
-		if (running)
+		// up to MBB_STEPS_PER_PASS steps of a running trajectory per pass of the work-fetch loop, as
+		// the fast kernel does
+		for (int step = 0; step < MBB_STEPS_PER_PASS && running; step++)
 		{
 			const mb_variant& var = B.vars[vi];
 			const NET net(B, var);

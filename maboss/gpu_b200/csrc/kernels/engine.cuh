@@ -247,6 +247,7 @@ __device__ __forceinline__ void mb_fused_body(const mb_fused_params& P)
 // reference; not bit-exact (different random streams and rate rounding below 2^-shift).
 constexpr int MB_WPG = state_words <= 2 ? 1 : (state_words <= 8 ? 2 : 8);
 constexpr int MB_GROUPS = (state_words + MB_WPG - 1) / MB_WPG;
+constexpr int MB_STEPS_PER_PASS = 4;
 
 // OR of a non-internal index contribution over the warp (128-bit indices as four 32-bit parts).
 __device__ __forceinline__ mb_idx_t mb_or_all(mb_idx_t v)
@@ -820,7 +821,10 @@ extern "C" __global__ void __launch_bounds__(128, 5) mb_fused_fast(mb_fused_para
 			running = true;
 		}
 
-		if (running)
+		// up to MB_STEPS_PER_PASS steps of a running trajectory per pass of the work-fetch loop (its
+		// votes and branches once per four steps: +2.4 % on the 1000-node network, +2.9 % on the
+		// 50-node one; a lane whose trajectory ends idles for the rest of the pass)
+		for (int step = 0; step < MB_STEPS_PER_PASS && running; step++)
 		{
 			const uint4 rb = curand4(&rng); // x: waiting time, (y, z): flip
 			float tn;
