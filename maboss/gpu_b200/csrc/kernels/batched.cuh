@@ -111,7 +111,6 @@ struct mbb_net_rt
 // 8 groups 7.26e9 transitions/s, 4 groups 6.70e9, 16 groups 6.34e9 (predicated updates of every
 // group register at each rate change cost more than the longer word walk saves)
 constexpr int MBB_GROUPS = 8;
-constexpr int MBB_STEPS_PER_PASS = 4;
 
 struct mbb_lane
 {
@@ -398,20 +397,10 @@ __device__ void mbb_body(const mb_batch_params& B)
 			c.st = v.st - off;
 			c.un = v.un - off;
 			c.ws = v.ws - off;
-			for (int w = 0; w < net.W(); w++)
-			{
-				const int i = 32 * w + lane;
-				bool on = false;
-				if (i < net.N())
-				{
-					curandStatePhilox4_32_10_t r;
-					curand_init(B.seed, stream, (unsigned long long)i, &r);
-					on = curand_uniform(&r) <= __ldg(var.istate + i);
-				}
-				const uint32_t word = __ballot_sync(0xffffffffu, on);
+			mb_philox_initial_state(B.seed, stream, net.N(), var.istate, [&](int w, uint32_t word) {
 				if (lane == 0)
 					c.S(w) = word;
-			}
+			});
 			__syncwarp();
 			unsigned long long gsx[MBB_GROUPS];
 #pragma unroll
@@ -496,9 +485,9 @@ __device__ void mbb_body(const mb_batch_params& B)
 			}
 		}
 
-		// up to MBB_STEPS_PER_PASS steps of a running trajectory per pass of the work-fetch loop, as
-		// the fast kernel does
-		for (int step = 0; step < MBB_STEPS_PER_PASS && running; step++)
+		// one step per pass of the work-fetch loop: several (as the fast kernel does) made these
+		// kernels spill (62 bytes) and halved the throughput of the 256-variant sweep
+		if (running)
 		{
 			const mb_variant& var = B.vars[vi];
 			const NET net(B, var);

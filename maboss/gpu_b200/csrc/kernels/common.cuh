@@ -1,7 +1,8 @@
-// Device helpers that do not depend on the model: hashing, fixed-point window accumulation and a
-// runtime-width fixed-point hash insert. Shared by the NVRTC-compiled engine (kernels/engine.cuh)
-// and the ahead-of-time compiled batched kernels (kernels/batched.cuh).
+// Device helpers that do not depend on the model: hashing, fixed-point window accumulation, a
+// runtime-width fixed-point hash insert and the Philox initial state. Shared by the NVRTC-compiled
+// engine (kernels/engine.cuh) and the ahead-of-time compiled batched kernels (kernels/batched.cuh).
 #pragma once
+#include <curand_kernel.h>
 
 __device__ __forceinline__ unsigned long long mb_mix64(unsigned long long x)
 {
@@ -210,4 +211,46 @@ __device__ inline void mb_fixed_insert_rt(const mb_stats_params& p, const unsign
 		}
 	}
 	atomicAdd(p.fp_overflow, 1u);
+}
+
+// ---------------------------------------------------------------- Philox initial state
+
+// The initial state of one trajectory, drawn by a whole warp (fast and batched kernels): node i is
+// on when the uniform that curand_init(seed, stream, i) followed by curand_uniform gives is at most
+// istate[i]. That uniform is output i % 4 of the stream's Philox block i / 4, so one block serves
+// four nodes: lane L draws block 32c + L (nodes 128c + 4L .. 4L + 3) with curand_uniform4, and the
+// lanes of the four words of that chunk take their node's uniform from it by shuffles (one block
+// per lane per 128 nodes instead of one per node; the same states). set_word(w, bits) receives
+// each state word (the same value on every lane).
+template <class SET_WORD>
+__device__ __forceinline__ void mb_philox_initial_state(unsigned long long seed, unsigned long long stream,
+														int n_nodes, const float* __restrict__ istate,
+														SET_WORD set_word)
+{
+	const int lane = threadIdx.x & 31;
+	const int n_words = (n_nodes + 31) >> 5;
+	for (int c = 0; 4 * c < n_words; c++)
+	{
+		float4 u4 = make_float4(1.f, 1.f, 1.f, 1.f);
+		const int b = 32 * c + lane;
+		if (4 * b < n_nodes)
+		{
+			curandStatePhilox4_32_10_t r;
+			curand_init(seed, stream, 4ull * (unsigned long long)b, &r);
+			u4 = curand_uniform4(&r);
+		}
+		for (int ww = 0; ww < 4 && 4 * c + ww < n_words; ww++)
+		{
+			const int w = 4 * c + ww, i = 32 * w + lane;
+			const int src = 8 * ww + (lane >> 2);
+			const float ux = __shfl_sync(0xffffffffu, u4.x, src);
+			const float uy = __shfl_sync(0xffffffffu, u4.y, src);
+			const float uz = __shfl_sync(0xffffffffu, u4.z, src);
+			const float uw = __shfl_sync(0xffffffffu, u4.w, src);
+			const int k = lane & 3;
+			const float u = k == 0 ? ux : k == 1 ? uy : k == 2 ? uz : uw;
+			const bool on = i < n_nodes && u <= __ldg(istate + i);
+			set_word(w, __ballot_sync(0xffffffffu, on));
+		}
+	}
 }

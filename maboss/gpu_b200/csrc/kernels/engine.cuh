@@ -343,20 +343,10 @@ __device__ __forceinline__ void mb_incr_start(const mb_fused_params& P, const mb
 	v.st = v0.st - (threadIdx.x - col);
 	v.un = v0.un - (threadIdx.x - col);
 	v.ws = v0.ws - (threadIdx.x - col);
-	for (int w = 0; w < state_words; w++)
-	{
-		const int i = 32 * w + lane;
-		bool on = false;
-		if (i < state_size)
-		{
-			curandStatePhilox4_32_10_t r;
-			curand_init(P.seed, P.first_traj + t, (unsigned long long)i, &r);
-			on = curand_uniform(&r) <= __ldg(P.istate + i);
-		}
-		const uint32_t word = __ballot_sync(0xffffffffu, on);
+	mb_philox_initial_state(P.seed, P.first_traj + t, state_size, P.istate, [&](int w, uint32_t word) {
 		if (lane == 0)
 			v.S(w) = word;
-	}
+	});
 	__syncwarp();
 #pragma unroll
 	for (int g = 0; g < MB_GROUPS; g++)
