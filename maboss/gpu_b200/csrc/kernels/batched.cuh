@@ -67,11 +67,17 @@ struct mb_batch_params
 	unsigned gstride;	  // gstride = the launch's thread count
 };
 
+// The number of register group sums; words per group = ceil(W / 8). Measured on C5 (256 variants, 1 to 16 words):
+// 8 groups 7.26e9 transitions/s, 4 groups 6.70e9, 16 groups 6.34e9 (predicated updates of every
+// group register at each rate change cost more than the longer word walk saves)
+constexpr int MBB_GROUPS = 8;
+
 // Network access of the kernel body. mbb_net_rt reads a network's descriptor (every network of a
 // batch is runtime data: one launch covers networks of different sizes); the NVRTC build of a
 // single network's batch (MB_FAMILY_BATCH, below) instead gives the same quantities as compile-time
 // constants and tables of that network's generated code, so that loops over its words unroll and
 // no descriptor is read. The variant data (rates, derivatives, accumulators) stays runtime in both.
+
 struct mbb_net_rt
 {
 	const mb_net& n;
@@ -83,6 +89,9 @@ struct mbb_net_rt
 	__device__ __forceinline__ float max_time() const { return n.max_time; }
 	__device__ __forceinline__ float tick() const { return n.tick; }
 	__device__ __forceinline__ int wpg_shift() const { return n.wpg_shift; }
+	// the register groups the kernel keeps: all of them (a runtime bound on the group loops cost
+	// more than the updates of empty groups, whose prefixes then stay equal to the total)
+	__device__ __forceinline__ static constexpr int groups() { return MBB_GROUPS; }
 	__device__ __forceinline__ const uint2* dep() const { return n.dep; }
 	__device__ __forceinline__ const uint4* rec() const { return n.rec; }
 	__device__ __forceinline__ const uint4* ext() const { return n.ext; }
@@ -107,10 +116,6 @@ struct mbb_net_rt
 	}
 };
 
-// register group sums; words per group = ceil(W / 8). Measured on C5 (256 variants, 1 to 16 words):
-// 8 groups 7.26e9 transitions/s, 4 groups 6.70e9, 16 groups 6.34e9 (predicated updates of every
-// group register at each rate change cost more than the longer word walk saves)
-constexpr int MBB_GROUPS = 8;
 
 struct mbb_lane
 {
@@ -167,12 +172,14 @@ __device__ __forceinline__ bool mbb_logic(const NET& net, const mbb_lane& v, int
 }
 
 // gs[i] is the rate sum of groups 0..i (inclusive prefix sums; groups past the network's last are
-// empty, so their prefixes equal the total); a change d in group g moves every prefix from g on
-__device__ __forceinline__ void mbb_group_add(unsigned long long (&gs)[MBB_GROUPS], int g, long long d)
+// empty); a change d in group g moves every kept prefix from g on (ng = NET::groups(): the
+// network's groups in the specialised kernels, all MBB_GROUPS in the ahead-of-time ones)
+__device__ __forceinline__ void mbb_group_add(unsigned long long (&gs)[MBB_GROUPS], int g, long long d, int ng)
 {
 #pragma unroll
 	for (int i = 0; i < MBB_GROUPS; i++)
-		gs[i] += (i >= g) ? (unsigned long long)d : 0ull;
+		if (i < ng)
+			gs[i] += (i >= g) ? (unsigned long long)d : 0ull;
 }
 
 template <class NET>
@@ -408,7 +415,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 				gsx[g] = 0;
 			unsigned long long tot = 0;
 			uint32_t ix = 0;
-			const int wsh = net.wpg_shift();
+			const int wsh = net.wpg_shift(), ng = net.groups();
 			for (int w = 0; w < net.W(); w++)
 			{
 				const int i = 32 * w + lane;
@@ -433,7 +440,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 					c.U(w) = um;
 					c.Q(w) = qw;
 				}
-				mbb_group_add(gsx, w >> wsh, qw);
+				mbb_group_add(gsx, w >> wsh, qw, ng);
 				tot += qw;
 			}
 			__syncwarp();
@@ -534,14 +541,16 @@ __device__ void mbb_body(const mb_batch_params& B)
 			else
 			{
 				const unsigned long long r = __umul64hi(((unsigned long long)rb.y << 32) | rb.z, total);
-				const int wsh = net.wpg_shift(), wpg = 1 << wsh;
-				// the first group whose prefix sum exceeds r: the number of prefixes <= r (r < total,
-				// and the prefixes of the groups past the network's last equal the total)
+				const int wsh = net.wpg_shift(), wpg = 1 << wsh, ng = net.groups();
+				// the first group whose prefix sum exceeds r: the number of the kept prefixes <= r
+				// (r < total, the last kept prefix)
 				unsigned long long cum = 0;
 				int g = 0;
 #pragma unroll
 				for (int i = 0; i < MBB_GROUPS - 1; i++)
 				{
+					if (i + 1 >= ng)
+						break;
 					const bool le = gs[i] <= r;
 					g += le ? 1 : 0;
 					cum = le ? gs[i] : cum;
@@ -622,7 +631,7 @@ __device__ void mbb_body(const mb_batch_params& B)
 					{
 						const long long dq = (long long)qn - (long long)qo;
 						v.Q(wk) += (uint32_t)dq;
-						mbb_group_add(gs, wk >> wsh, dq);
+						mbb_group_add(gs, wk >> wsh, dq, ng);
 						total += (unsigned long long)dq;
 					}
 					if (GRAD && (unstable != was_unstable || on != was_on))
@@ -668,6 +677,8 @@ struct mbb_net_static
 	{
 		return state_words <= MBB_GROUPS ? 0 : state_words <= 2 * MBB_GROUPS ? 1 : state_words <= 4 * MBB_GROUPS ? 2 : 3;
 	}
+	// the register groups the kernel keeps: the network's own (compile-time loop bounds)
+	__device__ __forceinline__ static constexpr int groups() { return (state_words + (1 << wpg_shift()) - 1) >> wpg_shift(); }
 	__device__ __forceinline__ static const uint2* dep() { return reinterpret_cast<const uint2*>(mbg_inc_dep); }
 	__device__ __forceinline__ static const uint4* rec() { return mbg_inc_crec; }
 	__device__ __forceinline__ static const uint4* ext() { return mbg_inc_cext; }
