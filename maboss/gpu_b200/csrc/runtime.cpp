@@ -147,6 +147,16 @@ dbuf::~dbuf()
 		cudaFree(p);
 }
 
+void host_deleter::operator()(void* p) const
+{
+	if (!p)
+		return;
+	if (pinned)
+		cudaFreeHost(p);
+	else
+		std::free(p);
+}
+
 void dbuf::alloc(size_t n)
 {
 	if (p)
@@ -635,8 +645,25 @@ std::unique_ptr<result> stats_state::finalize(long long n, cudaStream_t s)
 		// sorted on the device, copied into the kept host buffers, decoded by host threads
 		if (nb > hbin_cap)
 		{
-			hbin_keys.reset(new uint64_t[2 * (size_t)nb]);
-			hbin_vals.reset(new long long[nb]);
+			hbin_keys.reset();
+			hbin_vals.reset();
+			hbin_cap = 0;
+			auto host_alloc = [](size_t bytes, bool& pinned) {
+				void* p = nullptr;
+				pinned = cudaMallocHost(&p, bytes) == cudaSuccess;
+				if (!pinned)
+				{
+					(void)cudaGetLastError();
+					p = std::malloc(bytes);
+					if (!p)
+						throw engine_error(MB_ERR_LIMIT, "out of host memory for the sparse bins");
+				}
+				return p;
+			};
+			void* hk = host_alloc(2 * (size_t)nb * sizeof(uint64_t), hbin_keys.get_deleter().pinned);
+			hbin_keys.reset(static_cast<uint64_t*>(hk));
+			void* hv = host_alloc((size_t)nb * sizeof(long long), hbin_vals.get_deleter().pinned);
+			hbin_vals.reset(static_cast<long long*>(hv));
 			hbin_cap = nb;
 		}
 		if (nb)

@@ -14,6 +14,7 @@
 
 #include "codegen.h"
 #include "maboss_b200.h"
+#include "sparse_bins.h"
 #include "kernels/params.cuh"
 
 namespace mb {
@@ -212,9 +213,9 @@ struct result
 	// at most 20 non-internal nodes but a large histogram (compact_min_cells or more cells): only its
 	// non-zero cells, in the same sparse form (sp_*), selected on the device; final states dense
 	bool compact = false;
-	std::vector<int> sp_w;
-	std::vector<unsigned __int128> sp_idx;
-	std::vector<long long> sp_val; // occupancy in fixed point (continuous) or count (discrete)
+	bulk_vector<int> sp_w;
+	bulk_vector<unsigned __int128> sp_idx;
+	bulk_vector<long long> sp_val; // occupancy in fixed point (continuous) or count (discrete)
 	std::vector<size_t> sp_begin;  // [n_windows + 1]
 	std::vector<unsigned __int128> fin_idx;
 	std::vector<unsigned> fin_cnt;
@@ -242,6 +243,13 @@ std::unique_ptr<result> merge_results(const std::vector<const result*>& parts);
 int occupancy_exponent(long long n_traj, float tick, bool discrete);
 int entropy_exponent(long long n_traj, float tick, bool discrete);
 
+// Frees host memory from cudaMallocHost (pinned) or, where pinning failed, from malloc.
+struct host_deleter
+{
+	bool pinned = true;
+	void operator()(void* p) const;
+};
+
 // Device accumulators of the three built-in statistics plugins (window averages, final
 // states, fixed points) for one run.
 struct stats_state
@@ -252,9 +260,10 @@ struct stats_state
 	dbuf bin_keys, bin_vals, out_bin_keys, out_bin_vals; // sparse bins (more than 20 non-internal nodes)
 	dbuf cell_idx, cell_vals; // non-zero cells of a large dense histogram (compact results), kept across runs
 	unsigned bin_cap = 0;
-	// host copies of the sorted bins, kept across runs (no re-allocation, no first-touch page faults)
-	std::unique_ptr<uint64_t[]> hbin_keys;
-	std::unique_ptr<long long[]> hbin_vals;
+	// host copies of the sorted bins, kept across runs (no re-allocation, no first-touch page
+	// faults), in pinned memory (copied at full link speed) unless pinning fails (then malloc)
+	std::unique_ptr<uint64_t[], host_deleter> hbin_keys;
+	std::unique_ptr<long long[], host_deleter> hbin_vals;
 	size_t hbin_cap = 0;
 	bool wide = false;
 	unsigned fp_cap = 0;

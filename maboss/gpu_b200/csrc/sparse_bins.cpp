@@ -72,8 +72,8 @@ void parallel(int T, F f)
 } // namespace
 
 void decode_sorted_bins(const uint64_t* keys, const long long* vals, size_t n, int n_windows, int threads,
-						std::vector<int>& sp_w, std::vector<unsigned __int128>& sp_idx,
-						std::vector<long long>& sp_val, std::vector<size_t>& sp_begin,
+						bulk_vector<int>& sp_w, bulk_vector<unsigned __int128>& sp_idx,
+						bulk_vector<long long>& sp_val, std::vector<size_t>& sp_begin,
 						std::vector<unsigned __int128>& fin_idx, std::vector<unsigned>& fin_cnt)
 {
 	// small inputs stay on the calling thread
@@ -104,24 +104,12 @@ void decode_sorted_bins(const uint64_t* keys, const long long* vals, size_t n, i
 		ow[t + 1] = ow[t] + nw[t];
 		of[t + 1] = of[t] + nf[t];
 	}
-	// resize value-initialises (gigabytes for a large job): the two largest vectors on their own threads
-	auto size_part = [&](int part) {
-		if (part == 0)
-			sp_idx.resize(ow[T]);
-		else if (part == 1)
-			sp_val.resize(ow[T]);
-		else
-		{
-			sp_w.resize(ow[T]);
-			fin_idx.resize(of[T]);
-			fin_cnt.resize(of[T]);
-		}
-	};
-	if (T > 1)
-		parallel(3, size_part);
-	else
-		for (int part = 0; part < 3; part++)
-			size_part(part);
+	// the entry vectors are not initialised (bulk_vector): pass 2 writes every element
+	sp_idx.resize(ow[T]);
+	sp_val.resize(ow[T]);
+	sp_w.resize(ow[T]);
+	fin_idx.resize(of[T]);
+	fin_cnt.resize(of[T]);
 	// pass 2: each chunk writes its entries at its offsets, adding equal adjacent keys
 	parallel(T, [&](int t) {
 		size_t a = ow[t], b = of[t];

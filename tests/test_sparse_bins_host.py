@@ -19,7 +19,8 @@ extern "C" int decode(const uint64_t* keys, const long long* vals, size_t n, int
                       int* sp_w, uint64_t* sp_idx, long long* sp_val, size_t* sp_begin, uint64_t* fin_idx,
                       unsigned* fin_cnt, size_t* counts)
 {
-    std::vector<int> w; std::vector<unsigned __int128> idx; std::vector<long long> val; std::vector<size_t> begin;
+    mb::bulk_vector<int> w; mb::bulk_vector<unsigned __int128> idx; mb::bulk_vector<long long> val;
+    std::vector<size_t> begin;
     std::vector<unsigned __int128> fi; std::vector<unsigned> fc;
     mb::decode_sorted_bins(keys, vals, n, n_windows, threads, w, idx, val, begin, fi, fc);
     counts[0] = w.size(); counts[1] = fi.size();
