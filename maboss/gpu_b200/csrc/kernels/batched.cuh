@@ -92,6 +92,7 @@ struct mbb_net_rt
 	// the register groups the kernel keeps: all of them (a runtime bound on the group loops cost
 	// more than the updates of empty groups, whose prefixes then stay equal to the total)
 	__device__ __forceinline__ static constexpr int groups() { return MBB_GROUPS; }
+	__device__ __forceinline__ static constexpr int steps_per_pass() { return 1; }
 	__device__ __forceinline__ const uint2* dep() const { return n.dep; }
 	__device__ __forceinline__ const uint4* rec() const { return n.rec; }
 	__device__ __forceinline__ const uint4* ext() const { return n.ext; }
@@ -492,9 +493,11 @@ __device__ void mbb_body(const mb_batch_params& B)
 			}
 		}
 
-		// one step per pass of the work-fetch loop: several (as the fast kernel does) made these
-		// kernels spill (62 bytes) and halved the throughput of the 256-variant sweep
-		if (running)
+		// steps per pass of the work-fetch loop: several (as in the fast kernel) only in the
+		// specialised gradient kernel (the gradient on the 50-node network 21.5 -> 20.6 ms); the
+		// specialised forward kernel lost 3.5 % with them, and the ahead-of-time kernels spilled 62
+		// bytes and halved the throughput of the 256-variant sweep
+		for (int step = 0; step < (GRAD ? NET::steps_per_pass() : 1) && running; step++)
 		{
 			const mb_variant& var = B.vars[vi];
 			const NET net(B, var);
@@ -679,6 +682,7 @@ struct mbb_net_static
 	}
 	// the register groups the kernel keeps: the network's own (compile-time loop bounds)
 	__device__ __forceinline__ static constexpr int groups() { return (state_words + (1 << wpg_shift()) - 1) >> wpg_shift(); }
+	__device__ __forceinline__ static constexpr int steps_per_pass() { return 4; }
 	__device__ __forceinline__ static const uint2* dep() { return reinterpret_cast<const uint2*>(mbg_inc_dep); }
 	__device__ __forceinline__ static const uint4* rec() { return mbg_inc_crec; }
 	__device__ __forceinline__ static const uint4* ext() { return mbg_inc_cext; }
