@@ -549,9 +549,8 @@ __device__ __forceinline__ int mb_exact_flip(const mb_incr_view& v, int j, mb_id
 		idx ^= (mb_idx_t)1 << pj;
 	ni_changed |= pj >= 0;
 	const int d0 = (int)nj.x, d1 = d0 + (int)(nj.y & 0xffffu);
-	for (int d = d0; d < d1; d++)
-	{
-		const uint4 hdr = __ldg(mbg_inc_crec + d);
+	// the dependents two at a time, both records' loads in flight (+1 % on the 1000-node network)
+	auto dependent = [&](int d, const uint4& hdr) {
 		const int k = (int)(hdr.x & 0xffffu);
 		const uint32_t bk = 1u << (k & 31);
 		const bool on = (v.S(k >> 5) & bk) != 0;
@@ -563,6 +562,15 @@ __device__ __forceinline__ int mb_exact_flip(const mb_incr_view& v, int j, mb_id
 			lo = min(lo, k >> 5);
 			ni_changed |= ((hdr.x >> 21) & 127u) != 0u;
 		}
+	};
+	for (int d = d0; d < d1; d += 2)
+	{
+		const bool two = d + 1 < d1;
+		const uint4 h0 = __ldg(mbg_inc_crec + d);
+		const uint4 h1 = two ? __ldg(mbg_inc_crec + d + 1) : make_uint4(0u, 0u, 0u, 0u);
+		dependent(d, h0);
+		if (two)
+			dependent(d + 1, h1);
 	}
 	return lo;
 }
