@@ -69,3 +69,14 @@ def assert_statistically_equal(p: np.ndarray, n1: int, q: np.ndarray, n2: int, a
     assert z.max() < z_crit, (z.max(), z_crit, int(z.argmax()))
     s2 = float((z[populated] ** 2).sum())
     assert chi2.sf(s2, m) > alpha, (s2 / m, m)
+
+
+def force_node(bnd: str, cfg: str, node: str, on: bool) -> tuple[str, str]:
+    """The model text with `node` forced, as a mutant: both rates 0 and initial state 1 (on) or 0 (off)."""
+    import re
+
+    pat = re.compile(r"(node\s+" + node + r"\s*\{)(.*?)(\})", re.S | re.I)
+    m = pat.search(bnd)
+    body = re.sub(r"rate_up\s*=[^;]*;", "rate_up = @logic ? 0 : 0;", m.group(2))
+    body = re.sub(r"rate_down\s*=[^;]*;", "rate_down = @logic ? 0 : 0;", body)
+    return bnd[:m.start(2)] + body + bnd[m.end(2):], cfg + f"\n{node}.istate = {1 if on else 0};\n"

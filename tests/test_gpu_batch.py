@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import maboss.gpu_b200 as mb
-from conftest import model_text
+from conftest import force_node, model_text
 from maboss.gpu_b200 import synth
 from oracle.oracle import OracleModel
 
@@ -402,17 +402,6 @@ def test_specialised_batch_kernels_equal_the_generic_ones(gpu):
         assert np.array_equal(x, y)
 
 
-def _force(bnd: str, cfg: str, node: str, on: bool) -> tuple[str, str]:
-    """The model text with `node` forced: both rates 0 and initial state 1 (on) or 0 (off)."""
-    import re
-
-    pat = re.compile(r"(node\s+" + node + r"\s*\{)(.*?)(\})", re.S | re.I)
-    m = pat.search(bnd)
-    body = re.sub(r"rate_up\s*=[^;]*;", "rate_up = @logic ? 0 : 0;", m.group(2))
-    body = re.sub(r"rate_down\s*=[^;]*;", "rate_down = @logic ? 0 : 0;", body)
-    return bnd[:m.start(2)] + body + bnd[m.end(2):], cfg + f"\n{node}.istate = {1 if on else 0};\n"
-
-
 @pytest.mark.parametrize("name,node,on", [("sizek", "PI3K", True), ("sizek", "PI3K", False),
                                           ("cellcycle", "CycE", True)])
 def test_mutant_equals_the_edited_model(gpu, name, node, on):
@@ -428,7 +417,7 @@ def test_mutant_equals_the_edited_model(gpu, name, node, on):
     wt = b.add_variant(net, n)
     mv = b.add_variant(net, n, mutants={node: on})
     b.run(11)
-    edited = mb.Model(*_force(bnd, cfg, node, on))
+    edited = mb.Model(*force_node(bnd, cfg, node, on))
     ref = gpu.compile(edited).run(mode="fast", sample_count=n, seed=11)
     got = b.result(mv)
     assert got.transitions == ref.transitions
